@@ -1,0 +1,53 @@
+// Shared device helpers for the Extended-RaBitQ IVF search kernels (sm_100a).
+#pragma once
+
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+namespace erq {
+
+constexpr int kFastSize = 32;     // vectors per FastScan block (inc/defines.hpp:13)
+constexpr int kMaxD = 2048;       // u16 lane sums of the reference are exact up to here
+constexpr int kMaxTopK = 1024;    // largest k the refine kernel's pool supports
+constexpr float kNormEps = 1e-5f; // normalize_query16's eps (inc/utils/space.hpp:756)
+constexpr float kConstBound = 0.58f;  // inc/index/fastscan/FastScan.hpp:295
+
+// Sum of 16 lane partials held by lanes 0..15 of a half-warp, combined in the
+// order GCC 13 expands _mm512_reduce_add_ps: (l, l+8), (l, l+4), (0,2)/(1,3),
+// then the last pair.  shfl_down by 8,4,2,1 inside a 16-lane segment performs
+// exactly those pairings (float addition is commutative, so a+b == b+a
+// bitwise).  The result is valid in lane 0 of the segment.
+__device__ __forceinline__ float tree16_sum(float v) {
+    v = __fadd_rn(v, __shfl_down_sync(0xffffffffu, v, 8, 16));
+    v = __fadd_rn(v, __shfl_down_sync(0xffffffffu, v, 4, 16));
+    v = __fadd_rn(v, __shfl_down_sync(0xffffffffu, v, 2, 16));
+    v = __fadd_rn(v, __shfl_down_sync(0xffffffffu, v, 1, 16));
+    return v;
+}
+
+// (float)(1.0 / (double)x): the reference computes these reciprocals in
+// double and rounds once to float (inc/utils/space.hpp:760,774;
+// inc/index/HASearcher.hpp:56).
+__device__ __forceinline__ float recip_via_double(float x) {
+    return __double2float_rn(__ddiv_rn(1.0, (double)x));
+}
+
+// (int16_t)(t + 0.5 - (t < 0)) evaluated in double (high_acc_quantize16,
+// inc/utils/space.hpp:708-709).  For |t| <= 8191 the double sum is exact, so
+// this is round-half-away-from-zero of t.
+__device__ __forceinline__ int quantize_round(float t) {
+    return (int)__double2int_rz(__dadd_rn(__dadd_rn((double)t, 0.5), t < 0.f ? -1.0 : 0.0));
+}
+
+// Orderable 64-bit key of (non-negative float distance, id): ascending keys
+// are ascending distance, ties by ascending id.
+__device__ __forceinline__ uint64_t dist_key(float d, uint32_t id) {
+    return ((uint64_t)__float_as_uint(d) << 32) | id;
+}
+
+__host__ __device__ __forceinline__ uint64_t div_up(uint64_t a, uint64_t b) {
+    return (a + b - 1) / b;
+}
+
+}  // namespace erq

@@ -1,0 +1,676 @@
+// C ABI of the B200 IVF search (include/erq.h, include/erq_debug.h).
+//
+// Host side: parse the reference's index file (IVF::load,
+// inc/index/IVF.hpp:254-293), place it in device memory in the layout of
+// layout.cuh, and drive the search pipeline of IVF::search
+// (inc/index/IVF.hpp:295-324) over batches of queries:
+//
+//   centroid_dist_kernel -> select_probe_kernel -> scan_kernel -> refine_kernel
+//
+// Per-call scratch comes from the stream-ordered allocator on the caller's
+// stream, so concurrent calls on different streams never share workspace.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/erq.h"
+#include "../../include/erq_debug.h"
+#include "coarse.cuh"
+#include "layout.cuh"
+#include "refine.cuh"
+#include "scan.cuh"
+
+using namespace erq;
+
+// ------------------------------------------------------------------ errors
+namespace {
+thread_local std::string g_last_error;
+
+erq_status fail(erq_status s, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return s;
+}
+
+#define ERQ_CUDA(call)                                                                    \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess) {                                                          \
+            return fail(e_ == cudaErrorMemoryAllocation ? ERQ_ERR_OUT_OF_MEMORY : ERQ_ERR_CUDA, \
+                        "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__,  \
+                        __LINE__);                                                        \
+        }                                                                                 \
+    } while (0)
+
+#define ERQ_TRY(expr)                  \
+    do {                               \
+        erq_status s_ = (expr);        \
+        if (s_ != ERQ_OK) return s_;   \
+    } while (0)
+
+// Restores the caller's current device on scope exit.
+struct DeviceGuard {
+    int prev = -1;
+    erq_status set(int dev) {
+        ERQ_CUDA(cudaGetDevice(&prev));
+        if (prev != dev) ERQ_CUDA(cudaSetDevice(dev));
+        return ERQ_OK;
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+bool is_device_ptr(const void* p) {
+    cudaPointerAttributes attr;
+    if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) {
+        cudaGetLastError();  // clear
+        return false;
+    }
+    return attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged;
+}
+
+// Stream-ordered scratch allocations released on scope exit.
+struct Scratch {
+    cudaStream_t stream;
+    std::vector<void*> ptrs;
+    explicit Scratch(cudaStream_t s) : stream(s) {}
+    template <typename T>
+    erq_status alloc(T** out, size_t count) {
+        void* p = nullptr;
+        const size_t bytes = std::max<size_t>(count * sizeof(T), 16);
+        cudaError_t e = cudaMallocAsync(&p, bytes, stream);
+        if (e != cudaSuccess)
+            return fail(e == cudaErrorMemoryAllocation ? ERQ_ERR_OUT_OF_MEMORY : ERQ_ERR_CUDA,
+                        "cudaMallocAsync(%zu bytes) failed: %s", bytes, cudaGetErrorString(e));
+        ptrs.push_back(p);
+        *out = static_cast<T*>(p);
+        return ERQ_OK;
+    }
+    ~Scratch() {
+        for (void* p : ptrs) cudaFreeAsync(p, stream);
+    }
+};
+
+}  // namespace
+
+// ------------------------------------------------------------------- index
+struct erq_index {
+    int device = 0;
+    uint64_t N = 0, DIM = 0, D = 0, K = 0, EX = 0;
+    uint64_t total_blocks = 0;
+    uint64_t device_bytes = 0;
+    std::vector<uint32_t> h_nblocks;     // per cluster
+    std::vector<uint64_t> top_blocks;    // top_blocks[p] = blocks of the p largest clusters
+    // device arrays
+    float* P = nullptr;
+    float* centroids = nullptr;
+    uint8_t* codes = nullptr;
+    float* onorm = nullptr;
+    uint8_t* excode = nullptr;
+    float* xipnorm = nullptr;
+    uint32_t* ids = nullptr;
+    uint32_t* c_first_block = nullptr;
+    uint32_t* c_first_vec = nullptr;
+    uint32_t* c_size = nullptr;
+    uint32_t* c_nblocks = nullptr;
+
+    ~erq_index() {
+        int prev = -1;
+        cudaGetDevice(&prev);
+        cudaSetDevice(device);
+        for (void* p : {(void*)P, (void*)centroids, (void*)codes, (void*)onorm, (void*)excode,
+                        (void*)xipnorm, (void*)ids, (void*)c_first_block, (void*)c_first_vec,
+                        (void*)c_size, (void*)c_nblocks})
+            if (p) cudaFree(p);
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+namespace {
+
+struct FileCloser {
+    void operator()(FILE* f) const {
+        if (f) fclose(f);
+    }
+};
+
+erq_status read_to_device(FILE* f, void* dst, size_t bytes, std::vector<uint8_t>& staging,
+                          const char* what) {
+    const size_t chunk = staging.size();
+    uint8_t* d = static_cast<uint8_t*>(dst);
+    for (size_t off = 0; off < bytes; off += chunk) {
+        const size_t n = std::min(chunk, bytes - off);
+        if (fread(staging.data(), 1, n, f) != n)
+            return fail(ERQ_ERR_FORMAT, "index file truncated while reading %s", what);
+        ERQ_CUDA(cudaMemcpy(d + off, staging.data(), n, cudaMemcpyHostToDevice));
+    }
+    return ERQ_OK;
+}
+
+template <typename T>
+erq_status dev_alloc(erq_index* idx, T** p, size_t count) {
+    const size_t bytes = std::max<size_t>(count * sizeof(T), 16);
+    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), bytes);
+    if (e != cudaSuccess)
+        return fail(e == cudaErrorMemoryAllocation ? ERQ_ERR_OUT_OF_MEMORY : ERQ_ERR_CUDA,
+                    "cudaMalloc(%zu bytes) failed: %s", bytes, cudaGetErrorString(e));
+    idx->device_bytes += bytes;
+    return ERQ_OK;
+}
+
+erq_status load_impl(const char* path, erq_index* idx) {
+    std::unique_ptr<FILE, FileCloser> f(fopen(path, "rb"));
+    if (!f) return fail(ERQ_ERR_IO, "cannot open index file '%s'", path);
+    uint64_t hdr[4];
+    if (fread(hdr, sizeof(uint64_t), 4, f.get()) != 4)
+        return fail(ERQ_ERR_FORMAT, "index file '%s' too short for its header", path);
+    idx->N = hdr[0];
+    idx->DIM = hdr[1];
+    idx->K = hdr[2];
+    idx->EX = hdr[3];
+    const uint64_t EX = idx->EX;
+    if (!(EX == 2 || EX == 3 || EX == 4 || EX == 6 || EX == 7 || EX == 8))
+        return fail(ERQ_ERR_FORMAT, "unsupported EX_BITS %llu (expected 2,3,4,6,7,8)",
+                    (unsigned long long)EX);
+    if (idx->DIM == 0 || idx->K == 0)
+        return fail(ERQ_ERR_FORMAT, "bad header: DIM=%llu K=%llu", (unsigned long long)idx->DIM,
+                    (unsigned long long)idx->K);
+    if (idx->K >= 20000)
+        return fail(ERQ_ERR_UNSUPPORTED,
+                    "K=%llu >= 20000: the reference keeps an HNSW coarse quantiser in a side file "
+                    "for such indexes, which this library does not read",
+                    (unsigned long long)idx->K);
+    idx->D = (idx->DIM + 63) / 64 * 64;
+    if (idx->D > (uint64_t)kMaxD)
+        return fail(ERQ_ERR_UNSUPPORTED, "padded dimension %llu exceeds %d",
+                    (unsigned long long)idx->D, kMaxD);
+    if (idx->N >= (1ull << 32))
+        return fail(ERQ_ERR_UNSUPPORTED, "N=%llu exceeds 2^32-1", (unsigned long long)idx->N);
+    const uint64_t D = idx->D, K = idx->K, N = idx->N;
+
+    std::vector<uint64_t> sizes(K);
+    if (fread(sizes.data(), sizeof(uint64_t), K, f.get()) != K)
+        return fail(ERQ_ERR_FORMAT, "index file truncated in the cluster sizes");
+    std::vector<uint32_t> first_block(K), first_vec(K), csize(K);
+    idx->h_nblocks.resize(K);
+    uint64_t tot = 0, blocks = 0;
+    for (uint64_t c = 0; c < K; ++c) {
+        if (sizes[c] > N) return fail(ERQ_ERR_FORMAT, "cluster %llu larger than N", (unsigned long long)c);
+        first_block[c] = (uint32_t)blocks;
+        first_vec[c] = (uint32_t)tot;
+        csize[c] = (uint32_t)sizes[c];
+        idx->h_nblocks[c] = (uint32_t)div_up(sizes[c], kFastSize);
+        tot += sizes[c];
+        blocks += idx->h_nblocks[c];
+    }
+    if (tot != N)
+        return fail(ERQ_ERR_FORMAT, "cluster sizes sum to %llu, header says N=%llu",
+                    (unsigned long long)tot, (unsigned long long)N);
+    idx->total_blocks = blocks;
+    {
+        std::vector<uint64_t> nbs(idx->h_nblocks.begin(), idx->h_nblocks.end());
+        std::sort(nbs.begin(), nbs.end(), std::greater<uint64_t>());
+        idx->top_blocks.assign(K + 1, 0);
+        for (uint64_t i = 0; i < K; ++i) idx->top_blocks[i + 1] = idx->top_blocks[i] + nbs[i];
+    }
+    // expected remaining size: P, centroids, short data, long codes, factors, ids
+    const uint64_t code_len = D * EX / 8;
+    const uint64_t raw_block = 4 * D + kFastSize * sizeof(float);
+
+    std::vector<uint8_t> staging(64ull << 20);
+    ERQ_TRY(dev_alloc(idx, &idx->P, D * D));
+    ERQ_TRY(read_to_device(f.get(), idx->P, D * D * sizeof(float), staging, "the rotation matrix"));
+    ERQ_TRY(dev_alloc(idx, &idx->centroids, K * D));
+    ERQ_TRY(read_to_device(f.get(), idx->centroids, K * D * sizeof(float), staging, "the centroids"));
+    {
+        uint8_t* raw = nullptr;
+        cudaError_t e = cudaMalloc(&raw, std::max<uint64_t>(blocks * raw_block, 16));
+        if (e != cudaSuccess) return fail(ERQ_ERR_OUT_OF_MEMORY, "cudaMalloc for short codes failed");
+        erq_status s = read_to_device(f.get(), raw, blocks * raw_block, staging, "the short codes");
+        if (s == ERQ_OK) s = dev_alloc(idx, &idx->codes, blocks * 4 * D);
+        if (s == ERQ_OK) s = dev_alloc(idx, &idx->onorm, blocks * kFastSize);
+        if (s == ERQ_OK && blocks > 0) {
+            transform_blocks_kernel<<<1184, 256>>>(raw, idx->codes, idx->onorm, blocks, (int)D);
+            e = cudaGetLastError();
+            if (e == cudaSuccess) e = cudaDeviceSynchronize();
+            if (e != cudaSuccess)
+                s = fail(ERQ_ERR_CUDA, "block layout kernel failed: %s", cudaGetErrorString(e));
+        }
+        cudaFree(raw);
+        if (s != ERQ_OK) return s;
+    }
+    ERQ_TRY(dev_alloc(idx, &idx->excode, N * code_len + 64));
+    ERQ_TRY(read_to_device(f.get(), idx->excode, N * code_len, staging, "the EX-bit codes"));
+    ERQ_TRY(dev_alloc(idx, &idx->xipnorm, N));
+    ERQ_TRY(read_to_device(f.get(), idx->xipnorm, N * sizeof(float), staging, "the EX factors"));
+    ERQ_TRY(dev_alloc(idx, &idx->ids, N));
+    ERQ_TRY(read_to_device(f.get(), idx->ids, N * sizeof(uint32_t), staging, "the ids"));
+    ERQ_TRY(dev_alloc(idx, &idx->c_first_block, K));
+    ERQ_TRY(dev_alloc(idx, &idx->c_first_vec, K));
+    ERQ_TRY(dev_alloc(idx, &idx->c_size, K));
+    ERQ_TRY(dev_alloc(idx, &idx->c_nblocks, K));
+    ERQ_CUDA(cudaMemcpy(idx->c_first_block, first_block.data(), K * 4, cudaMemcpyHostToDevice));
+    ERQ_CUDA(cudaMemcpy(idx->c_first_vec, first_vec.data(), K * 4, cudaMemcpyHostToDevice));
+    ERQ_CUDA(cudaMemcpy(idx->c_size, csize.data(), K * 4, cudaMemcpyHostToDevice));
+    ERQ_CUDA(cudaMemcpy(idx->c_nblocks, idx->h_nblocks.data(), K * 4, cudaMemcpyHostToDevice));
+    return ERQ_OK;
+}
+
+// ------------------------------------------------------------ pipeline
+size_t scan_smem_bytes(int D) { return 256 + (size_t)(D / 64) * 512 + (size_t)D * 4 + 64; }
+size_t refine_smem_bytes(int D, int k) {
+    const int kpad = (k + 31) & ~31;
+    return (size_t)kRefineWarps * ((size_t)D + 2 * kpad) * 4;
+}
+int next_pow2(int x) {
+    int p = 1;
+    while (p < x) p <<= 1;
+    return p;
+}
+
+erq_status configure_kernels(int D, int K, int k) {
+    const int kp2 = next_pow2(K);
+    ERQ_CUDA(cudaFuncSetAttribute(select_probe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  kp2 * 8));
+    ERQ_CUDA(cudaFuncSetAttribute(scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)scan_smem_bytes(D)));
+    const int rs = (int)refine_smem_bytes(D, k);
+    ERQ_CUDA(cudaFuncSetAttribute(refine_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, rs));
+    ERQ_CUDA(cudaFuncSetAttribute(refine_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, rs));
+    ERQ_CUDA(cudaFuncSetAttribute(refine_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, rs));
+    ERQ_CUDA(cudaFuncSetAttribute(refine_kernel<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, rs));
+    ERQ_CUDA(cudaFuncSetAttribute(refine_kernel<7>, cudaFuncAttributeMaxDynamicSharedMemorySize, rs));
+    ERQ_CUDA(cudaFuncSetAttribute(refine_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, rs));
+    return ERQ_OK;
+}
+
+// Device buffers of one query batch.
+struct Batch {
+    const float* qrot = nullptr;  // [nq][D] on device
+    uint64_t nq = 0;
+    float* dist = nullptr;        // [nq][K]
+    uint32_t* probe_cid = nullptr;
+    float* probe_sqy = nullptr;
+    uint64_t* s_off = nullptr;
+    int32_t* S = nullptr;
+    float* delta = nullptr;
+    float* sumq = nullptr;
+};
+
+// Largest query batch whose scan workspace fits the budget.
+uint64_t batch_queries(const erq_index* idx, uint64_t nprobe, uint64_t nq) {
+    const uint64_t per_q = 32ull * idx->top_blocks[nprobe] * sizeof(int32_t) +
+                           idx->K * sizeof(float) + nprobe * 24;
+    const uint64_t budget = 3ull << 30;
+    uint64_t b = std::max<uint64_t>(1, budget / std::max<uint64_t>(per_q, 1));
+    return std::min(b, nq);
+}
+
+erq_status alloc_batch(Scratch& s, const erq_index* idx, uint64_t nq, uint64_t nprobe, Batch& b) {
+    b.nq = nq;
+    ERQ_TRY(s.alloc(&b.dist, nq * idx->K));
+    ERQ_TRY(s.alloc(&b.probe_cid, nq * nprobe));
+    ERQ_TRY(s.alloc(&b.probe_sqy, nq * nprobe));
+    ERQ_TRY(s.alloc(&b.s_off, nq * nprobe));
+    ERQ_TRY(s.alloc(&b.S, nq * 32ull * idx->top_blocks[nprobe]));
+    ERQ_TRY(s.alloc(&b.delta, nq * nprobe));
+    ERQ_TRY(s.alloc(&b.sumq, nq * nprobe));
+    return ERQ_OK;
+}
+
+erq_status launch_probe(const erq_index* idx, const Batch& b, uint64_t nprobe, cudaStream_t st) {
+    const int D = (int)idx->D, K = (int)idx->K;
+    dim3 g1((unsigned)div_up(K, kCdTC), (unsigned)div_up(b.nq, kCdTQ));
+    centroid_dist_kernel<<<g1, 256, 0, st>>>(b.qrot, (int)b.nq, idx->centroids, K, D, b.dist);
+    ERQ_CUDA(cudaGetLastError());
+    const int kp2 = next_pow2(K);
+    const int thr = std::min(1024, std::max(128, kp2 / 8));
+    const uint64_t stride = 32ull * idx->top_blocks[nprobe];
+    select_probe_kernel<<<(unsigned)b.nq, thr, (size_t)kp2 * 8, st>>>(
+        b.dist, (int)b.nq, K, kp2, (int)nprobe, idx->c_nblocks, stride, b.probe_cid, b.probe_sqy,
+        b.s_off);
+    ERQ_CUDA(cudaGetLastError());
+    return ERQ_OK;
+}
+
+erq_status launch_scan(const erq_index* idx, const Batch& b, uint64_t nprobe, cudaStream_t st) {
+    ScanArgs a;
+    a.qrot = b.qrot;
+    a.centroids = idx->centroids;
+    a.probe_cid = b.probe_cid;
+    a.probe_sqy = b.probe_sqy;
+    a.codes = idx->codes;
+    a.c_first_block = idx->c_first_block;
+    a.c_nblocks = idx->c_nblocks;
+    a.s_off = b.s_off;
+    a.S = b.S;
+    a.qp_delta = b.delta;
+    a.qp_sumq = b.sumq;
+    a.D = (int)idx->D;
+    a.nprobe = (int)nprobe;
+    const uint64_t pairs = b.nq * nprobe;
+    if (pairs > 0x7fffffffull) return fail(ERQ_ERR_INVALID_ARGUMENT, "too many (query, probe) pairs");
+    scan_kernel<<<(unsigned)pairs, kScanWarps * 32, scan_smem_bytes(a.D), st>>>(a);
+    ERQ_CUDA(cudaGetLastError());
+    return ERQ_OK;
+}
+
+erq_status launch_refine(const erq_index* idx, const Batch& b, uint64_t nprobe, uint64_t k,
+                         uint32_t* out_ids, float* out_dists, cudaStream_t st) {
+    RefineArgs a;
+    a.qrot = b.qrot;
+    a.centroids = idx->centroids;
+    a.probe_cid = b.probe_cid;
+    a.probe_sqy = b.probe_sqy;
+    a.s_off = b.s_off;
+    a.S = b.S;
+    a.qp_delta = b.delta;
+    a.qp_sumq = b.sumq;
+    a.onorm = idx->onorm;
+    a.excode = idx->excode;
+    a.xipnorm = idx->xipnorm;
+    a.ids = idx->ids;
+    a.c_first_block = idx->c_first_block;
+    a.c_first_vec = idx->c_first_vec;
+    a.c_size = idx->c_size;
+    a.out_ids = out_ids;
+    a.out_dists = out_dists;
+    a.nq = (int)b.nq;
+    a.D = (int)idx->D;
+    a.EX = (int)idx->EX;
+    a.nprobe = (int)nprobe;
+    a.k = (int)k;
+    const unsigned grid = (unsigned)div_up(b.nq, kRefineWarps);
+    const size_t smem = refine_smem_bytes(a.D, a.k);
+    switch (idx->EX) {
+        case 2: refine_kernel<2><<<grid, kRefineWarps * 32, smem, st>>>(a); break;
+        case 3: refine_kernel<3><<<grid, kRefineWarps * 32, smem, st>>>(a); break;
+        case 4: refine_kernel<4><<<grid, kRefineWarps * 32, smem, st>>>(a); break;
+        case 6: refine_kernel<6><<<grid, kRefineWarps * 32, smem, st>>>(a); break;
+        case 7: refine_kernel<7><<<grid, kRefineWarps * 32, smem, st>>>(a); break;
+        case 8: refine_kernel<8><<<grid, kRefineWarps * 32, smem, st>>>(a); break;
+        default: return fail(ERQ_ERR_FORMAT, "bad EX");
+    }
+    ERQ_CUDA(cudaGetLastError());
+    return ERQ_OK;
+}
+
+erq_status check_search_args(const erq_index* idx, uint64_t nq, uint64_t k, uint64_t nprobe,
+                             const void* q, const void* ids) {
+    if (!idx) return fail(ERQ_ERR_INVALID_ARGUMENT, "index is NULL");
+    if (nq == 0) return ERQ_OK;
+    if (!q || !ids) return fail(ERQ_ERR_INVALID_ARGUMENT, "queries and ids must not be NULL");
+    if (k < 1 || k > (uint64_t)kMaxTopK)
+        return fail(ERQ_ERR_INVALID_ARGUMENT, "k=%llu outside [1, %d]", (unsigned long long)k, kMaxTopK);
+    if (nprobe < 1 || nprobe > idx->K)
+        return fail(ERQ_ERR_INVALID_ARGUMENT, "nprobe=%llu outside [1, K=%llu]",
+                    (unsigned long long)nprobe, (unsigned long long)idx->K);
+    if (nq > (1ull << 30)) return fail(ERQ_ERR_INVALID_ARGUMENT, "nq too large");
+    return ERQ_OK;
+}
+
+// Rotated queries on the device -> ids/dists on the device.
+erq_status search_device(const erq_index* idx, const float* qrot_dev, uint64_t nq, uint64_t k,
+                         uint64_t nprobe, uint32_t* ids_dev, float* dists_dev, cudaStream_t st) {
+    ERQ_TRY(configure_kernels((int)idx->D, (int)idx->K, (int)k));
+    const uint64_t bq = batch_queries(idx, nprobe, nq);
+    Scratch s(st);
+    Batch b;
+    ERQ_TRY(alloc_batch(s, idx, bq, nprobe, b));
+    for (uint64_t q0 = 0; q0 < nq; q0 += bq) {
+        b.nq = std::min(bq, nq - q0);
+        b.qrot = qrot_dev + q0 * idx->D;
+        ERQ_TRY(launch_probe(idx, b, nprobe, st));
+        ERQ_TRY(launch_scan(idx, b, nprobe, st));
+        ERQ_TRY(launch_refine(idx, b, nprobe, k, ids_dev + q0 * k,
+                              dists_dev ? dists_dev + q0 * k : nullptr, st));
+    }
+    return ERQ_OK;
+}
+
+erq_status rotate_device(const erq_index* idx, const float* q_dev, uint64_t nq, float* out_dev,
+                         cudaStream_t st) {
+    if (nq == 0) return ERQ_OK;
+    dim3 grid((unsigned)div_up(idx->D, kRotBN), (unsigned)div_up(nq, kRotBM));
+    rotate_kernel<<<grid, 256, 0, st>>>(q_dev, (int)nq, (int)idx->DIM, idx->P, (int)idx->D, out_dev);
+    ERQ_CUDA(cudaGetLastError());
+    return ERQ_OK;
+}
+
+// Shared body of erq_search / erq_search_raw.
+erq_status search_entry(const erq_index* idx, const float* queries, bool rotated, uint64_t nq,
+                        uint64_t k, uint64_t nprobe, uint32_t* ids, float* dists, void* stream) {
+    ERQ_TRY(check_search_args(idx, nq, k, nprobe, queries, ids));
+    if (nq == 0) return ERQ_OK;
+    DeviceGuard guard;
+    ERQ_TRY(guard.set(idx->device));
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const uint64_t in_cols = rotated ? idx->D : idx->DIM;
+    const bool q_dev = is_device_ptr(queries);
+    const bool ids_dev = is_device_ptr(ids);
+    const bool d_dev = dists == nullptr || is_device_ptr(dists);
+    Scratch s(st);
+    const float* qin = queries;
+    if (!q_dev) {
+        float* tmp = nullptr;
+        ERQ_TRY(s.alloc(&tmp, nq * in_cols));
+        ERQ_CUDA(cudaMemcpyAsync(tmp, queries, nq * in_cols * sizeof(float),
+                                 cudaMemcpyHostToDevice, st));
+        qin = tmp;
+    }
+    const float* qrot = qin;
+    if (!rotated) {
+        float* tmp = nullptr;
+        ERQ_TRY(s.alloc(&tmp, nq * idx->D));
+        ERQ_TRY(rotate_device(idx, qin, nq, tmp, st));
+        qrot = tmp;
+    }
+    uint32_t* ids_out = ids;
+    float* d_out = dists;
+    if (!ids_dev) ERQ_TRY(s.alloc(&ids_out, nq * k));
+    if (!d_dev) ERQ_TRY(s.alloc(&d_out, nq * k));
+    ERQ_TRY(search_device(idx, qrot, nq, k, nprobe, ids_out, d_out, st));
+    const bool host_io = !q_dev || !ids_dev || !d_dev;
+    if (!ids_dev)
+        ERQ_CUDA(cudaMemcpyAsync(ids, ids_out, nq * k * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    if (!d_dev)
+        ERQ_CUDA(cudaMemcpyAsync(dists, d_out, nq * k * sizeof(float), cudaMemcpyDeviceToHost, st));
+    if (host_io) ERQ_CUDA(cudaStreamSynchronize(st));
+    return ERQ_OK;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ C ABI
+extern "C" {
+
+int erq_version(void) { return ERQ_API_VERSION; }
+
+const char* erq_status_string(erq_status s) {
+    switch (s) {
+        case ERQ_OK: return "ok";
+        case ERQ_ERR_INVALID_ARGUMENT: return "invalid argument";
+        case ERQ_ERR_IO: return "i/o error";
+        case ERQ_ERR_FORMAT: return "bad index format";
+        case ERQ_ERR_UNSUPPORTED: return "unsupported";
+        case ERQ_ERR_CUDA: return "cuda error";
+        case ERQ_ERR_OUT_OF_MEMORY: return "out of memory";
+        case ERQ_ERR_TIMEOUT: return "timeout";
+    }
+    return "unknown status";
+}
+
+const char* erq_last_error(void) { return g_last_error.c_str(); }
+
+erq_status erq_index_load(const char* path, int device, erq_index** out) {
+    if (!out) return fail(ERQ_ERR_INVALID_ARGUMENT, "out is NULL");
+    *out = nullptr;
+    if (!path) return fail(ERQ_ERR_INVALID_ARGUMENT, "path is NULL");
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0)
+        return fail(ERQ_ERR_CUDA, "no CUDA device available (%s)", cudaGetErrorString(e));
+    if (device < 0 || device >= ndev)
+        return fail(ERQ_ERR_INVALID_ARGUMENT, "device %d outside [0, %d)", device, ndev);
+    DeviceGuard guard;
+    ERQ_TRY(guard.set(device));
+    std::unique_ptr<erq_index> idx(new (std::nothrow) erq_index());
+    if (!idx) return fail(ERQ_ERR_OUT_OF_MEMORY, "host allocation failed");
+    idx->device = device;
+    ERQ_TRY(load_impl(path, idx.get()));
+    *out = idx.release();
+    return ERQ_OK;
+}
+
+erq_status erq_index_get_info(const erq_index* idx, erq_index_info* info) {
+    if (!idx || !info) return fail(ERQ_ERR_INVALID_ARGUMENT, "NULL argument");
+    info->n = idx->N;
+    info->dim = idx->DIM;
+    info->padded_dim = idx->D;
+    info->num_clusters = idx->K;
+    info->ex_bits = idx->EX;
+    info->device_bytes = idx->device_bytes;
+    info->device = idx->device;
+    return ERQ_OK;
+}
+
+void erq_index_free(erq_index* idx) { delete idx; }
+
+erq_status erq_rotate(const erq_index* idx, const float* queries, uint64_t nq, float* rotated,
+                      void* stream) {
+    if (!idx) return fail(ERQ_ERR_INVALID_ARGUMENT, "index is NULL");
+    if (nq == 0) return ERQ_OK;
+    if (!queries || !rotated) return fail(ERQ_ERR_INVALID_ARGUMENT, "NULL buffer");
+    DeviceGuard guard;
+    ERQ_TRY(guard.set(idx->device));
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const bool q_dev = is_device_ptr(queries), o_dev = is_device_ptr(rotated);
+    Scratch s(st);
+    const float* qin = queries;
+    float* out = rotated;
+    if (!q_dev) {
+        float* tmp = nullptr;
+        ERQ_TRY(s.alloc(&tmp, nq * idx->DIM));
+        ERQ_CUDA(cudaMemcpyAsync(tmp, queries, nq * idx->DIM * 4, cudaMemcpyHostToDevice, st));
+        qin = tmp;
+    }
+    if (!o_dev) ERQ_TRY(s.alloc(&out, nq * idx->D));
+    ERQ_TRY(rotate_device(idx, qin, nq, out, st));
+    if (!o_dev) {
+        ERQ_CUDA(cudaMemcpyAsync(rotated, out, nq * idx->D * 4, cudaMemcpyDeviceToHost, st));
+        ERQ_CUDA(cudaStreamSynchronize(st));
+    } else if (!q_dev) {
+        ERQ_CUDA(cudaStreamSynchronize(st));
+    }
+    return ERQ_OK;
+}
+
+erq_status erq_search(const erq_index* idx, const float* rotated_queries, uint64_t nq, uint64_t k,
+                      uint64_t nprobe, uint32_t* ids, float* dists, void* stream) {
+    return search_entry(idx, rotated_queries, true, nq, k, nprobe, ids, dists, stream);
+}
+
+erq_status erq_search_raw(const erq_index* idx, const float* queries, uint64_t nq, uint64_t k,
+                          uint64_t nprobe, uint32_t* ids, float* dists, void* stream) {
+    return search_entry(idx, queries, false, nq, k, nprobe, ids, dists, stream);
+}
+
+// ------------------------------------------------------------- debug ABI
+erq_status erq_debug_probe(const erq_index* idx, const float* qrot, uint64_t nq, uint64_t nprobe,
+                           uint32_t* cids, float* sqr_y) {
+    if (!idx || !qrot || !cids || !sqr_y) return fail(ERQ_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (nprobe < 1 || nprobe > idx->K) return fail(ERQ_ERR_INVALID_ARGUMENT, "bad nprobe");
+    if (nq == 0) return ERQ_OK;
+    DeviceGuard guard;
+    ERQ_TRY(guard.set(idx->device));
+    ERQ_TRY(configure_kernels((int)idx->D, (int)idx->K, 1));
+    cudaStream_t st = 0;
+    Scratch s(st);
+    float* q = nullptr;
+    ERQ_TRY(s.alloc(&q, nq * idx->D));
+    ERQ_CUDA(cudaMemcpyAsync(q, qrot, nq * idx->D * 4, cudaMemcpyHostToDevice, st));
+    Batch b;
+    ERQ_TRY(alloc_batch(s, idx, nq, nprobe, b));
+    b.qrot = q;
+    ERQ_TRY(launch_probe(idx, b, nprobe, st));
+    ERQ_CUDA(cudaMemcpyAsync(cids, b.probe_cid, nq * nprobe * 4, cudaMemcpyDeviceToHost, st));
+    ERQ_CUDA(cudaMemcpyAsync(sqr_y, b.probe_sqy, nq * nprobe * 4, cudaMemcpyDeviceToHost, st));
+    ERQ_CUDA(cudaStreamSynchronize(st));
+    return ERQ_OK;
+}
+
+erq_status erq_debug_centroid_dists(const erq_index* idx, const float* qrot, uint64_t nq,
+                                    float* dist) {
+    if (!idx || !qrot || !dist) return fail(ERQ_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (nq == 0) return ERQ_OK;
+    DeviceGuard guard;
+    ERQ_TRY(guard.set(idx->device));
+    cudaStream_t st = 0;
+    Scratch s(st);
+    float* q = nullptr;
+    float* d = nullptr;
+    ERQ_TRY(s.alloc(&q, nq * idx->D));
+    ERQ_TRY(s.alloc(&d, nq * idx->K));
+    ERQ_CUDA(cudaMemcpyAsync(q, qrot, nq * idx->D * 4, cudaMemcpyHostToDevice, st));
+    dim3 g1((unsigned)div_up(idx->K, kCdTC), (unsigned)div_up(nq, kCdTQ));
+    centroid_dist_kernel<<<g1, 256, 0, st>>>(q, (int)nq, idx->centroids, (int)idx->K, (int)idx->D, d);
+    ERQ_CUDA(cudaGetLastError());
+    ERQ_CUDA(cudaMemcpyAsync(dist, d, nq * idx->K * 4, cudaMemcpyDeviceToHost, st));
+    ERQ_CUDA(cudaStreamSynchronize(st));
+    return ERQ_OK;
+}
+
+uint64_t erq_debug_scan_capacity(const erq_index* idx, uint64_t nq, uint64_t nprobe) {
+    if (!idx || nprobe > idx->K) return 0;
+    return nq * 32ull * idx->top_blocks[nprobe];
+}
+
+erq_status erq_debug_scan(const erq_index* idx, const float* qrot, uint64_t nq, uint64_t nprobe,
+                          uint32_t* cids, float* sqr_y, float* delta, float* sumq,
+                          uint64_t* s_offsets, int32_t* S, uint64_t s_capacity) {
+    if (!idx || !qrot || !cids || !sqr_y || !delta || !sumq || !s_offsets || !S)
+        return fail(ERQ_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (nprobe < 1 || nprobe > idx->K) return fail(ERQ_ERR_INVALID_ARGUMENT, "bad nprobe");
+    if (nq == 0) return ERQ_OK;
+    const uint64_t need = nq * 32ull * idx->top_blocks[nprobe];
+    if (s_capacity < need)
+        return fail(ERQ_ERR_INVALID_ARGUMENT, "S capacity %llu < %llu",
+                    (unsigned long long)s_capacity, (unsigned long long)need);
+    DeviceGuard guard;
+    ERQ_TRY(guard.set(idx->device));
+    ERQ_TRY(configure_kernels((int)idx->D, (int)idx->K, 1));
+    cudaStream_t st = 0;
+    Scratch s(st);
+    float* q = nullptr;
+    ERQ_TRY(s.alloc(&q, nq * idx->D));
+    ERQ_CUDA(cudaMemcpyAsync(q, qrot, nq * idx->D * 4, cudaMemcpyHostToDevice, st));
+    Batch b;
+    ERQ_TRY(alloc_batch(s, idx, nq, nprobe, b));
+    b.qrot = q;
+    ERQ_CUDA(cudaMemsetAsync(b.S, 0, need * 4, st));
+    ERQ_TRY(launch_probe(idx, b, nprobe, st));
+    ERQ_TRY(launch_scan(idx, b, nprobe, st));
+    const uint64_t np = nq * nprobe;
+    ERQ_CUDA(cudaMemcpyAsync(cids, b.probe_cid, np * 4, cudaMemcpyDeviceToHost, st));
+    ERQ_CUDA(cudaMemcpyAsync(sqr_y, b.probe_sqy, np * 4, cudaMemcpyDeviceToHost, st));
+    ERQ_CUDA(cudaMemcpyAsync(delta, b.delta, np * 4, cudaMemcpyDeviceToHost, st));
+    ERQ_CUDA(cudaMemcpyAsync(sumq, b.sumq, np * 4, cudaMemcpyDeviceToHost, st));
+    ERQ_CUDA(cudaMemcpyAsync(s_offsets, b.s_off, np * 8, cudaMemcpyDeviceToHost, st));
+    ERQ_CUDA(cudaMemcpyAsync(S, b.S, need * 4, cudaMemcpyDeviceToHost, st));
+    ERQ_CUDA(cudaStreamSynchronize(st));
+    return ERQ_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,99 @@
+"""ctypes binding of lib/liberq.so (include/erq.h, include/erq_debug.h).
+
+There is no fallback: if the CUDA library is missing or fails to load, every
+entry point raises.  Build it with ``make -C extended-rabitq_b200``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+PKG_ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(PKG_ROOT, "lib", "liberq.so")
+
+# erq_status values (include/erq.h)
+ERQ_OK = 0
+STATUS_NAMES = {
+    0: "ERQ_OK",
+    1: "ERQ_ERR_INVALID_ARGUMENT",
+    2: "ERQ_ERR_IO",
+    3: "ERQ_ERR_FORMAT",
+    4: "ERQ_ERR_UNSUPPORTED",
+    5: "ERQ_ERR_CUDA",
+    6: "ERQ_ERR_OUT_OF_MEMORY",
+    7: "ERQ_ERR_TIMEOUT",
+}
+
+# Every symbol include/erq.h and include/erq_debug.h declare.
+EXPORTED_SYMBOLS = (
+    "erq_version", "erq_status_string", "erq_last_error", "erq_index_load",
+    "erq_index_get_info", "erq_index_free", "erq_rotate", "erq_search", "erq_search_raw",
+    "erq_debug_scan_capacity", "erq_debug_centroid_dists", "erq_debug_probe", "erq_debug_scan",
+)
+
+
+class ErqError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        self.status = status
+        self.status_name = STATUS_NAMES.get(status, str(status))
+        super().__init__(f"{self.status_name}: {message}")
+
+
+class IndexInfo(C.Structure):
+    _fields_ = [
+        ("n", C.c_uint64),
+        ("dim", C.c_uint64),
+        ("padded_dim", C.c_uint64),
+        ("num_clusters", C.c_uint64),
+        ("ex_bits", C.c_uint64),
+        ("device_bytes", C.c_uint64),
+        ("device", C.c_int),
+    ]
+
+
+_lib = None
+
+
+def load_library(path: str | None = None) -> C.CDLL:
+    """Load liberq.so once and declare its signatures."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = path or LIB_PATH
+    if not os.path.exists(path):
+        raise ImportError(
+            f"{path} is not built; run `make -C {PKG_ROOT}` (this package has no CPU fallback)")
+    lib = C.CDLL(path)
+    vp, u64, f32p, u32p = C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p
+    lib.erq_version.restype = C.c_int
+    lib.erq_status_string.argtypes = [C.c_int]
+    lib.erq_status_string.restype = C.c_char_p
+    lib.erq_last_error.restype = C.c_char_p
+    lib.erq_index_load.argtypes = [C.c_char_p, C.c_int, C.POINTER(C.c_void_p)]
+    lib.erq_index_load.restype = C.c_int
+    lib.erq_index_get_info.argtypes = [vp, C.POINTER(IndexInfo)]
+    lib.erq_index_get_info.restype = C.c_int
+    lib.erq_index_free.argtypes = [vp]
+    lib.erq_index_free.restype = None
+    lib.erq_rotate.argtypes = [vp, f32p, u64, f32p, vp]
+    lib.erq_rotate.restype = C.c_int
+    lib.erq_search.argtypes = [vp, f32p, u64, u64, u64, u32p, f32p, vp]
+    lib.erq_search.restype = C.c_int
+    lib.erq_search_raw.argtypes = [vp, f32p, u64, u64, u64, u32p, f32p, vp]
+    lib.erq_search_raw.restype = C.c_int
+    lib.erq_debug_scan_capacity.argtypes = [vp, u64, u64]
+    lib.erq_debug_scan_capacity.restype = u64
+    lib.erq_debug_centroid_dists.argtypes = [vp, f32p, u64, f32p]
+    lib.erq_debug_centroid_dists.restype = C.c_int
+    lib.erq_debug_probe.argtypes = [vp, f32p, u64, u64, u32p, f32p]
+    lib.erq_debug_probe.restype = C.c_int
+    lib.erq_debug_scan.argtypes = [vp, f32p, u64, u64, u32p, f32p, f32p, f32p, vp, vp, u64]
+    lib.erq_debug_scan.restype = C.c_int
+    _lib = lib
+    return lib
+
+
+def check(status: int) -> None:
+    if status != ERQ_OK:
+        msg = load_library().erq_last_error().decode(errors="replace")
+        raise ErqError(status, msg)

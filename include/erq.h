@@ -1,0 +1,98 @@
+/* erq.h - C ABI of the B200 IVF search for Extended-RaBitQ indexes.
+ *
+ * The library (extended-rabitq_b200/lib/liberq.so) loads an index file written
+ * by the reference's IVF::save and answers IVF::search queries on one GPU.
+ * Every entry point takes plain pointers and sizes; pointers may be host or
+ * device memory (detected per pointer).  No entry point aborts: errors come
+ * back as erq_status codes with a message from erq_last_error().
+ *
+ * Reference interfaces replaced (paths relative to the reference project):
+ *   erq_index_load   <- IVF::load            inc/index/IVF.hpp:254-293
+ *   erq_index_get_info <- IVF::padded_dim / IVF::k and the header fields
+ *                                            inc/index/IVF.hpp:86-90,261-265
+ *   erq_rotate       <- Rotator::rotate       inc/index/Rotator.hpp:60-63, with the
+ *                       query padding of src/test_search.cpp:83-92
+ *   erq_search       <- IVF::search           inc/index/IVF.hpp:295-324
+ *   erq_search_raw   <- the rotate-then-search sequence of src/test_search.cpp:83-110
+ *   erq_index_free   <- IVF::~IVF             inc/index/IVF.hpp:106
+ */
+#ifndef ERQ_H
+#define ERQ_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ERQ_API_VERSION 1
+
+#if defined(__GNUC__)
+#define ERQ_API __attribute__((visibility("default")))
+#else
+#define ERQ_API
+#endif
+
+typedef enum erq_status {
+    ERQ_OK = 0,
+    ERQ_ERR_INVALID_ARGUMENT = 1, /* bad pointer, size, k, nprobe, ... */
+    ERQ_ERR_IO = 2,               /* index file cannot be opened or read */
+    ERQ_ERR_FORMAT = 3,           /* header or sizes inconsistent, file truncated */
+    ERQ_ERR_UNSUPPORTED = 4,      /* e.g. K >= 20000 (HNSW side file), D > 2048 */
+    ERQ_ERR_CUDA = 5,             /* a CUDA runtime call failed */
+    ERQ_ERR_OUT_OF_MEMORY = 6,    /* device or host allocation failed */
+    ERQ_ERR_TIMEOUT = 7           /* a bounded device-side wait gave up */
+} erq_status;
+
+typedef struct erq_index erq_index;
+
+typedef struct erq_index_info {
+    uint64_t n;            /* number of data vectors (N) */
+    uint64_t dim;          /* raw dimension (DIM) */
+    uint64_t padded_dim;   /* D = DIM rounded up to a multiple of 64 */
+    uint64_t num_clusters; /* K */
+    uint64_t ex_bits;      /* EX_BITS = total bits - 1, one of 2,3,4,6,7,8 */
+    uint64_t device_bytes; /* device memory held by the index */
+    int device;            /* CUDA device ordinal */
+} erq_index_info;
+
+/* Library version (ERQ_API_VERSION) and status text. */
+ERQ_API int erq_version(void);
+ERQ_API const char* erq_status_string(erq_status s);
+/* Message of the last failing call on this thread ("" if none). */
+ERQ_API const char* erq_last_error(void);
+
+/* Load an index file (the reference's IVF::save format, HIGH_ACC_FAST_SCAN
+ * layout) onto CUDA device `device`.  Rejects K >= 20000 (the reference then
+ * needs an HNSW side file) and D > 2048. */
+ERQ_API erq_status erq_index_load(const char* path, int device, erq_index** out);
+ERQ_API erq_status erq_index_get_info(const erq_index* index, erq_index_info* info);
+ERQ_API void erq_index_free(erq_index* index);
+
+/* rotated[nq][D] = pad(queries[nq][DIM]) * P, as test_search does before
+ * calling IVF::search.  `stream` is a cudaStream_t (NULL: default stream). */
+ERQ_API erq_status erq_rotate(const erq_index* index, const float* queries, uint64_t nq,
+                      float* rotated, void* stream);
+
+/* IVF::search for nq rotated queries (each D floats, row-major).
+ * ids[nq][k]: result ids in ascending estimated distance, exactly as the
+ *   reference's ResultPool::copy_results (unfilled slots are 0).
+ * dists[nq][k] (may be NULL): the pool's distance estimates; unfilled slots
+ *   are +inf.
+ * Requires 1 <= nprobe <= K and 1 <= k <= 1024.  The result equals the
+ * reference's on the same index and query bytes.  When any pointer is host
+ * memory the call returns after the results are in host memory; with device
+ * pointers only it is asynchronous on `stream`. */
+ERQ_API erq_status erq_search(const erq_index* index, const float* rotated_queries, uint64_t nq,
+                      uint64_t k, uint64_t nprobe, uint32_t* ids, float* dists, void* stream);
+
+/* Rotate then search: queries are raw DIM-float vectors. */
+ERQ_API erq_status erq_search_raw(const erq_index* index, const float* queries, uint64_t nq,
+                          uint64_t k, uint64_t nprobe, uint32_t* ids, float* dists,
+                          void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ERQ_H */

@@ -1,0 +1,47 @@
+/* erq_debug.h - per-stage entry points of liberq.so for parity testing.
+ *
+ * These run the same kernels as erq_search and copy the intermediate results
+ * of one stage back to host memory, so each stage can be compared with the
+ * reference on identical inputs.  All buffers are host memory; calls are
+ * synchronous on the default stream.
+ *
+ * Reference stages exposed:
+ *   erq_debug_centroid_dists <- L2Sqr16 over all centroids      inc/utils/space.hpp:18-39
+ *   erq_debug_probe    <- FlatInitializer::centroids_distances   inc/index/Initializer.hpp:55-68
+ *   erq_debug_scan     <- HASearcher::preparing + accumulate_one_block_high_acc's integer
+ *                         sums, per probed cluster             inc/index/HASearcher.hpp:121-185,
+ *                                                              inc/index/fastscan/FastScan.hpp:214-312
+ */
+#ifndef ERQ_DEBUG_H
+#define ERQ_DEBUG_H
+
+#include "erq.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Number of int32 entries erq_debug_scan may write for (nq, nprobe). */
+ERQ_API uint64_t erq_debug_scan_capacity(const erq_index* index, uint64_t nq, uint64_t nprobe);
+
+/* dist[nq][K]: squared distance of every rotated query to every centroid. */
+ERQ_API erq_status erq_debug_centroid_dists(const erq_index* index, const float* rotated_queries,
+                                    uint64_t nq, float* dist);
+
+/* cids/sqr_y[nq][nprobe]: probed clusters in ascending distance (ties by id). */
+ERQ_API erq_status erq_debug_probe(const erq_index* index, const float* rotated_queries, uint64_t nq,
+                           uint64_t nprobe, uint32_t* cids, float* sqr_y);
+
+/* For every (query q, probe rank p): cids, sqr_y, delta (query quantisation
+ * step) and sumq (sum of the normalised residual), each [nq][nprobe], and the
+ * exact integer sums <x_b, qq> of every vector of the probed cluster, 32 per
+ * FastScan block (padding lanes included), starting at S[s_offsets[q][p]].
+ * s_capacity must be at least erq_debug_scan_capacity(). */
+ERQ_API erq_status erq_debug_scan(const erq_index* index, const float* rotated_queries, uint64_t nq,
+                          uint64_t nprobe, uint32_t* cids, float* sqr_y, float* delta,
+                          float* sumq, uint64_t* s_offsets, int32_t* S, uint64_t s_capacity);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ERQ_DEBUG_H */
