@@ -28,6 +28,9 @@
 
 using namespace erq;
 
+// probe selection sorts all K centroid keys in shared memory (8 bytes each)
+constexpr uint64_t kMaxClusters = 16384;
+
 // ------------------------------------------------------------------ errors
 namespace {
 thread_local std::string g_last_error;
@@ -192,6 +195,9 @@ erq_status load_impl(const char* path, erq_index* idx) {
                     "K=%llu >= 20000: the reference keeps an HNSW coarse quantiser in a side file "
                     "for such indexes, which this library does not read",
                     (unsigned long long)idx->K);
+    if (idx->K > kMaxClusters)
+        return fail(ERQ_ERR_UNSUPPORTED, "K=%llu exceeds the %llu clusters the probe selection supports",
+                    (unsigned long long)idx->K, (unsigned long long)kMaxClusters);
     idx->D = (idx->DIM + 63) / 64 * 64;
     if (idx->D > (uint64_t)kMaxD)
         return fail(ERQ_ERR_UNSUPPORTED, "padded dimension %llu exceeds %d",
@@ -461,13 +467,17 @@ erq_status search_entry(const erq_index* idx, const float* queries, bool rotated
     const bool q_dev = is_device_ptr(queries);
     const bool ids_dev = is_device_ptr(ids);
     const bool d_dev = dists == nullptr || is_device_ptr(dists);
+    if ((ids_dev && (reinterpret_cast<uintptr_t>(ids) & 3)) ||
+        (dists && d_dev && (reinterpret_cast<uintptr_t>(dists) & 3)))
+        return fail(ERQ_ERR_INVALID_ARGUMENT, "ids/dists device buffers must be 4-byte aligned");
     Scratch s(st);
     const float* qin = queries;
-    if (!q_dev) {
+    // the kernels read queries as float4: device inputs off a 16-byte
+    // boundary are copied into aligned scratch first
+    if (!q_dev || (reinterpret_cast<uintptr_t>(queries) & 15)) {
         float* tmp = nullptr;
         ERQ_TRY(s.alloc(&tmp, nq * in_cols));
-        ERQ_CUDA(cudaMemcpyAsync(tmp, queries, nq * in_cols * sizeof(float),
-                                 cudaMemcpyHostToDevice, st));
+        ERQ_CUDA(cudaMemcpyAsync(tmp, queries, nq * in_cols * sizeof(float), cudaMemcpyDefault, st));
         qin = tmp;
     }
     const float* qrot = qin;

@@ -159,7 +159,11 @@ __global__ void __launch_bounds__(kScanWarps * 32) scan_kernel(ScanArgs a) {
         dst[0] = make_uint4(packed[0], packed[1], packed[2], packed[3]);
         dst[1] = make_uint4(packed[4], packed[5], packed[6], packed[7]);
     }
+    if (tid == 0) reinterpret_cast<uint32_t*>(red)[kScanWarps] = tables_s;
     __syncthreads();
+    // The lookups below are inline PTX; their addresses derive from this
+    // shared-memory read, which cannot move above the barrier.
+    const uint32_t tables_base = reinterpret_cast<volatile uint32_t*>(red)[kScanWarps];
 
     // 5. scan: warp w takes blocks w, w + kScanWarps, ...
     const uint32_t nb = a.c_nblocks[cid];
@@ -175,7 +179,7 @@ __global__ void __launch_bounds__(kScanWarps * 32) scan_kernel(ScanArgs a) {
 #pragma unroll 4
         for (int c = 0; c < nchunk; ++c) {
             const uint2 w = __ldg(src + c * 32);
-            const uint32_t base = tables_s + c * 512;
+            const uint32_t base = tables_base + c * 512;
             const uint32_t lo0 = ((w.x << 1) & 0x1E1E1E1Eu) | kconst;
             const uint32_t hi0 = ((w.x >> 3) & 0x1E1E1E1Eu) | kconst;
             lookup4<false>(lo0, hi0, base, acc_lo, acc_hi);
