@@ -1,0 +1,524 @@
+#!/usr/bin/env python3
+"""Benchmark of the B200 IVF search against the reference's CPU search.
+
+Metric: queries per second of IVF::search at the smallest nprobe whose
+recall@100 (against float64 brute force) reaches 0.95, on the 1M x 1536
+8-bit workload (K = 4096 clusters, 10,000 queries per step, top-100).
+
+One step = one pass of the whole query batch through rotation + coarse probe
++ FastScan scan + refinement + top-k.  `value` times steps whose raw queries
+are already in device memory; `e2e` times the same steps through the C ABI
+with pinned host buffers (host->device copy of the queries and
+device->host copy of ids and distances inside the timed region).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs one process per GPU (torchrun); each rank searches its own copy of
+the query batch against its own replica of the index (no data-path
+collective; weak scaling); time is the max over ranks.  `--impl reference`
+times the reference's own CPU search (built from its sources by
+oracle/Makefile) on this host's cores on samples of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(REPO, "extended-rabitq_b200")
+ORACLE_DIR = os.path.join(REPO, "oracle")
+for _p in (PKG, ORACLE_DIR):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+METRIC = "QPS @ recall@100≥0.95, 1M×1536 8-bit: learned-probe vs plain GPU vs ref CPU"
+
+CONFIGS = {
+    # the headline workload: openai1536-shaped synthetic data
+    "sphere1536-1M-8bit": dict(
+        gen="sphere", n=1_000_000, dim=1536, comps=4096, sigma=0.05, zipf=None, K=4096,
+        bits=8, nq=10_000, k=100, seed=20241, nprobe=None, recall_target=0.95,
+        data="synthetic: seeded 4096-component unit-sphere mixture, tangent sigma 0.05, "
+             "1M base + 10k queries, d=1536 (openai1536 stand-in)"),
+    # the small CPU-runnable case
+    "gauss128-100k-4bit": dict(
+        gen="gauss", n=100_000, dim=128, comps=256, sigma=0.3, zipf=None, K=1024,
+        bits=4, nq=1000, k=100, seed=11, nprobe=None, recall_target=0.95,
+        data="synthetic: seeded 256-component Gaussian mixture, sigma 0.3, 100k base + 1k "
+             "queries, d=128"),
+}
+DEFAULT_CONFIG = "sphere1536-1M-8bit"
+NPROBE_SWEEP = [1, 2, 3, 4, 5, 6, 8, 10, 12, 16, 20, 24, 32, 40, 48, 64, 80, 96, 128, 160,
+                192, 256, 320, 384, 512, 768, 1024]
+
+
+def log(*a):
+    print("[bench]", *a, file=sys.stderr, flush=True)
+
+
+# ------------------------------------------------------------------ data prep
+def cache_dir(name, cfg):
+    key = f"{name}-{cfg['n']}-{cfg['dim']}-{cfg['K']}-{cfg['bits']}-{cfg['nq']}-{cfg['seed']}"
+    return os.path.join(os.environ.get("ERQ_BENCH_CACHE", "/tmp/erq_bench"), key)
+
+
+def prepare(name, cfg, device="cuda"):
+    """Generate data, cluster, build the index file and the ground truth on
+    the GPU (torch plumbing; none of this is timed).  Cached on disk."""
+    d = cache_dir(name, cfg)
+    done = os.path.join(d, "done")
+    if os.path.exists(done):
+        return d
+    import torch
+
+    from erq_b200 import build_index, datasets, indexfile
+
+    os.makedirs(d, exist_ok=True)
+    t0 = time.time()
+    if cfg["gen"] == "sphere":
+        base, query = datasets.sphere_mixture_torch(cfg["n"], cfg["dim"], cfg["comps"],
+                                                    cfg["sigma"], cfg["seed"], cfg["nq"],
+                                                    cfg["zipf"], device=device)
+    else:
+        base, query = datasets.gaussian_mixture_torch(cfg["n"], cfg["dim"], cfg["comps"],
+                                                      cfg["sigma"], cfg["seed"], cfg["nq"],
+                                                      device=device)
+    log(f"generated {cfg['n']}x{cfg['dim']} in {time.time() - t0:.1f}s")
+    cent, ids = datasets.kmeans_torch(base, cfg["K"], iters=20, seed=cfg["seed"] + 1)
+    log(f"k-means K={cfg['K']} done at {time.time() - t0:.1f}s")
+    arr = build_index.build_index_torch(base, cent, ids, cfg["bits"], seed=cfg["seed"] + 2)
+    indexfile.write_index(os.path.join(d, "ivf.index"), arr)
+    del arr
+    log(f"index built at {time.time() - t0:.1f}s")
+    gt, gtd = datasets.ground_truth_torch(base, query, cfg["k"])
+    np.save(os.path.join(d, "query.npy"), query.cpu().numpy())
+    np.save(os.path.join(d, "gt.npy"), gt.cpu().numpy().astype(np.uint32))
+    np.save(os.path.join(d, "gt_dist.npy"), gtd.cpu().numpy())
+    # a slice of the base for the distance-ratio metric on a query subset
+    np.save(os.path.join(d, "base.npy"), base.cpu().numpy())
+    log(f"ground truth done at {time.time() - t0:.1f}s")
+    del base, query, cent, ids, gt, gtd
+    torch.cuda.empty_cache()
+    open(done, "w").write("ok\n")
+    return d
+
+
+# ------------------------------------------------------------------ clocks
+CLOCK_FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+
+class ClockSampler:
+    def __init__(self, gpu_index: int):
+        self.proc = None
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={CLOCK_FIELDS}", "--format=csv,noheader,nounits",
+                 "-i", str(gpu_index), "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        out, _ = self.proc.communicate(timeout=10)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# --------------------------------------------------------------- CPU baselines
+def cpu_has_avx512() -> bool:
+    try:
+        flags = open("/proc/cpuinfo").read()
+    except OSError:
+        return False
+    return all(f in flags for f in ("avx512f", "avx512bw", "avx512vl", "avx512dq", "avx512cd"))
+
+
+def cpu_searcher(index_path):
+    """The reference's own search (stock flags) when it is built and the host
+    has AVX-512, else the C restatement.  Returns (searcher, kind, note)."""
+    import oracle
+
+    if oracle.reference_available(stock=True) and cpu_has_avx512():
+        return oracle.Reference(index_path, stock=True), "reference", ""
+    note = ("reference build missing" if not oracle.reference_available(stock=True)
+            else "host lacks AVX-512; reference cannot run")
+    oracle.build_oracle()
+    return oracle.Oracle(index_path), "port", note
+
+
+def time_cpu(searcher, kind, query_raw, k, nprobe, threads, budget_s, max_n):
+    """Time searcher on a bounded sample: queries whose measured cost fits
+    budget_s.  Returns (qps, n, seconds, rotate_s, search_s)."""
+    if kind == "reference":
+        rotate = searcher.rotate
+    else:
+        P = searcher.rotation()
+        D = P.shape[0]
+
+        def rotate(q):
+            pad = np.zeros((q.shape[0], D), np.float32)
+            pad[:, :q.shape[1]] = q
+            return pad @ P
+    probe_n = min(max_n, max(threads * 4, 32))
+    q = query_raw[:probe_n]
+    t0 = time.perf_counter()
+    qr = rotate(q)
+    searcher.search(qr, k, nprobe, nthreads=threads)
+    per_q = (time.perf_counter() - t0) / probe_n
+    n = int(min(max_n, max(probe_n, budget_s / max(per_q, 1e-9))))
+    q = query_raw[:n]
+    t0 = time.perf_counter()
+    qr = rotate(q)
+    t1 = time.perf_counter()
+    searcher.search(qr, k, nprobe, nthreads=threads)
+    t2 = time.perf_counter()
+    return n / (t2 - t0), n, t2 - t0, t1 - t0, t2 - t1
+
+
+# ------------------------------------------------------------------ helpers
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def choose_nprobe(idx, qraw, gt, cfg):
+    """Smallest nprobe of the sweep reaching the recall target (all queries)."""
+    from erq_b200 import metrics
+
+    k = cfg["k"]
+    sweep = [p for p in NPROBE_SWEEP if p <= cfg["K"]]
+    if cfg.get("nprobe"):
+        sweep = [cfg["nprobe"]] + [p for p in sweep if p > cfg["nprobe"]]
+    best = None
+    for p in sweep:
+        ids, _ = idx.search_raw(qraw, k, p, with_dists=False)
+        r = metrics.recall_at_k(ids.view(np.uint32) if ids.dtype != np.uint32 else ids, gt, k)
+        log(f"nprobe={p}: recall@{k}={r:.4f}")
+        best = (p, r, ids)
+        if r >= cfg["recall_target"]:
+            break
+    return best
+
+
+def run_e2e(idx, query, k, nprobe, ids0, stream, args, world):
+    """The same steps through the C ABI with pinned host buffers: the H2D
+    copy of the raw queries and the D2H copy of ids + distances are inside
+    the timed region (the call returns when the results are on the host)."""
+    import torch
+
+    nq = query.shape[0]
+    qh = torch.from_numpy(query).pin_memory()
+    ids_h = torch.empty((nq, k), dtype=torch.int32).pin_memory()
+    dist_h = torch.empty((nq, k), dtype=torch.float32).pin_memory()
+
+    def step_host():
+        idx.search_raw(qh, k, nprobe, ids=ids_h, dists=dist_h, stream=stream)
+
+    for _ in range(args.warmup):
+        step_host()
+    barrier(world)
+    torch.cuda.synchronize()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(args.steps):
+        step_host()
+    f1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    e2e_ms = max_over_ranks(f0.elapsed_time(f1), world)
+    assert (ids_h.numpy().view(np.uint32) == ids0).all()
+    return {"value": round(world * nq * args.steps / (e2e_ms / 1e3), 1), "unit": "queries/s",
+            "h2d_bytes_per_step": int(nq * query.shape[1] * 4),
+            "d2h_bytes_per_step": int(nq * k * 8)}
+
+
+# ------------------------------------------------------------------ our arm
+def run_ours(args, cfg, name):
+    import torch
+
+    from erq_b200 import IVF, indexfile, metrics
+    from erq_b200 import _lib as L
+
+    world, rank, local = dist_setup(args)
+    torch.cuda.set_device(local)
+    if rank == 0:
+        d = prepare(name, cfg)
+    barrier(world)
+    d = prepare(name, cfg) if rank != 0 else d
+    index_path = os.path.join(d, "ivf.index")
+    query = np.load(os.path.join(d, "query.npy"))
+    gt = np.load(os.path.join(d, "gt.npy"))
+    if args.queries:
+        query, gt = query[:args.queries], gt[:args.queries]
+    nq, k = query.shape[0], cfg["k"]
+
+    idx = IVF(index_path, device=local)
+    if args.nprobe:
+        cfg = dict(cfg, nprobe=args.nprobe)
+    nprobe, recall, ids0 = choose_nprobe(idx, query, gt, cfg)
+    # distance ratio on the first 1000 queries (get_ratio, inc/utils/tools.hpp:16-51)
+    base = np.load(os.path.join(d, "base.npy"), mmap_mode="r")
+    sub = min(1000, nq)
+    ratio = metrics.average_distance_ratio(query[:sub], base, ids0[:sub].astype(np.int64),
+                                           gt[:sub].astype(np.int64), k)
+    # algorithmic bytes of the scan kernel: every probed block's codes read
+    # and its 32 int32 sums written, (4D + 128) bytes per block
+    arr = indexfile.read_index(index_path)
+    nblocks = (arr.sizes.astype(np.int64) + 31) // 32
+    qrot = idx.rotate(query)
+    cids, _ = idx.debug_probe(qrot, nprobe)
+    scan_bytes_per_step = int(nblocks[cids.astype(np.int64)].sum()) * (4 * arr.D + 128)
+    del arr, qrot
+
+    stream = torch.cuda.current_stream()
+    qd = torch.from_numpy(query).cuda()
+    ids_d = torch.empty((nq, k), dtype=torch.int32, device="cuda")
+    dist_d = torch.empty((nq, k), dtype=torch.float32, device="cuda")
+
+    def step_device():
+        idx.search_raw(qd, k, nprobe, ids=ids_d, dists=dist_d, stream=stream)
+
+    for _ in range(args.warmup):
+        step_device()
+    torch.cuda.synchronize()
+    # device results equal the host-path results used for recall
+    assert (ids_d.cpu().numpy().view(np.uint32) == ids0).all()
+    barrier(world)
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    L.profile_reset()
+    L.profile_enable(True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step_device()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    L.profile_enable(False)
+    barrier(world)
+    clocks = sampler.stop()
+    ms = max_over_ranks(e0.elapsed_time(e1), world)
+    prof = L.profile_read()
+    value = world * nq * args.steps / (ms / 1e3)
+
+    e2e_block = None
+    if not args.no_e2e:
+        e2e_block = run_e2e(idx, query, k, nprobe, ids0, stream, args, world)
+
+    scan_n, scan_ms = prof["scan"]
+    launches = sum(v[0] for v in prof.values())
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(REPO, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    peak = peaks.get("hbm_gbs")
+    peak_src = "measured" if peak else "fallback"
+    peak = peak or 6650.0
+    achieved = None
+    if scan_n:
+        per_launch_bytes = scan_bytes_per_step * args.steps / scan_n
+        achieved = per_launch_bytes / (scan_ms / scan_n / 1e3) / 1e9
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        searcher, kind, note = cpu_searcher(index_path)
+        threads = os.cpu_count() or 1
+        qps, n, sec, rot_s, srch_s = time_cpu(searcher, kind, query, k, nprobe, threads,
+                                              args.cpu_budget, nq)
+        cpu = {"value": round(qps, 2), "unit": "queries/s", "cores": threads, "kind": kind,
+               "sample": f"first {n} of the {nq} queries at nprobe={nprobe}, "
+                         f"{threads} threads, {sec:.1f}s (rotate {rot_s:.2f}s + search "
+                         f"{srch_s:.2f}s)" + (f"; {note}" if note else "")}
+        searcher.close()
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": round(value, 1), "unit": "queries/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(ms / args.steps, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+            "data": cfg["data"],
+            "config": {"workload": f"{name}: plain fixed-nprobe GPU search, "
+                                   f"{cfg['n']}x{cfg['dim']}, K={cfg['K']}, {cfg['bits']}-bit, "
+                                   f"{nq} queries per step, top-{k}",
+                       "nprobe": nprobe, "recall@100": round(recall, 5),
+                       "distance_ratio": round(ratio, 5), "queries_per_step": nq,
+                       "parallelism": f"replicas x{world} (queries replicated per GPU)",
+                       "l2": "inputs larger than L2: every step streams "
+                             f"{scan_bytes_per_step / 1e9:.1f} GB of packed codes from a "
+                             f"{os.path.getsize(index_path) / 1e9:.2f} GB index"},
+            "e2e": e2e_block,
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1) if achieved else None,
+                         "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4) if achieved else None,
+                         "traffic": None, "kernel": "scan_kernel",
+                         "peak_source": f"{peak_src} hbm_gbs (copy)"},
+            "kernels_ms_per_step": {kk: round(v[1] / args.steps, 4) for kk, v in prof.items()},
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+        }
+        print(json.dumps(out), flush=True)
+    idx.free()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+# ------------------------------------------------------------ reference arm
+def run_reference(args, cfg, name):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    d = prepare(name, cfg)
+    index_path = os.path.join(d, "ivf.index")
+    query = np.load(os.path.join(d, "query.npy"))
+    k, nq = cfg["k"], query.shape[0]
+    searcher, kind, note = cpu_searcher(index_path)
+    threads = os.cpu_count() or 1
+    nprobe = cfg.get("nprobe")
+    if not nprobe:
+        # the recall-driven nprobe, found with the reference itself on a sample
+        from erq_b200 import metrics
+
+        gt = np.load(os.path.join(d, "gt.npy"))
+        sub = min(500, nq)
+        nprobe = NPROBE_SWEEP[-1]
+        for p in NPROBE_SWEEP:
+            if p > cfg["K"]:
+                break
+            if kind == "reference":
+                qr = searcher.rotate(query[:sub])
+                ids = searcher.search(qr, k, p, nthreads=threads)
+            else:
+                P = searcher.rotation()
+                pad = np.zeros((sub, P.shape[0]), np.float32)
+                pad[:, :query.shape[1]] = query[:sub]
+                ids, _ = searcher.search(pad @ P, k, p, nthreads=threads)
+            r = metrics.recall_at_k(ids, gt[:sub], k)
+            log(f"reference nprobe={p}: recall@{k}={r:.4f} (first {sub} queries)")
+            if r >= cfg["recall_target"]:
+                nprobe = p
+                break
+    per_step = []
+    samples = []
+    offset = 0
+    for s in range(args.warmup + args.steps):
+        qs = np.roll(query, -offset, axis=0)
+        qps, n, sec, _, _ = time_cpu(searcher, kind, qs, k, nprobe, threads, args.ref_step_s, nq)
+        offset = (offset + n) % nq
+        if s >= args.warmup:
+            per_step.append(sec)
+            samples.append(n)
+    total_q, total_s = sum(samples), sum(per_step)
+    value = total_q / total_s
+    out = {
+        "metric": METRIC, "impl": "reference", "value": round(value, 2), "unit": "queries/s",
+        "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(1e3 * total_s / args.steps, 2),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "data": cfg["data"],
+        "config": {"workload": f"{name}: the reference's IVF::search (AVX-512 CPU) on samples "
+                               f"of the {nq}-query batch, top-{k}", "nprobe": nprobe},
+        "cpu_baseline": {"value": round(value, 2), "unit": "queries/s", "cores": threads,
+                         "kind": kind,
+                         "sample": f"{args.steps} steps of ~{args.ref_step_s:.0f}s each, "
+                                   f"{total_q} queries total at nprobe={nprobe} incl. the "
+                                   "reference's own query rotation" + (f"; {note}" if note else "")},
+        "e2e": {"value": round(value, 2), "unit": "queries/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    searcher.close()
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--config", choices=sorted(CONFIGS), default=DEFAULT_CONFIG)
+    ap.add_argument("--cpu-budget", type=float, default=15.0,
+                    help="seconds of CPU search for the cpu_baseline sample")
+    ap.add_argument("--ref-step-s", type=float, default=6.0,
+                    help="seconds of CPU search per step of the reference arm")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer e2e timing")
+    ap.add_argument("--queries", type=int, default=0,
+                    help="use only the first N queries of the batch (profiling cases)")
+    ap.add_argument("--nprobe", type=int, default=0,
+                    help="start the recall sweep at this nprobe")
+    ap.add_argument("--prep-only", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and not args.prep_only:
+        log("warm-up raised to the minimum of 3 steps")
+        args.warmup = 3
+    cfg = CONFIGS[args.config]
+    if args.prep_only:
+        print(prepare(args.config, cfg))
+        return
+    if args.impl == "reference":
+        run_reference(args, cfg, args.config)
+    else:
+        run_ours(args, cfg, args.config)
+
+
+if __name__ == "__main__":
+    main()

@@ -16,6 +16,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -84,16 +85,18 @@ bool is_device_ptr(const void* p) {
     return attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged;
 }
 
-// Stream-ordered scratch allocations released on scope exit.
+// Stream-ordered scratch allocations (from the index's memory pool) released
+// on scope exit.
 struct Scratch {
     cudaStream_t stream;
+    cudaMemPool_t pool;
     std::vector<void*> ptrs;
-    explicit Scratch(cudaStream_t s) : stream(s) {}
+    Scratch(cudaStream_t s, cudaMemPool_t p) : stream(s), pool(p) {}
     template <typename T>
     erq_status alloc(T** out, size_t count) {
         void* p = nullptr;
         const size_t bytes = std::max<size_t>(count * sizeof(T), 16);
-        cudaError_t e = cudaMallocAsync(&p, bytes, stream);
+        cudaError_t e = cudaMallocFromPoolAsync(&p, bytes, pool, stream);
         if (e != cudaSuccess)
             return fail(e == cudaErrorMemoryAllocation ? ERQ_ERR_OUT_OF_MEMORY : ERQ_ERR_CUDA,
                         "cudaMallocAsync(%zu bytes) failed: %s", bytes, cudaGetErrorString(e));
@@ -103,6 +106,60 @@ struct Scratch {
     }
     ~Scratch() {
         for (void* p : ptrs) cudaFreeAsync(p, stream);
+    }
+};
+
+// ----------------------------------------------------------------- profiler
+// Event pairs around kernel launches, resolved lazily by erq_profile_read.
+enum KernelId { kRotate = 0, kCentroidDist, kSelectProbe, kScan, kRefine, kNumKernels };
+const char* const kKernelNames[kNumKernels] = {"rotate", "centroid_dist", "select_probe", "scan",
+                                               "refine"};
+
+struct Profiler {
+    std::mutex mu;
+    bool on = false;
+    struct Rec {
+        int kernel;
+        int device;
+        cudaEvent_t start, stop;
+    };
+    std::vector<Rec> pending;
+    uint64_t launches[kNumKernels] = {};
+    double ms[kNumKernels] = {};
+};
+Profiler& profiler() {
+    static Profiler p;
+    return p;
+}
+
+// Records the start event on construction and the stop event on finish().
+struct LaunchTimer {
+    int kernel;
+    cudaStream_t stream;
+    cudaEvent_t start = nullptr, stop = nullptr;
+    bool active = false;
+    LaunchTimer(int k, cudaStream_t s) : kernel(k), stream(s) {
+        Profiler& p = profiler();
+        {
+            std::lock_guard<std::mutex> g(p.mu);
+            active = p.on;
+        }
+        if (!active) return;
+        if (cudaEventCreate(&start) != cudaSuccess || cudaEventCreate(&stop) != cudaSuccess) {
+            active = false;
+            return;
+        }
+        cudaEventRecord(start, stream);
+    }
+    void finish() {
+        if (!active) return;
+        cudaEventRecord(stop, stream);
+        int dev = 0;
+        cudaGetDevice(&dev);
+        Profiler& p = profiler();
+        std::lock_guard<std::mutex> g(p.mu);
+        p.pending.push_back({kernel, dev, start, stop});
+        active = false;
     }
 };
 
@@ -128,11 +185,17 @@ struct erq_index {
     uint32_t* c_first_vec = nullptr;
     uint32_t* c_size = nullptr;
     uint32_t* c_nblocks = nullptr;
+    // per-call scratch pool; keeps freed blocks for reuse by later calls
+    cudaMemPool_t pool = nullptr;
 
     ~erq_index() {
         int prev = -1;
         cudaGetDevice(&prev);
         cudaSetDevice(device);
+        if (pool) {
+            cudaDeviceSynchronize();
+            cudaMemPoolDestroy(pool);
+        }
         for (void* p : {(void*)P, (void*)centroids, (void*)codes, (void*)onorm, (void*)excode,
                         (void*)xipnorm, (void*)ids, (void*)c_first_block, (void*)c_first_vec,
                         (void*)c_size, (void*)c_nblocks})
@@ -271,6 +334,13 @@ erq_status load_impl(const char* path, erq_index* idx) {
     ERQ_CUDA(cudaMemcpy(idx->c_first_vec, first_vec.data(), K * 4, cudaMemcpyHostToDevice));
     ERQ_CUDA(cudaMemcpy(idx->c_size, csize.data(), K * 4, cudaMemcpyHostToDevice));
     ERQ_CUDA(cudaMemcpy(idx->c_nblocks, idx->h_nblocks.data(), K * 4, cudaMemcpyHostToDevice));
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = idx->device;
+    ERQ_CUDA(cudaMemPoolCreate(&idx->pool, &props));
+    uint64_t keep = ~0ull;
+    ERQ_CUDA(cudaMemPoolSetAttribute(idx->pool, cudaMemPoolAttrReleaseThreshold, &keep));
     return ERQ_OK;
 }
 
@@ -278,7 +348,7 @@ erq_status load_impl(const char* path, erq_index* idx) {
 size_t scan_smem_bytes(int D) { return 256 + (size_t)(D / 64) * 512 + (size_t)D * 4 + 64; }
 size_t refine_smem_bytes(int D, int k) {
     const int kpad = (k + 31) & ~31;
-    return (size_t)kRefineWarps * ((size_t)D + 2 * kpad) * 4;
+    return (size_t)kRefineWarps * refine_warp_smem_bytes(D, kpad);
 }
 int next_pow2(int x) {
     int p = 1;
@@ -339,14 +409,18 @@ erq_status alloc_batch(Scratch& s, const erq_index* idx, uint64_t nq, uint64_t n
 erq_status launch_probe(const erq_index* idx, const Batch& b, uint64_t nprobe, cudaStream_t st) {
     const int D = (int)idx->D, K = (int)idx->K;
     dim3 g1((unsigned)div_up(K, kCdTC), (unsigned)div_up(b.nq, kCdTQ));
+    LaunchTimer t1(kCentroidDist, st);
     centroid_dist_kernel<<<g1, 256, 0, st>>>(b.qrot, (int)b.nq, idx->centroids, K, D, b.dist);
+    t1.finish();
     ERQ_CUDA(cudaGetLastError());
     const int kp2 = next_pow2(K);
     const int thr = std::min(1024, std::max(128, kp2 / 8));
     const uint64_t stride = 32ull * idx->top_blocks[nprobe];
+    LaunchTimer t2(kSelectProbe, st);
     select_probe_kernel<<<(unsigned)b.nq, thr, (size_t)kp2 * 8, st>>>(
         b.dist, (int)b.nq, K, kp2, (int)nprobe, idx->c_nblocks, stride, b.probe_cid, b.probe_sqy,
         b.s_off);
+    t2.finish();
     ERQ_CUDA(cudaGetLastError());
     return ERQ_OK;
 }
@@ -368,7 +442,9 @@ erq_status launch_scan(const erq_index* idx, const Batch& b, uint64_t nprobe, cu
     a.nprobe = (int)nprobe;
     const uint64_t pairs = b.nq * nprobe;
     if (pairs > 0x7fffffffull) return fail(ERQ_ERR_INVALID_ARGUMENT, "too many (query, probe) pairs");
+    LaunchTimer t(kScan, st);
     scan_kernel<<<(unsigned)pairs, kScanWarps * 32, scan_smem_bytes(a.D), st>>>(a);
+    t.finish();
     ERQ_CUDA(cudaGetLastError());
     return ERQ_OK;
 }
@@ -400,6 +476,7 @@ erq_status launch_refine(const erq_index* idx, const Batch& b, uint64_t nprobe, 
     a.k = (int)k;
     const unsigned grid = (unsigned)div_up(b.nq, kRefineWarps);
     const size_t smem = refine_smem_bytes(a.D, a.k);
+    LaunchTimer t(kRefine, st);
     switch (idx->EX) {
         case 2: refine_kernel<2><<<grid, kRefineWarps * 32, smem, st>>>(a); break;
         case 3: refine_kernel<3><<<grid, kRefineWarps * 32, smem, st>>>(a); break;
@@ -409,6 +486,7 @@ erq_status launch_refine(const erq_index* idx, const Batch& b, uint64_t nprobe, 
         case 8: refine_kernel<8><<<grid, kRefineWarps * 32, smem, st>>>(a); break;
         default: return fail(ERQ_ERR_FORMAT, "bad EX");
     }
+    t.finish();
     ERQ_CUDA(cudaGetLastError());
     return ERQ_OK;
 }
@@ -432,7 +510,7 @@ erq_status search_device(const erq_index* idx, const float* qrot_dev, uint64_t n
                          uint64_t nprobe, uint32_t* ids_dev, float* dists_dev, cudaStream_t st) {
     ERQ_TRY(configure_kernels((int)idx->D, (int)idx->K, (int)k));
     const uint64_t bq = batch_queries(idx, nprobe, nq);
-    Scratch s(st);
+    Scratch s(st, idx->pool);
     Batch b;
     ERQ_TRY(alloc_batch(s, idx, bq, nprobe, b));
     for (uint64_t q0 = 0; q0 < nq; q0 += bq) {
@@ -450,7 +528,9 @@ erq_status rotate_device(const erq_index* idx, const float* q_dev, uint64_t nq, 
                          cudaStream_t st) {
     if (nq == 0) return ERQ_OK;
     dim3 grid((unsigned)div_up(idx->D, kRotBN), (unsigned)div_up(nq, kRotBM));
+    LaunchTimer t(kRotate, st);
     rotate_kernel<<<grid, 256, 0, st>>>(q_dev, (int)nq, (int)idx->DIM, idx->P, (int)idx->D, out_dev);
+    t.finish();
     ERQ_CUDA(cudaGetLastError());
     return ERQ_OK;
 }
@@ -470,7 +550,7 @@ erq_status search_entry(const erq_index* idx, const float* queries, bool rotated
     if ((ids_dev && (reinterpret_cast<uintptr_t>(ids) & 3)) ||
         (dists && d_dev && (reinterpret_cast<uintptr_t>(dists) & 3)))
         return fail(ERQ_ERR_INVALID_ARGUMENT, "ids/dists device buffers must be 4-byte aligned");
-    Scratch s(st);
+    Scratch s(st, idx->pool);
     const float* qin = queries;
     // the kernels read queries as float4: device inputs off a 16-byte
     // boundary are copied into aligned scratch first
@@ -567,7 +647,7 @@ erq_status erq_rotate(const erq_index* idx, const float* queries, uint64_t nq, f
     ERQ_TRY(guard.set(idx->device));
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const bool q_dev = is_device_ptr(queries), o_dev = is_device_ptr(rotated);
-    Scratch s(st);
+    Scratch s(st, idx->pool);
     const float* qin = queries;
     float* out = rotated;
     if (!q_dev) {
@@ -607,7 +687,7 @@ erq_status erq_debug_probe(const erq_index* idx, const float* qrot, uint64_t nq,
     ERQ_TRY(guard.set(idx->device));
     ERQ_TRY(configure_kernels((int)idx->D, (int)idx->K, 1));
     cudaStream_t st = 0;
-    Scratch s(st);
+    Scratch s(st, idx->pool);
     float* q = nullptr;
     ERQ_TRY(s.alloc(&q, nq * idx->D));
     ERQ_CUDA(cudaMemcpyAsync(q, qrot, nq * idx->D * 4, cudaMemcpyHostToDevice, st));
@@ -628,7 +708,7 @@ erq_status erq_debug_centroid_dists(const erq_index* idx, const float* qrot, uin
     DeviceGuard guard;
     ERQ_TRY(guard.set(idx->device));
     cudaStream_t st = 0;
-    Scratch s(st);
+    Scratch s(st, idx->pool);
     float* q = nullptr;
     float* d = nullptr;
     ERQ_TRY(s.alloc(&q, nq * idx->D));
@@ -662,7 +742,7 @@ erq_status erq_debug_scan(const erq_index* idx, const float* qrot, uint64_t nq, 
     ERQ_TRY(guard.set(idx->device));
     ERQ_TRY(configure_kernels((int)idx->D, (int)idx->K, 1));
     cudaStream_t st = 0;
-    Scratch s(st);
+    Scratch s(st, idx->pool);
     float* q = nullptr;
     ERQ_TRY(s.alloc(&q, nq * idx->D));
     ERQ_CUDA(cudaMemcpyAsync(q, qrot, nq * idx->D * 4, cudaMemcpyHostToDevice, st));
@@ -680,6 +760,50 @@ erq_status erq_debug_scan(const erq_index* idx, const float* qrot, uint64_t nq, 
     ERQ_CUDA(cudaMemcpyAsync(s_offsets, b.s_off, np * 8, cudaMemcpyDeviceToHost, st));
     ERQ_CUDA(cudaMemcpyAsync(S, b.S, need * 4, cudaMemcpyDeviceToHost, st));
     ERQ_CUDA(cudaStreamSynchronize(st));
+    return ERQ_OK;
+}
+
+void erq_profile_enable(int on) {
+    Profiler& p = profiler();
+    std::lock_guard<std::mutex> g(p.mu);
+    p.on = on != 0;
+}
+
+void erq_profile_reset(void) {
+    Profiler& p = profiler();
+    std::lock_guard<std::mutex> g(p.mu);
+    for (auto& r : p.pending) {
+        cudaEventSynchronize(r.stop);
+        cudaEventDestroy(r.start);
+        cudaEventDestroy(r.stop);
+    }
+    p.pending.clear();
+    for (int i = 0; i < kNumKernels; ++i) {
+        p.launches[i] = 0;
+        p.ms[i] = 0.0;
+    }
+}
+
+erq_status erq_profile_read(const char* kernel, uint64_t* launches, double* total_ms) {
+    if (!kernel || !launches || !total_ms) return fail(ERQ_ERR_INVALID_ARGUMENT, "NULL argument");
+    int id = -1;
+    for (int i = 0; i < kNumKernels; ++i)
+        if (strcmp(kernel, kKernelNames[i]) == 0) id = i;
+    if (id < 0) return fail(ERQ_ERR_INVALID_ARGUMENT, "unknown kernel '%s'", kernel);
+    Profiler& p = profiler();
+    std::lock_guard<std::mutex> g(p.mu);
+    for (auto& r : p.pending) {
+        ERQ_CUDA(cudaEventSynchronize(r.stop));
+        float ms = 0.f;
+        ERQ_CUDA(cudaEventElapsedTime(&ms, r.start, r.stop));
+        p.launches[r.kernel] += 1;
+        p.ms[r.kernel] += ms;
+        cudaEventDestroy(r.start);
+        cudaEventDestroy(r.stop);
+    }
+    p.pending.clear();
+    *launches = p.launches[id];
+    *total_ms = p.ms[id];
     return ERQ_OK;
 }
 

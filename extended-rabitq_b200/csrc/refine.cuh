@@ -44,60 +44,140 @@ struct RefineArgs {
 };
 
 constexpr int kRefineWarps = 4;
+constexpr int kChunkBlocks = 4;  // blocks whose candidates are refined together
 
-// Value of dim 16*s + l of one EX-bit code (store_compacted_code layouts,
-// inc/index/Quantizer.hpp:491-631).
+// float(v) for 0 <= v < 256 held in byte `i` of `w`: 0x4B0000vv is 2^23 + v.
+__device__ __forceinline__ float byte_to_float(uint32_t w, int i) {
+    return __fsub_rn(__int_as_float((int)__byte_perm(w, 0x4B000000u, 0x7540u | (uint32_t)i)),
+                     8388608.f);
+}
+
+// Four consecutive dims (16*sub + 4*qd .. +3 of a 64-dim group) of one EX-bit
+// code as bytes of a word.  `w` holds the group's 8*EX bytes as 2*EX words.
+// Layouts: store_compacted_code, inc/index/Quantizer.hpp:491-631.
 template <int EX>
-__device__ __forceinline__ uint32_t ex_value(const uint8_t* __restrict__ code, int s, int l) {
+__device__ __forceinline__ uint32_t ex_quad(const uint32_t* w, int sub, int qd) {
     if (EX == 8) {
-        return code[16 * s + l];
-    } else if (EX == 4) {
-        return (code[16 * (s >> 1) + l] >> (4 * (s & 1))) & 15u;
-    } else if (EX == 2 || EX == 3) {
-        constexpr int seg = (EX == 2) ? 16 : 24;
-        const uint8_t* c = code + seg * (s >> 2);
-        const int sub = s & 3;
-        uint32_t v = (c[l] >> (2 * sub)) & 3u;
+        return w[4 * sub + qd];
+    } else if (EX == 4) {  // per 32 dims: 16 bytes, low nibble = dims 0-15
+        const uint32_t c = w[4 * (sub >> 1) + qd];
+        return (sub & 1) ? ((c >> 4) & 0x0F0F0F0Fu) : (c & 0x0F0F0F0Fu);
+    } else if (EX == 2 || EX == 3) {  // 2 bits at 2*sub of bytes 0-15
+        uint32_t v = (w[qd] >> (2 * sub)) & 0x03030303u;
         if (EX == 3) {
-            const int d = 16 * sub + l;  // dim within the 64-dim group
-            const uint8_t tb = c[16 + (d & 7)];  // byte m = d % 8 of the top-bit word
-            v |= ((tb >> (d >> 3)) & 1u) << 2;
+            // bit j of byte m of the top word = bit 2 of dim 8j + m; these
+            // dims have m = (4qd .. 4qd+3) % 8 and j = 2*sub + qd/2
+            const uint32_t t = w[4 + (qd & 1)];
+            const int j = 2 * sub + (qd >> 1);
+            v |= ((j <= 2) ? (t << (2 - j)) : (t >> (j - 2))) & 0x04040404u;
         }
         return v;
-    } else {  // EX == 6 || EX == 7
-        constexpr int seg = (EX == 6) ? 48 : 56;
-        const uint8_t* c = code + seg * (s >> 2);
-        const int sub = s & 3;
+    } else {  // EX == 6 || EX == 7: c1 = bytes 0-15, c2 = 16-31, c3 = 32-47
+        const uint32_t c1 = w[qd], c2 = w[4 + qd], c3 = w[8 + qd];
         uint32_t v;
         if (sub == 0) {
-            v = c[l] & 63u;
+            v = c1 & 0x3F3F3F3Fu;
         } else if (sub == 1) {
-            v = c[16 + l] & 63u;
+            v = c2 & 0x3F3F3F3Fu;
         } else if (sub == 2) {
-            v = ((uint32_t)(c[l] >> 6) << 4) | (c[32 + l] & 15u);
+            v = ((c1 >> 2) & 0x30303030u) | (c3 & 0x0F0F0F0Fu);
         } else {
-            v = ((uint32_t)(c[16 + l] >> 6) << 4) | (c[32 + l] >> 4);
+            v = ((c2 >> 2) & 0x30303030u) | ((c3 >> 4) & 0x0F0F0F0Fu);
         }
-        if (EX == 7) {
-            const int d = 16 * sub + l;
-            const uint8_t tb = c[48 + (d & 7)];
-            v |= ((tb >> (d >> 3)) & 1u) << 6;
+        if (EX == 7) {  // bit 6 from the top word (after 48 bytes)
+            const uint32_t t = w[12 + (qd & 1)];
+            const int j = 2 * sub + (qd >> 1);
+            v |= ((j <= 6) ? (t << (6 - j)) : (t >> (j - 6))) & 0x40404040u;
         }
         return v;
     }
 }
 
-// <unit_q, ex code>: lane l of the 16-lane segment accumulates
-// fma(unit_q[16s+l], code[16s+l], acc) in ascending s; result in lane 0.
+// <unit_q, ex code> computed by one thread in the reference's order:
+// accumulator l takes fma(unit_q[16s+l], code[16s+l], acc[l]) for s = 0,1,...
+// then the reduce tree (IP*_fxu* in inc/utils/space.hpp).  unit_q is in
+// shared memory and read as broadcasts (all lanes walk the same dims).
 template <int EX>
-__device__ __forceinline__ float ex_ip(const float* __restrict__ unit_q,
-                                       const uint8_t* __restrict__ code, int D, int l) {
-    float acc = 0.f;
-    const int nsteps = D >> 4;
-#pragma unroll 8
-    for (int s = 0; s < nsteps; ++s)
-        acc = __fmaf_rn(unit_q[16 * s + l], (float)ex_value<EX>(code, s, l), acc);
-    return tree16_sum(acc);
+__device__ __forceinline__ float ex_ip_thread(const float* __restrict__ uq,
+                                              const uint8_t* __restrict__ code, int D) {
+    float acc[16];
+#pragma unroll
+    for (int l = 0; l < 16; ++l) acc[l] = 0.f;
+    const uint2* src = reinterpret_cast<const uint2*>(code);
+    for (int t = 0; t < (D >> 6); ++t) {
+        uint32_t w[2 * EX];
+#pragma unroll
+        for (int i = 0; i < EX; ++i) {
+            const uint2 x = __ldg(src + EX * t + i);
+            w[2 * i] = x.x;
+            w[2 * i + 1] = x.y;
+        }
+        const float4* u4 = reinterpret_cast<const float4*>(uq + 64 * t);
+#pragma unroll
+        for (int sub = 0; sub < 4; ++sub) {
+#pragma unroll
+            for (int qd = 0; qd < 4; ++qd) {
+                const uint32_t v = ex_quad<EX>(w, sub, qd);
+                const float4 u = u4[4 * sub + qd];
+                acc[4 * qd + 0] = __fmaf_rn(u.x, byte_to_float(v, 0), acc[4 * qd + 0]);
+                acc[4 * qd + 1] = __fmaf_rn(u.y, byte_to_float(v, 1), acc[4 * qd + 1]);
+                acc[4 * qd + 2] = __fmaf_rn(u.z, byte_to_float(v, 2), acc[4 * qd + 2]);
+                acc[4 * qd + 3] = __fmaf_rn(u.w, byte_to_float(v, 3), acc[4 * qd + 3]);
+            }
+        }
+    }
+    float t3[8], t6[4];
+#pragma unroll
+    for (int l = 0; l < 8; ++l) t3[l] = __fadd_rn(acc[l + 8], acc[l]);
+#pragma unroll
+    for (int m = 0; m < 4; ++m) t6[m] = __fadd_rn(t3[m + 4], t3[m]);
+    return __fadd_rn(__fadd_rn(t6[0], t6[2]), __fadd_rn(t6[1], t6[3]));
+}
+
+// ResultPool::insert + distk (inc/index/Pool.hpp:15-31) on a pool held in
+// shared memory, executed by the whole warp.
+__device__ __forceinline__ void pool_insert(float* pool_d, uint32_t* pool_id, int& size, int k,
+                                            float& distk, float dnew, uint32_t inew, int lane) {
+    if (size == k && dnew > pool_d[size - 1]) return;
+    // lower_bound: number of entries < dnew
+    int lo = 0;
+    for (int i0 = 0; i0 < size; i0 += 32) {
+        const int i = i0 + lane;
+        const bool lt = i < size && pool_d[i] < dnew;
+        lo += __popc(__ballot_sync(0xffffffffu, lt));
+    }
+    // shift [lo, last) up by one; when full the entry at k-1 falls off.
+    // Chunks of 32 from the top down: each chunk is read before the chunk
+    // below writes into its first slot.
+    const int last = size < k ? size : k - 1;
+    for (int i0 = lo + ((last - lo - 1) >> 5) * 32; last > lo && i0 >= lo; i0 -= 32) {
+        const int i = i0 + lane;
+        float sv = 0.f;
+        uint32_t si = 0u;
+        if (i < last) {
+            sv = pool_d[i];
+            si = pool_id[i];
+        }
+        __syncwarp();
+        if (i < last) {
+            pool_d[i + 1] = sv;
+            pool_id[i + 1] = si;
+        }
+        __syncwarp();
+    }
+    if (lane == 0) {
+        pool_d[lo] = dnew;
+        pool_id[lo] = inew;
+    }
+    __syncwarp();
+    size += size < k;
+    distk = size == k ? pool_d[k - 1] : FLT_MAX;
+}
+
+// Shared memory of one warp: unit_q[D] | ipq, onorm, ex_dist, id [128 each] |
+// candidate list [128 bytes] | pool_d[kpad] | pool_id[kpad]
+__host__ __device__ constexpr size_t refine_warp_smem_bytes(int D, int kpad) {
+    return (size_t)D * 4 + (size_t)kChunkBlocks * 32 * 16 + kChunkBlocks * 32 + (size_t)kpad * 8;
 }
 
 template <int EX>
@@ -108,9 +188,14 @@ __global__ void __launch_bounds__(kRefineWarps * 32) refine_kernel(RefineArgs a)
     if (q >= a.nq) return;
     const int D = a.D, k = a.k;
     const int kpad = (k + 31) & ~31;
-    float* unit_q = reinterpret_cast<float*>(smem_raw) +
-                    (size_t)warp * (D + 2 * kpad);
-    float* pool_d = unit_q + D;
+    uint8_t* base = smem_raw + (size_t)warp * refine_warp_smem_bytes(D, kpad);
+    float* uq = reinterpret_cast<float*>(base);
+    float* c_ipq = uq + D;
+    float* c_on = c_ipq + kChunkBlocks * 32;
+    float* c_ed = c_on + kChunkBlocks * 32;
+    uint32_t* c_id = reinterpret_cast<uint32_t*>(c_ed + kChunkBlocks * 32);
+    uint8_t* c_list = reinterpret_cast<uint8_t*>(c_id + kChunkBlocks * 32);
+    float* pool_d = reinterpret_cast<float*>(c_list + kChunkBlocks * 32);
     uint32_t* pool_id = reinterpret_cast<uint32_t*>(pool_d + kpad);
     const int code_len = D * EX / 8;
     const int fac_rescale = 1 << EX;
@@ -143,95 +228,83 @@ __global__ void __launch_bounds__(kRefineWarps * 32) refine_kernel(RefineArgs a)
         const int32_t* S = a.S + a.s_off[qp];
         const uint32_t nblocks = (n + 31) >> 5;
         bool uq_ready = false;
-        for (uint32_t b = 0; b < nblocks; ++b) {
-            const float ipq = __fmul_rn(__int2float_rn(S[32 * b + lane]), delta);
-            const float on = a.onorm[(size_t)(fb + b) * 32 + lane];
-            float lb = __fsub_rn(ipq, c1);
-            lb = __fmul_rn(lb, c2);
-            lb = __fmul_rn(lb, on);
-            lb = __fadd_rn(lb, c3);
-            lb = __fadd_rn(lb, __fmul_rn(on, on));
-            const bool valid = 32 * b + lane < n;
-            uint32_t mask = __ballot_sync(0xffffffffu, valid && (lb < distk));
-            if (mask && !uq_ready) {
-                // unit_q for the refinement (same arithmetic as the scan kernel)
+        for (uint32_t cb = 0; cb < nblocks; cb += kChunkBlocks) {
+            const int nbc = (int)min((uint32_t)kChunkBlocks, nblocks - cb);
+            float lb[kChunkBlocks];
+            bool valid[kChunkBlocks];
+#pragma unroll
+            for (int b = 0; b < kChunkBlocks; ++b) {
+                valid[b] = false;
+                lb[b] = 0.f;
+                if (b < nbc) {
+                    const uint32_t blk = cb + b;
+                    const float ipq = __fmul_rn(__int2float_rn(S[32 * blk + lane]), delta);
+                    const float on = a.onorm[(size_t)(fb + blk) * 32 + lane];
+                    float t = __fsub_rn(ipq, c1);
+                    t = __fmul_rn(t, c2);
+                    t = __fmul_rn(t, on);
+                    t = __fadd_rn(t, c3);
+                    lb[b] = __fadd_rn(t, __fmul_rn(on, on));
+                    valid[b] = 32 * blk + lane < n;
+                    c_ipq[32 * b + lane] = ipq;
+                    c_on[32 * b + lane] = on;
+                }
+            }
+            // Every candidate of these blocks has lb < distk at its block's
+            // start <= distk now, so {lb < distk now} holds them all.
+            int cnt = 0;
+#pragma unroll
+            for (int b = 0; b < kChunkBlocks; ++b) {
+                const uint32_t m = __ballot_sync(0xffffffffu, valid[b] && lb[b] < distk);
+                if ((m >> lane) & 1u) c_list[cnt + __popc(m & ((1u << lane) - 1u))] = (uint8_t)(32 * b + lane);
+                cnt += __popc(m);
+            }
+            if (cnt == 0) continue;
+            if (!uq_ready) {
                 const float* cv = a.centroids + (size_t)cid * D;
                 if (y > kNormEps) {
                     const float fac = recip_via_double(y);
-                    for (int i = lane; i < D; i += 32)
-                        unit_q[i] = __fmul_rn(__fsub_rn(qv[i], cv[i]), fac);
+                    for (int i = lane; i < D; i += 32) uq[i] = __fmul_rn(__fsub_rn(qv[i], cv[i]), fac);
                 } else {
                     const float fill = recip_via_double(__fsqrt_rn((float)D));
-                    for (int i = lane; i < D; i += 32) unit_q[i] = fill;
+                    for (int i = lane; i < D; i += 32) uq[i] = fill;
                 }
-                __syncwarp();
                 uq_ready = true;
             }
-            while (mask) {
-                // two candidates at a time, one per half-warp
-                const int j0 = __ffs(mask) - 1;
-                mask &= mask - 1;
-                const int j1 = mask ? __ffs(mask) - 1 : -1;
-                if (j1 >= 0) mask &= mask - 1;
-                const int hw = lane >> 4, l = lane & 15;
-                const int jm = hw ? (j1 >= 0 ? j1 : j0) : j0;
-                const size_t pos = (size_t)first_vec + 32 * b + jm;
-                const float ip = ex_ip<EX>(unit_q, a.excode + pos * code_len, D, l);
-                // distance estimate in lane 0 of each half (HASearcher.hpp:225-232)
-                const float ipq_j = __shfl_sync(0xffffffffu, ipq, jm);
-                const float on_j = __shfl_sync(0xffffffffu, on, jm);
-                float ex_dist = 0.f;
-                uint32_t id = 0;
-                if (l == 0) {
-                    const float sqr_x = __fmul_rn(on_j, on_j);
-                    const float t = __fadd_rn(__fmul_rn((float)fac_rescale, ipq_j), ip);
+            __syncwarp();
+            // refine the candidates, one per lane (inactive lanes repeat the
+            // first one so the warp stays converged on the broadcast reads)
+            for (int r = 0; r < cnt; r += 32) {
+                const int i = r + lane;
+                const int slot = c_list[i < cnt ? i : 0];
+                const size_t pos = (size_t)first_vec + 32 * cb + slot;
+                const float ip = ex_ip_thread<EX>(uq, a.excode + pos * code_len, D);
+                if (i < cnt) {
+                    // inc/index/HASearcher.hpp:225-232
+                    const float on = c_on[slot];
+                    const float sqr_x = __fmul_rn(on, on);
+                    const float t = __fadd_rn(__fmul_rn((float)fac_rescale, c_ipq[slot]), ip);
                     const double br = __dsub_rn((double)t, ex_sub);
                     const float xy = __fmul_rn(a.xipnorm[pos], y);
                     const float f = __fadd_rn(sqr_x, sqy);
-                    ex_dist = __double2float_rn(__dsub_rn((double)f, __dmul_rn((double)xy, br)));
-                    id = a.ids[pos];
-                }
-                const int ncand = j1 >= 0 ? 2 : 1;
-                for (int t = 0; t < ncand; ++t) {
-                    const float dnew = __shfl_sync(0xffffffffu, ex_dist, 16 * t);
-                    const uint32_t inew = __shfl_sync(0xffffffffu, id, 16 * t);
-                    // ResultPool::insert
-                    if (size == k && dnew > pool_d[size - 1]) continue;
-                    // lower_bound: number of entries < dnew
-                    int lo = 0;
-                    for (int i0 = 0; i0 < size; i0 += 32) {
-                        const int i = i0 + lane;
-                        const bool lt = i < size && pool_d[i] < dnew;
-                        lo += __popc(__ballot_sync(0xffffffffu, lt));
-                    }
-                    // shift [lo, last) up by one; when full the entry at k-1
-                    // falls off.  Chunks of 32 from the top down: each chunk is
-                    // read before the chunk below writes into its first slot.
-                    const int last = size < k ? size : k - 1;
-                    for (int i0 = lo + ((last - lo - 1) >> 5) * 32; last > lo && i0 >= lo; i0 -= 32) {
-                        const int i = i0 + lane;
-                        float sv = 0.f;
-                        uint32_t si = 0u;
-                        if (i < last) {
-                            sv = pool_d[i];
-                            si = pool_id[i];
-                        }
-                        __syncwarp();
-                        if (i < last) {
-                            pool_d[i + 1] = sv;
-                            pool_id[i + 1] = si;
-                        }
-                        __syncwarp();
-                    }
-                    if (lane == 0) {
-                        pool_d[lo] = dnew;
-                        pool_id[lo] = inew;
-                    }
-                    __syncwarp();
-                    size += size < k;
-                    distk = size == k ? pool_d[k - 1] : FLT_MAX;
+                    c_ed[slot] = __double2float_rn(__dsub_rn((double)f, __dmul_rn((double)xy, br)));
+                    c_id[slot] = a.ids[pos];
                 }
             }
+            __syncwarp();
+            // exact replay: the mask of each block against the threshold at
+            // the block's start, candidates in ascending lane order
+#pragma unroll
+            for (int b = 0; b < kChunkBlocks; ++b) {
+                uint32_t mask = __ballot_sync(0xffffffffu, valid[b] && lb[b] < distk);
+                while (mask) {
+                    const int j = __ffs(mask) - 1;
+                    mask &= mask - 1;
+                    pool_insert(pool_d, pool_id, size, k, distk, c_ed[32 * b + j], c_id[32 * b + j],
+                                lane);
+                }
+            }
+            __syncwarp();
         }
     }
     uint32_t* oid = a.out_ids + (size_t)q * k;

@@ -29,6 +29,7 @@ EXPORTED_SYMBOLS = (
     "erq_version", "erq_status_string", "erq_last_error", "erq_index_load",
     "erq_index_get_info", "erq_index_free", "erq_rotate", "erq_search", "erq_search_raw",
     "erq_debug_scan_capacity", "erq_debug_centroid_dists", "erq_debug_probe", "erq_debug_scan",
+    "erq_profile_enable", "erq_profile_reset", "erq_profile_read",
 )
 
 
@@ -89,6 +90,11 @@ def load_library(path: str | None = None) -> C.CDLL:
     lib.erq_debug_probe.restype = C.c_int
     lib.erq_debug_scan.argtypes = [vp, f32p, u64, u64, u32p, f32p, f32p, f32p, vp, vp, u64]
     lib.erq_debug_scan.restype = C.c_int
+    lib.erq_profile_enable.argtypes = [C.c_int]
+    lib.erq_profile_enable.restype = None
+    lib.erq_profile_reset.restype = None
+    lib.erq_profile_read.argtypes = [C.c_char_p, C.POINTER(C.c_uint64), C.POINTER(C.c_double)]
+    lib.erq_profile_read.restype = C.c_int
     _lib = lib
     return lib
 
@@ -97,3 +103,25 @@ def check(status: int) -> None:
     if status != ERQ_OK:
         msg = load_library().erq_last_error().decode(errors="replace")
         raise ErqError(status, msg)
+
+
+KERNELS = ("rotate", "centroid_dist", "select_probe", "scan", "refine")
+
+
+def profile_enable(on: bool = True) -> None:
+    load_library().erq_profile_enable(1 if on else 0)
+
+
+def profile_reset() -> None:
+    load_library().erq_profile_reset()
+
+
+def profile_read() -> dict:
+    """{kernel: (launches, total_ms)} since the last reset (waits for the events)."""
+    lib = load_library()
+    out = {}
+    for k in KERNELS:
+        n, ms = C.c_uint64(), C.c_double()
+        check(lib.erq_profile_read(k.encode(), C.byref(n), C.byref(ms)))
+        out[k] = (int(n.value), float(ms.value))
+    return out

@@ -110,3 +110,132 @@ def ground_truth(base: np.ndarray, query: np.ndarray, k: int):
         sel = b[ids[s:s + step]]
         dist[s:s + step] = np.sum((sel - qq[:, None, :]) ** 2, axis=2)
     return ids, dist
+
+
+# ---------------------------------------------------------------- GPU versions
+# torch is used here as data-preparation plumbing for the large workloads
+# (generation, clustering, ground truth); the search itself never uses it.
+
+def sphere_mixture_torch(n: int, d: int, n_comp: int, sigma: float, seed: int,
+                         n_query: int = 0, zipf_s: float | None = None, device="cuda"):
+    """GPU twin of ``sphere_mixture`` (same distribution, different stream)."""
+    import torch
+
+    g = torch.Generator(device=device).manual_seed(seed)
+    centres = torch.randn(n_comp, d, generator=g, device=device)
+    centres /= centres.norm(dim=1, keepdim=True)
+    if zipf_s is None:
+        comp = torch.randint(0, n_comp, (n + n_query,), generator=g, device=device)
+    else:
+        w = torch.tensor(zipf_weights(n_comp, zipf_s), device=device)
+        perm = torch.randperm(n_comp, generator=g, device=device)
+        comp = perm[torch.multinomial(w, n + n_query, replacement=True, generator=g)]
+    out = torch.empty(n + n_query, d, device=device)
+    step = 1 << 17
+    for s in range(0, n + n_query, step):
+        c = centres[comp[s:s + step]]
+        noise = torch.randn(c.shape, generator=g, device=device)
+        noise -= (noise * c).sum(1, keepdim=True) * c
+        p = c + sigma * noise
+        out[s:s + step] = p / p.norm(dim=1, keepdim=True)
+    return out[:n], out[n:]
+
+
+def gaussian_mixture_torch(n: int, d: int, n_comp: int, sigma: float, seed: int,
+                           n_query: int = 0, device="cuda"):
+    import torch
+
+    g = torch.Generator(device=device).manual_seed(seed)
+    centres = torch.randn(n_comp, d, generator=g, device=device)
+    comp = torch.randint(0, n_comp, (n + n_query,), generator=g, device=device)
+    x = centres[comp] + sigma * torch.randn(n + n_query, d, generator=g, device=device)
+    return x[:n], x[n:]
+
+
+def kmeans_torch(x, k: int, iters: int = 20, seed: int = 0):
+    """Lloyd's k-means on the GPU (TF32 distance products, float32 updates).
+    Returns (centroids [k, d] float32, ids [n] int64) with ids the nearest
+    final centroid."""
+    import torch
+
+    g = torch.Generator(device=x.device).manual_seed(seed)
+    c = x[torch.randperm(x.shape[0], generator=g, device=x.device)[:k]].clone()
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = True
+    try:
+        def assign(cent):
+            cc = (cent * cent).sum(1)
+            ids = torch.empty(x.shape[0], dtype=torch.long, device=x.device)
+            step = 1 << 16
+            for s in range(0, x.shape[0], step):
+                xs = x[s:s + step]
+                ids[s:s + step] = (cc[None, :] - 2.0 * xs @ cent.T).argmin(1)
+            return ids
+
+        rng = np.random.default_rng(seed)
+        for _ in range(iters):
+            a = assign(c)
+            sums = torch.zeros_like(c).index_add_(0, a, x)
+            cnt = torch.bincount(a, minlength=k)
+            nz = cnt > 0
+            c[nz] = sums[nz] / cnt[nz, None].to(x.dtype)
+            _split_empty_clusters(c, cnt.cpu().numpy(), rng)
+        a = assign(c)
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = prev
+    return c, a
+
+
+def _split_empty_clusters(c, counts, rng, eps: float = 1.0 / 1024):
+    """Re-seed every empty cluster by splitting a populated one, chosen with
+    probability proportional to its size: the two centroids become the old
+    one scaled by (1 +- eps) alternately per dimension and the members are
+    shared (the empty-cluster rule of faiss's k-means, which the reference's
+    clustering step uses, python/ivf.py)."""
+    import torch
+
+    counts = counts.astype(np.float64).copy()
+    empty = np.flatnonzero(counts == 0)
+    if empty.size == 0:
+        return
+    n, k = counts.sum(), counts.size
+    sign = torch.ones(c.shape[1], device=c.device, dtype=c.dtype)
+    sign[1::2] = -1.0
+    for ci in empty:
+        p = np.maximum(counts - 1.0, 0.0)
+        p /= p.sum() if p.sum() > 0 else 1.0
+        cj = int(rng.choice(k, p=p)) if p.sum() > 0 else int(np.argmax(counts))
+        c[ci] = c[cj] * (1 + eps * sign)
+        c[cj] = c[cj] * (1 - eps * sign)
+        counts[ci] = counts[cj] / 2
+        counts[cj] -= counts[ci]
+    del n
+
+
+def ground_truth_torch(base, query, k: int, qstep: int = 2048, bstep: int = 1 << 18):
+    """Exact top-k by float64 squared L2 on the GPU.  Returns (ids int64
+    [nq, k], dists float64 [nq, k])."""
+    import torch
+
+    nq = query.shape[0]
+    best_d = torch.full((nq, k), float("inf"), dtype=torch.float64, device=base.device)
+    best_i = torch.zeros((nq, k), dtype=torch.long, device=base.device)
+    for b0 in range(0, base.shape[0], bstep):
+        b = base[b0:b0 + bstep].double()
+        bb = (b * b).sum(1)
+        for q0 in range(0, nq, qstep):
+            q = query[q0:q0 + qstep].double()
+            d = (q * q).sum(1, keepdim=True) - 2.0 * q @ b.T + bb[None, :]
+            kk = min(k, d.shape[1])
+            vd, vi = d.topk(kk, dim=1, largest=False)
+            cat_d = torch.cat([best_d[q0:q0 + qstep], vd], 1)
+            cat_i = torch.cat([best_i[q0:q0 + qstep], vi + b0], 1)
+            o = torch.argsort(cat_d, dim=1, stable=True)[:, :k]
+            best_d[q0:q0 + qstep] = cat_d.gather(1, o)
+            best_i[q0:q0 + qstep] = cat_i.gather(1, o)
+    # exact distances of the selected ids, summed directly in float64
+    for q0 in range(0, nq, qstep):
+        q = query[q0:q0 + qstep].double()
+        sel = base[best_i[q0:q0 + qstep]].double()
+        best_d[q0:q0 + qstep] = ((sel - q[:, None, :]) ** 2).sum(2)
+    return best_i, best_d

@@ -41,6 +41,16 @@ ERQ_API erq_status erq_debug_scan(const erq_index* index, const float* rotated_q
                           uint64_t nprobe, uint32_t* cids, float* sqr_y, float* delta,
                           float* sumq, uint64_t* s_offsets, int32_t* S, uint64_t s_capacity);
 
+/* Kernel timing.  While enabled, every kernel launch of the search and
+ * rotation entry points is bracketed by CUDA events recorded on the stream
+ * the kernel runs on.  erq_profile_read waits for the recorded events and
+ * returns, for one kernel ("rotate", "centroid_dist", "select_probe", "scan",
+ * "refine"), the number of launches and their summed device time since the
+ * last reset.  Process-wide; meant for benchmarks. */
+ERQ_API void erq_profile_enable(int on);
+ERQ_API void erq_profile_reset(void);
+ERQ_API erq_status erq_profile_read(const char* kernel, uint64_t* launches, double* total_ms);
+
 #ifdef __cplusplus
 }
 #endif
