@@ -583,6 +583,43 @@ erq_status search_entry(const erq_index* idx, const float* queries, bool rotated
 
 }  // namespace
 
+// ------------------------------------------------- allocation-free search
+// Scratch of erq_search_noalloc: one fixed array in this module's device
+// memory (every GPU that loads the library holds it until the process
+// exits).  Host code must not take its address with &; the device address is
+// fetched once per device with cudaGetSymbolAddress.
+constexpr uint64_t kNoAllocScratchBytes = 64ull << 20;
+static __device__ __align__(256) uint8_t g_noalloc_scratch[kNoAllocScratchBytes];
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+uint8_t* g_noalloc_ptr[kMaxDevices] = {};
+
+// Device address of the scratch array on `device`, which must be current.
+erq_status noalloc_scratch(int device, uint8_t** out) {
+    if (device < 0 || device >= kMaxDevices)
+        return fail(ERQ_ERR_UNSUPPORTED, "device ordinal %d above %d", device, kMaxDevices - 1);
+    std::lock_guard<std::mutex> g(g_noalloc_mu);
+    if (!g_noalloc_ptr[device]) {
+        void* p = nullptr;
+        ERQ_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+        g_noalloc_ptr[device] = static_cast<uint8_t*>(p);
+    }
+    *out = g_noalloc_ptr[device];
+    return ERQ_OK;
+}
+
+uint64_t align256(uint64_t b) { return (b + 255) & ~255ull; }
+
+// Scratch bytes one call needs for nq queries at this nprobe.
+uint64_t noalloc_bytes(const erq_index* idx, uint64_t nq, uint64_t nprobe) {
+    const uint64_t np = nq * nprobe;
+    return align256(nq * idx->K * 4) + 2 * align256(np * 4) + align256(np * 8) +
+           align256(nq * 32ull * idx->top_blocks[nprobe] * 4) + 2 * align256(np * 4);
+}
+}  // namespace
+
 // ------------------------------------------------------------------ C ABI
 extern "C" {
 
@@ -675,6 +712,59 @@ erq_status erq_search(const erq_index* idx, const float* rotated_queries, uint64
 erq_status erq_search_raw(const erq_index* idx, const float* queries, uint64_t nq, uint64_t k,
                           uint64_t nprobe, uint32_t* ids, float* dists, void* stream) {
     return search_entry(idx, queries, false, nq, k, nprobe, ids, dists, stream);
+}
+
+erq_status erq_search_noalloc(const erq_index* idx, const float* rotated_queries, uint64_t nq,
+                              uint64_t k, uint64_t nprobe, uint32_t* ids, float* dists,
+                              void* stream) {
+    ERQ_TRY(check_search_args(idx, nq, k, nprobe, rotated_queries, ids));
+    if (nq == 0) return ERQ_OK;
+    DeviceGuard guard;
+    ERQ_TRY(guard.set(idx->device));
+    if (!is_device_ptr(rotated_queries) || !is_device_ptr(ids) || (dists && !is_device_ptr(dists)))
+        return fail(ERQ_ERR_INVALID_ARGUMENT,
+                    "erq_search_noalloc takes device memory only (queries, ids, dists)");
+    if ((reinterpret_cast<uintptr_t>(rotated_queries) & 15) ||
+        (reinterpret_cast<uintptr_t>(ids) & 3) || (reinterpret_cast<uintptr_t>(dists) & 3))
+        return fail(ERQ_ERR_INVALID_ARGUMENT,
+                    "queries must be 16-byte aligned and ids/dists 4-byte aligned");
+    const uint64_t need = noalloc_bytes(idx, nq, nprobe);
+    if (need > kNoAllocScratchBytes) {
+        uint64_t fit = 0;
+        while (fit < nq && noalloc_bytes(idx, fit + 1, nprobe) <= kNoAllocScratchBytes) ++fit;
+        return fail(ERQ_ERR_INVALID_ARGUMENT,
+                    "%llu queries at nprobe=%llu need %llu bytes of scratch; the static scratch "
+                    "holds %llu bytes (at most %llu queries per call here)",
+                    (unsigned long long)nq, (unsigned long long)nprobe, (unsigned long long)need,
+                    (unsigned long long)kNoAllocScratchBytes, (unsigned long long)fit);
+    }
+    uint8_t* base = nullptr;
+    ERQ_TRY(noalloc_scratch(idx->device, &base));
+    ERQ_TRY(configure_kernels((int)idx->D, (int)idx->K, (int)k));
+    // Carve the batch buffers.  Every element a kernel reads is written
+    // earlier in the same call, so nothing needs clearing between calls.
+    const uint64_t np = nq * nprobe;
+    Batch b;
+    b.nq = nq;
+    b.qrot = rotated_queries;
+    uint8_t* cur = base;
+    auto take = [&cur](uint64_t bytes) {
+        uint8_t* p = cur;
+        cur += align256(bytes);
+        return p;
+    };
+    b.dist = reinterpret_cast<float*>(take(nq * idx->K * 4));
+    b.probe_cid = reinterpret_cast<uint32_t*>(take(np * 4));
+    b.probe_sqy = reinterpret_cast<float*>(take(np * 4));
+    b.s_off = reinterpret_cast<uint64_t*>(take(np * 8));
+    b.S = reinterpret_cast<int32_t*>(take(nq * 32ull * idx->top_blocks[nprobe] * 4));
+    b.delta = reinterpret_cast<float*>(take(np * 4));
+    b.sumq = reinterpret_cast<float*>(take(np * 4));
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    ERQ_TRY(launch_probe(idx, b, nprobe, st));
+    ERQ_TRY(launch_scan(idx, b, nprobe, st));
+    ERQ_TRY(launch_refine(idx, b, nprobe, k, ids, dists, st));
+    return ERQ_OK;
 }
 
 // ------------------------------------------------------------- debug ABI

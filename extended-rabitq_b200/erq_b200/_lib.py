@@ -28,6 +28,7 @@ STATUS_NAMES = {
 EXPORTED_SYMBOLS = (
     "erq_version", "erq_status_string", "erq_last_error", "erq_index_load",
     "erq_index_get_info", "erq_index_free", "erq_rotate", "erq_search", "erq_search_raw",
+    "erq_search_noalloc",
     "erq_debug_scan_capacity", "erq_debug_centroid_dists", "erq_debug_probe", "erq_debug_scan",
     "erq_profile_enable", "erq_profile_reset", "erq_profile_read",
 )
@@ -82,6 +83,8 @@ def load_library(path: str | None = None) -> C.CDLL:
     lib.erq_search.restype = C.c_int
     lib.erq_search_raw.argtypes = [vp, f32p, u64, u64, u64, u32p, f32p, vp]
     lib.erq_search_raw.restype = C.c_int
+    lib.erq_search_noalloc.argtypes = [vp, f32p, u64, u64, u64, u32p, f32p, vp]
+    lib.erq_search_noalloc.restype = C.c_int
     lib.erq_debug_scan_capacity.argtypes = [vp, u64, u64]
     lib.erq_debug_scan_capacity.restype = u64
     lib.erq_debug_centroid_dists.argtypes = [vp, f32p, u64, f32p]

@@ -92,6 +92,27 @@ ERQ_API erq_status erq_search_raw(const erq_index* index, const float* queries, 
                           uint64_t k, uint64_t nprobe, uint32_t* ids, float* dists,
                           void* stream);
 
+/* erq_search without any memory allocation.  Has no counterpart in the
+ * reference: it is for callers that cannot allocate device memory while a
+ * query runs - engines that hand all GPU memory to their own allocator up
+ * front, or serving loops that forbid allocation on the request path - and
+ * so cannot let erq_search take its scratch from a memory pool.
+ *
+ * All pointers must be device memory (queries 16-byte aligned, ids/dists
+ * 4-byte aligned); the call is asynchronous on `stream`.  The pipeline's
+ * scratch is a fixed 64 MiB array in the library's device memory, held on
+ * every GPU that loads the library until the process exits.  A request that
+ * does not fit (about nq * (4K + 128 * blocks of the nprobe largest clusters)
+ * bytes) fails with ERQ_ERR_INVALID_ARGUMENT and a message giving the largest
+ * batch that fits.  The first call on a device looks up the array's device
+ * address; make that first call before any stream capture.  Every call uses
+ * the same array: calls that overlap on the GPU (different streams, or
+ * different threads without ordering) race and must be serialised by the
+ * caller.  Results equal erq_search's. */
+ERQ_API erq_status erq_search_noalloc(const erq_index* index, const float* rotated_queries,
+                                      uint64_t nq, uint64_t k, uint64_t nprobe, uint32_t* ids,
+                                      float* dists, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
