@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <cstdarg>
 #include <cstdio>
+#include <cmath>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -23,6 +24,8 @@
 #include "../../include/erq.h"
 #include "../../include/erq_debug.h"
 #include "coarse.cuh"
+#include "gemm.cuh"
+#include "probe.cuh"
 #include "layout.cuh"
 #include "refine.cuh"
 #include "scan.cuh"
@@ -111,9 +114,19 @@ struct Scratch {
 
 // ----------------------------------------------------------------- profiler
 // Event pairs around kernel launches, resolved lazily by erq_profile_read.
-enum KernelId { kRotate = 0, kCentroidDist, kSelectProbe, kScan, kRefine, kNumKernels };
+enum KernelId {
+    kRotate = 0,
+    kCentroidDist,
+    kSelectProbe,
+    kScan,
+    kRefine,
+    kSplit,
+    kGemm,
+    kProbe,
+    kNumKernels
+};
 const char* const kKernelNames[kNumKernels] = {"rotate", "centroid_dist", "select_probe", "scan",
-                                               "refine"};
+                                               "refine", "split",  "gemm",          "probe"};
 
 struct Profiler {
     std::mutex mu;
@@ -185,6 +198,12 @@ struct erq_index {
     uint32_t* c_first_vec = nullptr;
     uint32_t* c_size = nullptr;
     uint32_t* c_nblocks = nullptr;
+    // split-BF16 operands of the tensor-core GEMMs (gemm.cuh)
+    __nv_bfloat16* c_split = nullptr;   // [K][3D] centroids (hi | lo | hi)
+    __nv_bfloat16* pt_split = nullptr;  // [D][3D] rows of P^T (hi | lo | hi)
+    float* cn = nullptr;                // [K] squared centroid norms
+    float cn_max = 0.f;
+    float eps_rel = 0.f;                // distance-estimate bound (probe.cuh)
     // per-call scratch pool; keeps freed blocks for reuse by later calls
     cudaMemPool_t pool = nullptr;
 
@@ -198,7 +217,8 @@ struct erq_index {
         }
         for (void* p : {(void*)P, (void*)centroids, (void*)codes, (void*)onorm, (void*)excode,
                         (void*)xipnorm, (void*)ids, (void*)c_first_block, (void*)c_first_vec,
-                        (void*)c_size, (void*)c_nblocks})
+                        (void*)c_size, (void*)c_nblocks, (void*)c_split, (void*)pt_split,
+                        (void*)cn})
             if (p) cudaFree(p);
         if (prev >= 0) cudaSetDevice(prev);
     }
@@ -334,6 +354,40 @@ erq_status load_impl(const char* path, erq_index* idx) {
     ERQ_CUDA(cudaMemcpy(idx->c_first_vec, first_vec.data(), K * 4, cudaMemcpyHostToDevice));
     ERQ_CUDA(cudaMemcpy(idx->c_size, csize.data(), K * 4, cudaMemcpyHostToDevice));
     ERQ_CUDA(cudaMemcpy(idx->c_nblocks, idx->h_nblocks.data(), K * 4, cudaMemcpyHostToDevice));
+    // split-BF16 GEMM operands: centroids and the rows of P^T
+    ERQ_TRY(dev_alloc(idx, &idx->c_split, K * 3 * D));
+    ERQ_TRY(dev_alloc(idx, &idx->pt_split, D * 3 * D));
+    ERQ_TRY(dev_alloc(idx, &idx->cn, K));
+    {
+        std::vector<float> hp(D * D), hpt(D * D);
+        ERQ_CUDA(cudaMemcpy(hp.data(), idx->P, D * D * 4, cudaMemcpyDeviceToHost));
+        for (uint64_t i = 0; i < D; ++i)
+            for (uint64_t j = 0; j < D; ++j) hpt[j * D + i] = hp[i * D + j];
+        float* tmp = nullptr;
+        ERQ_CUDA(cudaMalloc(&tmp, D * D * 4));
+        cudaError_t e = cudaMemcpy(tmp, hpt.data(), D * D * 4, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) {
+            split_rows_kernel<<<(unsigned)D, 256>>>(tmp, (int)D, (int)D, (int)D, false,
+                                                    idx->pt_split, nullptr);
+            split_rows_kernel<<<(unsigned)K, 256>>>(idx->centroids, (int)K, (int)D, (int)D, false,
+                                                    idx->c_split, idx->cn);
+            e = cudaGetLastError();
+            if (e == cudaSuccess) e = cudaDeviceSynchronize();
+        }
+        cudaFree(tmp);
+        if (e != cudaSuccess) return fail(ERQ_ERR_CUDA, "split operands: %s", cudaGetErrorString(e));
+        std::vector<float> hcn(K);
+        ERQ_CUDA(cudaMemcpy(hcn.data(), idx->cn, K * 4, cudaMemcpyDeviceToHost));
+        idx->cn_max = *std::max_element(hcn.begin(), hcn.end());
+        // |estimate - true| <= (qn + cn) * (7 D u + 3.2 * 2^-16 + 3u) for the
+        // split-BF16 products accumulated in FP32 plus the norm sums and the
+        // epilogue; the reference's own L2Sqr16 value is within
+        // 2 (D/16 + 6) u (qn + cn) of the true distance.  25% margin.
+        const double u = std::ldexp(1.0, -24);
+        const double dd = (double)D;
+        idx->eps_rel = (float)(1.25 * (7 * dd * u + 3.2 * std::ldexp(1.0, -16) + 3 * u +
+                                       2 * (dd / 16 + 6) * u));
+    }
     cudaMemPoolProps props = {};
     props.allocType = cudaMemAllocationTypePinned;
     props.location.type = cudaMemLocationTypeDevice;
@@ -362,6 +416,8 @@ erq_status configure_kernels(int D, int K, int k) {
                                   kp2 * 8));
     ERQ_CUDA(cudaFuncSetAttribute(scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)scan_smem_bytes(D)));
+    ERQ_CUDA(cudaFuncSetAttribute(probe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)probe_smem_bytes(D, K, kp2)));
     const int rs = (int)refine_smem_bytes(D, k);
     ERQ_CUDA(cudaFuncSetAttribute(refine_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, rs));
     ERQ_CUDA(cudaFuncSetAttribute(refine_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, rs));
@@ -383,12 +439,14 @@ struct Batch {
     int32_t* S = nullptr;
     float* delta = nullptr;
     float* sumq = nullptr;
+    __nv_bfloat16* qsplit = nullptr;  // [nq][3D] split rotated queries
+    float* qn = nullptr;              // [nq]
 };
 
 // Largest query batch whose scan workspace fits the budget.
 uint64_t batch_queries(const erq_index* idx, uint64_t nprobe, uint64_t nq) {
     const uint64_t per_q = 32ull * idx->top_blocks[nprobe] * sizeof(int32_t) +
-                           idx->K * sizeof(float) + nprobe * 24;
+                           idx->K * sizeof(float) + nprobe * 24 + 6 * idx->D + 4;
     const uint64_t budget = 3ull << 30;
     uint64_t b = std::max<uint64_t>(1, budget / std::max<uint64_t>(per_q, 1));
     return std::min(b, nq);
@@ -403,6 +461,62 @@ erq_status alloc_batch(Scratch& s, const erq_index* idx, uint64_t nq, uint64_t n
     ERQ_TRY(s.alloc(&b.S, nq * 32ull * idx->top_blocks[nprobe]));
     ERQ_TRY(s.alloc(&b.delta, nq * nprobe));
     ERQ_TRY(s.alloc(&b.sumq, nq * nprobe));
+    ERQ_TRY(s.alloc(&b.qsplit, nq * 3 * idx->D));
+    ERQ_TRY(s.alloc(&b.qn, nq));
+    return ERQ_OK;
+}
+
+// Candidate count for the probe: nprobe plus a margin (probe.cuh).
+int probe_candidates(uint64_t nprobe) {
+    return (int)(nprobe + std::max<uint64_t>(32, nprobe / 2));
+}
+
+// Coarse probe on tensor cores: split the rotated queries, estimate all
+// distances with the split-BF16 GEMM, then the exact probe kernel.
+erq_status launch_probe_tc(const erq_index* idx, const Batch& b, uint64_t nprobe,
+                           cudaStream_t st) {
+    const int D = (int)idx->D, K = (int)idx->K;
+    {
+        LaunchTimer t(kSplit, st);
+        split_rows_kernel<<<(unsigned)b.nq, 256, 0, st>>>(b.qrot, (int)b.nq, D, D, true, b.qsplit,
+                                                          b.qn);
+        t.finish();
+        ERQ_CUDA(cudaGetLastError());
+    }
+    {
+        GemmEpilogue epi;
+        epi.row_norm = b.qn;
+        epi.col_norm = idx->cn;
+        dim3 grid((unsigned)div_up(K, kGemmBN), (unsigned)div_up(b.nq, kGemmBM));
+        LaunchTimer t(kGemm, st);
+        gemm_bf16_tn_kernel<<<grid, kGemmThreads, 0, st>>>(b.qsplit, idx->c_split, b.dist,
+                                                          (int)b.nq, K, 3 * D, epi);
+        t.finish();
+        ERQ_CUDA(cudaGetLastError());
+    }
+    ProbeArgs a;
+    a.approx = b.dist;
+    a.qrot = b.qrot;
+    a.centroids = idx->centroids;
+    a.qn = b.qn;
+    a.c_nblocks = idx->c_nblocks;
+    a.cn_max = idx->cn_max;
+    a.eps_rel = idx->eps_rel;
+    a.stride = 32ull * idx->top_blocks[nprobe];
+    a.probe_cid = b.probe_cid;
+    a.probe_sqy = b.probe_sqy;
+    a.s_off = b.s_off;
+    a.fallbacks = nullptr;
+    a.nq = (int)b.nq;
+    a.K = K;
+    a.Kpow2 = next_pow2(K);
+    a.D = D;
+    a.nprobe = (int)nprobe;
+    a.M = probe_candidates(nprobe);
+    LaunchTimer t(kProbe, st);
+    probe_kernel<<<(unsigned)b.nq, kProbeThreads, probe_smem_bytes(D, K, a.Kpow2), st>>>(a);
+    t.finish();
+    ERQ_CUDA(cudaGetLastError());
     return ERQ_OK;
 }
 
@@ -516,7 +630,7 @@ erq_status search_device(const erq_index* idx, const float* qrot_dev, uint64_t n
     for (uint64_t q0 = 0; q0 < nq; q0 += bq) {
         b.nq = std::min(bq, nq - q0);
         b.qrot = qrot_dev + q0 * idx->D;
-        ERQ_TRY(launch_probe(idx, b, nprobe, st));
+        ERQ_TRY(launch_probe_tc(idx, b, nprobe, st));
         ERQ_TRY(launch_scan(idx, b, nprobe, st));
         ERQ_TRY(launch_refine(idx, b, nprobe, k, ids_dev + q0 * k,
                               dists_dev ? dists_dev + q0 * k : nullptr, st));
@@ -524,12 +638,25 @@ erq_status search_device(const erq_index* idx, const float* qrot_dev, uint64_t n
     return ERQ_OK;
 }
 
+// out[nq][D] = pad(q[nq][DIM]) * P on tensor cores (split-BF16, FP32 accumulation).
 erq_status rotate_device(const erq_index* idx, const float* q_dev, uint64_t nq, float* out_dev,
                          cudaStream_t st) {
     if (nq == 0) return ERQ_OK;
-    dim3 grid((unsigned)div_up(idx->D, kRotBN), (unsigned)div_up(nq, kRotBM));
+    const int D = (int)idx->D;
+    Scratch s(st, idx->pool);
+    __nv_bfloat16* qs = nullptr;
+    ERQ_TRY(s.alloc(&qs, nq * 3 * (uint64_t)D));
+    {
+        LaunchTimer t(kSplit, st);
+        split_rows_kernel<<<(unsigned)nq, 256, 0, st>>>(q_dev, (int)nq, (int)idx->DIM, D, true, qs,
+                                                        nullptr);
+        t.finish();
+        ERQ_CUDA(cudaGetLastError());
+    }
+    dim3 grid((unsigned)div_up(D, kGemmBN), (unsigned)div_up(nq, kGemmBM));
     LaunchTimer t(kRotate, st);
-    rotate_kernel<<<grid, 256, 0, st>>>(q_dev, (int)nq, (int)idx->DIM, idx->P, (int)idx->D, out_dev);
+    gemm_bf16_tn_kernel<<<grid, kGemmThreads, 0, st>>>(qs, idx->pt_split, out_dev, (int)nq, D,
+                                                      3 * D, GemmEpilogue());
     t.finish();
     ERQ_CUDA(cudaGetLastError());
     return ERQ_OK;
@@ -784,7 +911,7 @@ erq_status erq_debug_probe(const erq_index* idx, const float* qrot, uint64_t nq,
     Batch b;
     ERQ_TRY(alloc_batch(s, idx, nq, nprobe, b));
     b.qrot = q;
-    ERQ_TRY(launch_probe(idx, b, nprobe, st));
+    ERQ_TRY(launch_probe_tc(idx, b, nprobe, st));
     ERQ_CUDA(cudaMemcpyAsync(cids, b.probe_cid, nq * nprobe * 4, cudaMemcpyDeviceToHost, st));
     ERQ_CUDA(cudaMemcpyAsync(sqr_y, b.probe_sqy, nq * nprobe * 4, cudaMemcpyDeviceToHost, st));
     ERQ_CUDA(cudaStreamSynchronize(st));
@@ -840,7 +967,7 @@ erq_status erq_debug_scan(const erq_index* idx, const float* qrot, uint64_t nq, 
     ERQ_TRY(alloc_batch(s, idx, nq, nprobe, b));
     b.qrot = q;
     ERQ_CUDA(cudaMemsetAsync(b.S, 0, need * 4, st));
-    ERQ_TRY(launch_probe(idx, b, nprobe, st));
+    ERQ_TRY(launch_probe_tc(idx, b, nprobe, st));
     ERQ_TRY(launch_scan(idx, b, nprobe, st));
     const uint64_t np = nq * nprobe;
     ERQ_CUDA(cudaMemcpyAsync(cids, b.probe_cid, np * 4, cudaMemcpyDeviceToHost, st));

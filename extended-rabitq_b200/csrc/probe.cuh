@@ -1,0 +1,225 @@
+// Coarse probe from tensor-core distance estimates, exact by construction.
+//
+// FlatInitializer::centroids_distances (inc/index/Initializer.hpp:55-68)
+// ranks all K centroids by L2Sqr16 (inc/utils/space.hpp:18-39) and keeps the
+// nprobe nearest.  Here the GEMM of gemm.cuh gives an estimate a_c of every
+// squared distance with |a_c - true_c| <= eps_a, and one thread block per query
+//   1. selects the M smallest estimates (radix select on order-preserving
+//      keys): candidate set S, and A = the (M+1)-th smallest estimate;
+//   2. recomputes the exact reference value e_c (16 ordered FMA chains + the
+//      reduce tree) for every c in S and sorts S by (e_c, c);
+//   3. checks A - eps > e_(nprobe), eps = eps_a + the reference's own rounding
+//      bound.  Any centroid outside S then has e_c >= A - eps > e_(nprobe), so
+//      the first nprobe of S are exactly the reference's choice (ties by id);
+//   4. if the check fails, computes e_c for all K centroids and sorts them all.
+#pragma once
+
+#include "common.cuh"
+
+namespace erq {
+
+struct ProbeArgs {
+    const float* approx;      // [nq][K] distance estimates
+    const float* qrot;        // [nq][D]
+    const float* centroids;   // [K][D]
+    const float* qn;          // [nq] squared query norms
+    const uint32_t* c_nblocks; // [K]
+    float cn_max;             // largest squared centroid norm
+    float eps_rel;            // eps = eps_rel * (qn + cn_max)
+    uint64_t stride;          // scan workspace per query (int32 entries)
+    uint32_t* probe_cid;      // [nq][nprobe]
+    float* probe_sqy;         // [nq][nprobe]
+    uint64_t* s_off;          // [nq][nprobe]
+    uint32_t* fallbacks;      // optional counter of queries that took step 4
+    int nq, K, Kpow2, D, nprobe, M;
+};
+
+constexpr int kProbeThreads = 256;
+
+__device__ __forceinline__ uint32_t order_key(float f) {
+    const uint32_t b = __float_as_uint(f);
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__device__ __forceinline__ float order_key_value(uint32_t k) {
+    return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
+}
+
+// Exact L2Sqr16 of (q, centroid c) by the 16 lanes of a half-warp; valid in
+// the half-warp's lane 0.
+__device__ __forceinline__ float l2sqr16_halfwarp(const float* __restrict__ q,
+                                                  const float* __restrict__ c, int D, int l) {
+    float acc = 0.f;
+#pragma unroll 4
+    for (int i = l; i < D; i += 16) {
+        const float t = __fsub_rn(q[i], c[i]);
+        acc = __fmaf_rn(t, t, acc);
+    }
+    return tree16_sum(acc);
+}
+
+// Bitonic sort of n (power of two) 64-bit keys in shared memory, ascending.
+__device__ __forceinline__ void block_bitonic_sort(uint64_t* keys, int n) {
+    for (int size = 2; size <= n; size <<= 1) {
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            for (int t = threadIdx.x; t < (n >> 1); t += blockDim.x) {
+                const int lo = 2 * t - (t & (stride - 1));
+                const int hi = lo + stride;
+                const bool up = (lo & size) == 0;
+                const uint64_t a = keys[lo], b = keys[hi];
+                if ((a > b) == up) {
+                    keys[lo] = b;
+                    keys[hi] = a;
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// Shared memory: q[D] | keys u32 [K] | sort keys u64 [Kpow2] | hist[256] | misc
+__host__ __device__ constexpr size_t probe_smem_bytes(int D, int K, int Kpow2) {
+    return (size_t)D * 4 + (size_t)K * 4 + 8 + (size_t)Kpow2 * 8 + 256 * 4 + 64;
+}
+
+__global__ void __launch_bounds__(kProbeThreads) probe_kernel(ProbeArgs a) {
+    extern __shared__ __align__(16) uint8_t smem_raw[];
+    const int q = blockIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int K = a.K, D = a.D;
+    float* qs = reinterpret_cast<float*>(smem_raw);
+    uint32_t* keys = reinterpret_cast<uint32_t*>(qs + D);
+    uint64_t* sk = reinterpret_cast<uint64_t*>(
+        reinterpret_cast<uint8_t*>(keys) + (((size_t)K * 4 + 15) & ~size_t(15)));
+    uint32_t* hist = reinterpret_cast<uint32_t*>(sk + a.Kpow2);
+    int* misc = reinterpret_cast<int*>(hist + 256);  // [0] digit [1] before [2] count [3] ok
+
+    for (int i = tid; i < D; i += blockDim.x) qs[i] = a.qrot[(size_t)q * D + i];
+    const float* aq = a.approx + (size_t)q * K;
+    for (int c = tid; c < K; c += blockDim.x) keys[c] = order_key(aq[c]);
+    __syncthreads();
+
+    const int M = a.M;
+    const bool select_all = M + 1 > K;
+    uint32_t kstar = 0xffffffffu;
+    if (!select_all) {
+        // radix select of the (M+1)-th smallest key, 8 bits at a time
+        uint32_t prefix = 0, pmask = 0;
+        int rank = M + 1;
+        for (int shift = 24; shift >= 0; shift -= 8) {
+            for (int i = tid; i < 256; i += blockDim.x) hist[i] = 0;
+            __syncthreads();
+            for (int c = tid; c < K; c += blockDim.x) {
+                const uint32_t kk = keys[c];
+                if ((kk & pmask) == prefix) atomicAdd(&hist[(kk >> shift) & 255u], 1u);
+            }
+            __syncthreads();
+            if (warp == 0) {
+                uint32_t h[8], s = 0;
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    h[i] = hist[8 * lane + i];
+                    s += h[i];
+                }
+                uint32_t incl = s;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o) incl += v;
+                }
+                const uint32_t excl = incl - s;
+                const bool here = excl < (uint32_t)rank && incl >= (uint32_t)rank;
+                if (here) {
+                    uint32_t run = excl;
+                    int d = 0;
+                    for (; d < 8; ++d) {
+                        if (run + h[d] >= (uint32_t)rank) break;
+                        run += h[d];
+                    }
+                    misc[0] = 8 * lane + d;
+                    misc[1] = (int)run;
+                }
+            }
+            __syncthreads();
+            prefix |= (uint32_t)misc[0] << shift;
+            pmask |= 0xffu << shift;
+            rank -= misc[1];
+            __syncthreads();
+        }
+        kstar = prefix;
+    }
+    // candidates: every centroid whose estimate is below the (M+1)-th
+    if (tid == 0) misc[2] = 0;
+    __syncthreads();
+    for (int c = tid; c < K; c += blockDim.x) {
+        if (select_all || keys[c] < kstar) {
+            const int slot = atomicAdd(&misc[2], 1);
+            sk[slot] = (uint64_t)c;  // id for now; exact distance filled below
+        }
+    }
+    __syncthreads();
+    const int ns = misc[2];
+    // exact distances of the candidates, 16 per pass (one per half-warp)
+    const int hw = tid >> 4, l = tid & 15, nhw = blockDim.x >> 4;
+    for (int base = 0; base < ns; base += nhw) {
+        const int i = base + hw;
+        const uint32_t c = (uint32_t)(sk[i < ns ? i : 0] & 0xffffffffu);
+        const float e = l2sqr16_halfwarp(qs, a.centroids + (size_t)c * D, D, l);
+        if (l == 0 && i < ns) sk[i] = dist_key(e, c);
+    }
+    int nsort = 1;
+    while (nsort < ns) nsort <<= 1;
+    __syncthreads();
+    for (int i = ns + tid; i < nsort; i += blockDim.x) sk[i] = ~0ull;
+    __syncthreads();
+    block_bitonic_sort(sk, nsort);
+    // bound check
+    if (tid == 0) {
+        bool ok = ns >= a.nprobe;
+        if (ok && !select_all) {
+            const float e_n = __uint_as_float((uint32_t)(sk[a.nprobe - 1] >> 32));
+            const float eps = a.eps_rel * (a.qn[q] + a.cn_max);
+            const float A = order_key_value(kstar);
+            ok = (A - eps > e_n) && (e_n == e_n);
+        }
+        misc[3] = ok ? 1 : 0;
+        if (!ok && a.fallbacks) atomicAdd(a.fallbacks, 1u);
+    }
+    __syncthreads();
+    if (!misc[3]) {
+        // exact distances of all K centroids
+        for (int base = 0; base < K; base += nhw) {
+            const int c = base + hw;
+            const float e = l2sqr16_halfwarp(qs, a.centroids + (size_t)min(c, K - 1) * D, D, l);
+            if (l == 0 && c < K) sk[c] = dist_key(e, (uint32_t)c);
+        }
+        __syncthreads();
+        for (int i = K + tid; i < a.Kpow2; i += blockDim.x) sk[i] = ~0ull;
+        __syncthreads();
+        block_bitonic_sort(sk, a.Kpow2);
+    }
+    // outputs + exclusive prefix of 32*nblocks over the probe order (warp 0)
+    if (warp == 0) {
+        uint64_t run = (uint64_t)q * a.stride;
+        for (int p0 = 0; p0 < a.nprobe; p0 += 32) {
+            const int p = p0 + lane;
+            uint32_t nbv = 0;
+            if (p < a.nprobe) {
+                const uint64_t key = sk[p];
+                const uint32_t cid = (uint32_t)(key & 0xffffffffu);
+                a.probe_cid[(size_t)q * a.nprobe + p] = cid;
+                a.probe_sqy[(size_t)q * a.nprobe + p] = __uint_as_float((uint32_t)(key >> 32));
+                nbv = 32u * a.c_nblocks[cid];
+            }
+            uint32_t incl = nbv;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t n = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += n;
+            }
+            if (p < a.nprobe) a.s_off[(size_t)q * a.nprobe + p] = run + (incl - nbv);
+            run += __shfl_sync(0xffffffffu, incl, 31);
+        }
+    }
+}
+
+}  // namespace erq

@@ -108,7 +108,8 @@ def check(status: int) -> None:
         raise ErqError(status, msg)
 
 
-KERNELS = ("rotate", "centroid_dist", "select_probe", "scan", "refine")
+KERNELS = ("rotate", "centroid_dist", "select_probe", "scan", "refine", "split", "gemm",
+           "probe")
 
 
 def profile_enable(on: bool = True) -> None:

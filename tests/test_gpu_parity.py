@@ -180,3 +180,30 @@ def test_errors_are_reported(tmp_path):
     ids, _ = idx.search_batch(g["qrot"], int(g["k"]), int(g["nprobe"]))
     assert (ids == g["ids"]).all()
     idx.free()
+
+
+def test_probe_lists_many_queries(oracle_mod):
+    """Tensor-core estimates + exact recompute give the reference's probe
+    lists for thousands of queries, including queries at a centroid and
+    queries equidistant from several centroids."""
+    from erq_b200 import IVF
+
+    for name in golden_cases():
+        g = load_golden(name)
+        idx = IVF(g["path"])
+        o = oracle_mod.Oracle(g["path"])
+        cent = o.centroids()
+        rng = np.random.default_rng(3)
+        n = 1500
+        q = (cent[rng.integers(0, o.K, n)] + rng.choice([0.0, 0.05, 0.5], size=(n, 1)) *
+             rng.standard_normal((n, o.D))).astype(np.float32)
+        q[:20] = cent[rng.integers(0, o.K, 20)]          # exactly on a centroid
+        q[20:40] = 0.5 * (cent[0] + cent[1])              # halfway between two
+        for nprobe in sorted({1, 3, min(o.K, 8), o.K}):
+            cids, sq = idx.debug_probe(q, nprobe)
+            for i in range(0, n, 97):
+                c_o, s_o = o.probe(q[i], nprobe)
+                assert (cids[i] == c_o).all(), (name, nprobe, i)
+                assert (bits(sq[i]) == bits(s_o)).all()
+        idx.free()
+        o.close()
