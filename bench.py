@@ -203,38 +203,13 @@ def time_cpu(searcher, kind, query_raw, k, nprobe, threads, budget_s, max_n):
 
 
 # ------------------------------------------------------------------ helpers
+from erq_b200.replicas import barrier, finish as dist_finish, max_over_ranks  # noqa: E402
+
+
 def dist_setup(args):
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import datetime
+    from erq_b200 import replicas
 
-        import torch
-        import torch.distributed as dist
-
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                device_id=torch.device("cuda", local))
-    return world, rank, local
-
-
-def barrier(world):
-    if world > 1:
-        import torch.distributed as dist
-
-        dist.barrier()
-
-
-def max_over_ranks(x, world):
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    return replicas.init(timeout_s=600)
 
 
 def choose_nprobe(idx, qraw, gt, cfg):
@@ -415,10 +390,7 @@ def run_ours(args, cfg, name):
         }
         print(json.dumps(out), flush=True)
     idx.free()
-    if world > 1:
-        import torch.distributed as dist
-
-        dist.destroy_process_group()
+    dist_finish(world)
 
 
 # ------------------------------------------------------------ reference arm

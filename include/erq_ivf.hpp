@@ -1,0 +1,102 @@
+// erq_ivf.hpp - C++ facade of liberq.so with the reference's IVF interface.
+//
+// Header-only; link with -lerq (extended-rabitq_b200/lib/liberq.so).  The class
+// keeps the names, argument meaning and call pattern of the reference's IVF
+// (inc/index/IVF.hpp:62-127) and Rotator (inc/index/Rotator.hpp:9-63) so host
+// code written against them (src/test_search.cpp) keeps its structure:
+//
+//   IVF ivf;  ivf.load(path);                      // IVF::load
+//   ivf.rotator().rotate(queries, nq, rotated);     // Rotator::rotate
+//   ivf.search(&rotated[i * D], nullptr, k, nprobe, results);   // IVF::search
+//
+// Differences a caller sees:
+//   * rotate takes raw row-major buffers instead of Eigen matrices;
+//   * errors throw erq::Error (the reference asserts or aborts);
+//   * search_batch answers many queries in one call (the GPU's fast path);
+//   * building an index (IVF(n, dim, k, b) + construct + save) stays with the
+//     reference's create_index, whose files this class reads.
+#pragma once
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+
+#include "erq.h"
+
+namespace erq {
+
+class Error : public std::runtime_error {
+   public:
+    Error(erq_status s, const std::string& what) : std::runtime_error(what), status(s) {}
+    erq_status status;
+};
+
+inline void check(erq_status s) {
+    if (s != ERQ_OK) throw Error(s, std::string(erq_status_string(s)) + ": " + erq_last_error());
+}
+
+class IVF;
+
+// Rotator::rotate over raw buffers: rotated[nq][D] = pad(queries[nq][DIM]) * P.
+class Rotator {
+   public:
+    void rotate(const float* queries, size_t nq, float* rotated, void* stream = nullptr) const {
+        check(erq_rotate(index_, queries, nq, rotated, stream));
+    }
+    size_t size() const;
+
+   private:
+    friend class IVF;
+    const erq_index* index_ = nullptr;
+    size_t D_ = 0;
+};
+
+inline size_t Rotator::size() const { return D_; }
+
+class IVF {
+   public:
+    IVF() = default;
+    explicit IVF(int device) : device_(device) {}
+    IVF(const IVF&) = delete;
+    IVF& operator=(const IVF&) = delete;
+    ~IVF() { erq_index_free(index_); }
+
+    // IVF::load (inc/index/IVF.hpp:254-293)
+    void load(const char* filename) {
+        erq_index* idx = nullptr;
+        check(erq_index_load(filename, device_, &idx));
+        erq_index_free(index_);
+        index_ = idx;
+        check(erq_index_get_info(index_, &info_));
+        rot_.index_ = index_;
+        rot_.D_ = info_.padded_dim;
+    }
+
+    // IVF::search (inc/index/IVF.hpp:295-324): one rotated query (D floats);
+    // `data` is unused, as in the reference; results gets k ids.
+    void search(const float* query, const float* data, size_t k, size_t nprobe,
+                uint32_t* results) const {
+        (void)data;
+        check(erq_search(index_, query, 1, k, nprobe, results, nullptr, nullptr));
+    }
+
+    // Many rotated queries at once (host or device buffers); dists may be null.
+    void search_batch(const float* queries, size_t nq, size_t k, size_t nprobe, uint32_t* ids,
+                      float* dists = nullptr, void* stream = nullptr) const {
+        check(erq_search(index_, queries, nq, k, nprobe, ids, dists, stream));
+    }
+
+    size_t padded_dim() const { return info_.padded_dim; }  // IVF::padded_dim
+    size_t k() const { return info_.num_clusters; }         // IVF::k
+    size_t size() const { return info_.n; }
+    size_t dim() const { return info_.dim; }
+    Rotator& rotator() { return rot_; }                      // IVF::rotator
+
+   private:
+    int device_ = 0;
+    erq_index* index_ = nullptr;
+    erq_index_info info_{};
+    Rotator rot_;
+};
+
+}  // namespace erq

@@ -1,0 +1,79 @@
+"""The C++ facade (include/erq_ivf.hpp) and the test_search-style driver.
+
+CPU: the facade header compiles and the driver links against liberq.so.
+GPU: on a small seeded dataset (files named as src/test_search.cpp expects),
+the driver's recall column equals the recall of the reference's own
+test_search binary on the same index file, nprobe by nprobe.
+"""
+import csv
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import PKG, REPO
+
+DRIVER = os.path.join(PKG, "bin", "erq_test_search")
+REF_TEST_SEARCH = os.path.join(REPO, "oracle", "_ref", "test_search_strict")
+
+
+def test_facade_header_compiles(tmp_path):
+    src = tmp_path / "t.cpp"
+    src.write_text('#include "erq_ivf.hpp"\nint main() { erq::IVF ivf; return (int)ivf.k(); }\n')
+    subprocess.run(["g++", "-std=c++17", "-fsyntax-only", "-I", os.path.join(REPO, "include"),
+                    str(src)], check=True)
+
+
+def test_driver_builds():
+    subprocess.run(["make", "-s", "-C", PKG, "bin/erq_test_search"], check=True)
+    assert os.access(DRIVER, os.X_OK)
+
+
+def _write_dataset(root, ds, bits):
+    torch = pytest.importorskip("torch")
+    from erq_b200 import build_index, datasets, indexfile, vecs
+
+    d = os.path.join(root, "data", ds)
+    os.makedirs(d, exist_ok=True)
+    base, query = datasets.gaussian_mixture(6000, 128, 32, 0.3, seed=5, n_query=64)
+    cent, ids = datasets.kmeans(base, 64, iters=10, seed=6)
+    gt, _ = datasets.ground_truth(base, query, 100)
+    arr = build_index.build_index_torch(torch.from_numpy(base), torch.from_numpy(cent),
+                                        torch.from_numpy(ids.astype(np.int64)), bits, seed=7)
+    indexfile.write_index(os.path.join(d, f"ivf_exhaf{bits}.index"), arr)
+    vecs.write_vecs(os.path.join(d, f"{ds}_base.fvecs"), base)
+    vecs.write_vecs(os.path.join(d, f"{ds}_query.fvecs"), query)
+    vecs.write_vecs(os.path.join(d, f"{ds}_groundtruth.ivecs"), gt)
+    return d
+
+
+def _read_csv(path):
+    with open(path) as f:
+        return {int(r["nprobe"]): r for r in csv.DictReader(f)}
+
+
+@pytest.mark.gpu
+def test_driver_recall_equals_reference_test_search(tmp_path):
+    subprocess.run(["make", "-s", "-C", PKG, "bin/erq_test_search"], check=True)
+    ds, bits = "tiny128", 5
+    _write_dataset(str(tmp_path), ds, bits)
+    ours = tmp_path / "ours.csv"
+    subprocess.run([DRIVER, str(tmp_path / "data"), ds, str(bits), str(ours)], check=True,
+                   timeout=600)
+    rows = _read_csv(ours)
+    assert rows and all(float(r["QPS"]) > 0 for r in rows.values())
+    assert max(float(r["recall"]) for r in rows.values()) > 0.9
+    if not os.path.exists(REF_TEST_SEARCH):
+        pytest.skip("reference test_search not built")
+    # the unmodified reference driver reads ../data/<ds> and writes ../results
+    os.makedirs(tmp_path / "bin", exist_ok=True)
+    os.makedirs(tmp_path / "results" / "exrabitq", exist_ok=True)
+    subprocess.run([REF_TEST_SEARCH, ds, str(bits)], cwd=tmp_path / "bin", check=True,
+                   stdout=subprocess.DEVNULL, timeout=600)
+    ref = _read_csv(tmp_path / "results" / "exrabitq" / f"{ds}_exhaf{bits}.csv")
+    common = sorted(set(rows) & set(ref))
+    assert common
+    for np_ in common:
+        assert float(rows[np_]["recall"]) == pytest.approx(float(ref[np_]["recall"]), abs=1e-6)
+        assert float(rows[np_]["ratio"]) == pytest.approx(float(ref[np_]["ratio"]), rel=1e-4)
