@@ -15,6 +15,8 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cmath>
+#include <numeric>
+#include <random>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -25,6 +27,7 @@
 #include "../../include/erq_debug.h"
 #include "coarse.cuh"
 #include "gemm.cuh"
+#include "mlp.cuh"
 #include "probe.cuh"
 #include "layout.cuh"
 #include "refine.cuh"
@@ -402,7 +405,7 @@ erq_status load_impl(const char* path, erq_index* idx) {
 size_t scan_smem_bytes(int D) { return 256 + (size_t)(D / 64) * 512 + (size_t)D * 4 + 64; }
 size_t refine_smem_bytes(int D, int k) {
     const int kpad = (k + 31) & ~31;
-    return (size_t)kRefineWarps * refine_warp_smem_bytes(D, kpad);
+    return refine_smem_bytes_per_query(D, kpad);
 }
 int next_pow2(int x) {
     int p = 1;
@@ -473,8 +476,8 @@ int probe_candidates(uint64_t nprobe) {
 
 // Coarse probe on tensor cores: split the rotated queries, estimate all
 // distances with the split-BF16 GEMM, then the exact probe kernel.
-erq_status launch_probe_tc(const erq_index* idx, const Batch& b, uint64_t nprobe,
-                           cudaStream_t st) {
+erq_status launch_probe_tc(const erq_index* idx, const Batch& b, uint64_t nprobe, cudaStream_t st,
+                           float* near_d = nullptr) {
     const int D = (int)idx->D, K = (int)idx->K;
     {
         LaunchTimer t(kSplit, st);
@@ -507,12 +510,16 @@ erq_status launch_probe_tc(const erq_index* idx, const Batch& b, uint64_t nprobe
     a.probe_sqy = b.probe_sqy;
     a.s_off = b.s_off;
     a.fallbacks = nullptr;
+    a.near_d = near_d;
     a.nq = (int)b.nq;
     a.K = K;
     a.Kpow2 = next_pow2(K);
     a.D = D;
     a.nprobe = (int)nprobe;
-    a.M = probe_candidates(nprobe);
+    // with features requested the 64 nearest distances are proven exact too
+    a.check_rank = near_d ? (int)std::max<uint64_t>(nprobe, std::min<uint64_t>(kFeatDists, K))
+                          : (int)nprobe;
+    a.M = probe_candidates(a.check_rank);
     LaunchTimer t(kProbe, st);
     probe_kernel<<<(unsigned)b.nq, kProbeThreads, probe_smem_bytes(D, K, a.Kpow2), st>>>(a);
     t.finish();
@@ -539,7 +546,8 @@ erq_status launch_probe(const erq_index* idx, const Batch& b, uint64_t nprobe, c
     return ERQ_OK;
 }
 
-erq_status launch_scan(const erq_index* idx, const Batch& b, uint64_t nprobe, cudaStream_t st) {
+erq_status launch_scan(const erq_index* idx, const Batch& b, uint64_t nprobe, cudaStream_t st,
+                       const int* q_nprobe = nullptr) {
     ScanArgs a;
     a.qrot = b.qrot;
     a.centroids = idx->centroids;
@@ -552,6 +560,7 @@ erq_status launch_scan(const erq_index* idx, const Batch& b, uint64_t nprobe, cu
     a.S = b.S;
     a.qp_delta = b.delta;
     a.qp_sumq = b.sumq;
+    a.q_nprobe = q_nprobe;
     a.D = (int)idx->D;
     a.nprobe = (int)nprobe;
     const uint64_t pairs = b.nq * nprobe;
@@ -564,7 +573,8 @@ erq_status launch_scan(const erq_index* idx, const Batch& b, uint64_t nprobe, cu
 }
 
 erq_status launch_refine(const erq_index* idx, const Batch& b, uint64_t nprobe, uint64_t k,
-                         uint32_t* out_ids, float* out_dists, cudaStream_t st) {
+                         uint32_t* out_ids, float* out_dists, cudaStream_t st,
+                         const int* q_nprobe = nullptr) {
     RefineArgs a;
     a.qrot = b.qrot;
     a.centroids = idx->centroids;
@@ -583,21 +593,22 @@ erq_status launch_refine(const erq_index* idx, const Batch& b, uint64_t nprobe, 
     a.c_size = idx->c_size;
     a.out_ids = out_ids;
     a.out_dists = out_dists;
+    a.q_nprobe = q_nprobe;
     a.nq = (int)b.nq;
     a.D = (int)idx->D;
     a.EX = (int)idx->EX;
     a.nprobe = (int)nprobe;
     a.k = (int)k;
-    const unsigned grid = (unsigned)div_up(b.nq, kRefineWarps);
+    const unsigned grid = (unsigned)b.nq;
     const size_t smem = refine_smem_bytes(a.D, a.k);
     LaunchTimer t(kRefine, st);
     switch (idx->EX) {
-        case 2: refine_kernel<2><<<grid, kRefineWarps * 32, smem, st>>>(a); break;
-        case 3: refine_kernel<3><<<grid, kRefineWarps * 32, smem, st>>>(a); break;
-        case 4: refine_kernel<4><<<grid, kRefineWarps * 32, smem, st>>>(a); break;
-        case 6: refine_kernel<6><<<grid, kRefineWarps * 32, smem, st>>>(a); break;
-        case 7: refine_kernel<7><<<grid, kRefineWarps * 32, smem, st>>>(a); break;
-        case 8: refine_kernel<8><<<grid, kRefineWarps * 32, smem, st>>>(a); break;
+        case 2: refine_kernel<2><<<grid, kRefineThreads, smem, st>>>(a); break;
+        case 3: refine_kernel<3><<<grid, kRefineThreads, smem, st>>>(a); break;
+        case 4: refine_kernel<4><<<grid, kRefineThreads, smem, st>>>(a); break;
+        case 6: refine_kernel<6><<<grid, kRefineThreads, smem, st>>>(a); break;
+        case 7: refine_kernel<7><<<grid, kRefineThreads, smem, st>>>(a); break;
+        case 8: refine_kernel<8><<<grid, kRefineThreads, smem, st>>>(a); break;
         default: return fail(ERQ_ERR_FORMAT, "bad EX");
     }
     t.finish();
@@ -705,6 +716,149 @@ erq_status search_entry(const erq_index* idx, const float* queries, bool rotated
     if (!d_dev)
         ERQ_CUDA(cudaMemcpyAsync(dists, d_out, nq * k * sizeof(float), cudaMemcpyDeviceToHost, st));
     if (host_io) ERQ_CUDA(cudaStreamSynchronize(st));
+    return ERQ_OK;
+}
+
+}  // namespace
+
+
+// ----------------------------------------------------------- learned probing
+struct erq_probe_model {
+    int device = 0;
+    float* w = nullptr;             // [kMlpParams] FP32 master weights
+    __nv_bfloat16* wb = nullptr;    // [kMlpParams] BF16 copy used by the forward pass
+    float* mean = nullptr;          // [kMlpIn] feature standardisation
+    float* stdv = nullptr;          // [kMlpIn]
+    int* bins_dev = nullptr;        // [kMlpBins] probe count of each class
+    int bins[kMlpBins] = {};
+
+    ~erq_probe_model() {
+        int prev = -1;
+        cudaGetDevice(&prev);
+        cudaSetDevice(device);
+        for (void* p : {(void*)w, (void*)wb, (void*)mean, (void*)stdv, (void*)bins_dev})
+            if (p) cudaFree(p);
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+namespace {
+
+template <typename TB>
+erq_status mlp_mm(const float* A, long sam, long sak, const TB* B, long sbk, long sbn, float* C,
+                  int M, int N, int K, const float* bias, bool relu, cudaStream_t st) {
+    dim3 grid((unsigned)div_up(N, 16), (unsigned)div_up(M, 16));
+    mlp_matmul_kernel<TB><<<grid, 256, 0, st>>>(A, sam, sak, B, sbk, sbn, C, M, N, K, bias, relu,
+                                                false);
+    ERQ_CUDA(cudaGetLastError());
+    return ERQ_OK;
+}
+
+// Activations of one batch.
+struct MlpWork {
+    float* x = nullptr;   // [B][320] standardised features
+    float* h1 = nullptr;  // [B][256]
+    float* h2 = nullptr;  // [B][256]
+    float* z = nullptr;   // [B][8]
+    float* probs = nullptr;
+    float* dz = nullptr;
+    float* dh2 = nullptr;
+    float* dh1 = nullptr;
+    float* loss = nullptr;  // [B]
+};
+
+erq_status mlp_alloc(Scratch& s, int B, bool train, MlpWork& w) {
+    ERQ_TRY(s.alloc(&w.x, (size_t)B * kMlpIn));
+    ERQ_TRY(s.alloc(&w.h1, (size_t)B * kMlpHidden));
+    ERQ_TRY(s.alloc(&w.h2, (size_t)B * kMlpHidden));
+    ERQ_TRY(s.alloc(&w.z, (size_t)B * kMlpBins));
+    ERQ_TRY(s.alloc(&w.probs, (size_t)B * kMlpBins));
+    if (train) {
+        ERQ_TRY(s.alloc(&w.dz, (size_t)B * kMlpBins));
+        ERQ_TRY(s.alloc(&w.dh2, (size_t)B * kMlpHidden));
+        ERQ_TRY(s.alloc(&w.dh1, (size_t)B * kMlpHidden));
+        ERQ_TRY(s.alloc(&w.loss, (size_t)B));
+    }
+    return ERQ_OK;
+}
+
+// logits z = W3 relu(W2 relu(W1 x + b1) + b2) + b3, BF16 weights, FP32 sums.
+erq_status mlp_forward(const erq_probe_model* m, const MlpWork& w, int B, cudaStream_t st) {
+    ERQ_TRY(mlp_mm(w.x, kMlpIn, 1, m->wb + kW1, 1, kMlpIn, w.h1, B, kMlpHidden, kMlpIn,
+                   m->w + kB1, true, st));
+    ERQ_TRY(mlp_mm(w.h1, kMlpHidden, 1, m->wb + kW2, 1, kMlpHidden, w.h2, B, kMlpHidden,
+                   kMlpHidden, m->w + kB2, true, st));
+    ERQ_TRY(mlp_mm(w.h2, kMlpHidden, 1, m->wb + kW3, 1, kMlpHidden, w.z, B, kMlpBins, kMlpHidden,
+                   m->w + kB3, false, st));
+    return ERQ_OK;
+}
+
+// Gradients of the mean cross-entropy into g (parameter layout of mlp.cuh).
+erq_status mlp_backward(const erq_probe_model* m, const MlpWork& w, int B, float* g,
+                        cudaStream_t st) {
+    // output layer
+    ERQ_TRY(mlp_mm(w.dz, 1, kMlpBins, w.h2, kMlpHidden, 1, g + kW3, kMlpBins, kMlpHidden, B,
+                   (const float*)nullptr, false, st));
+    mlp_bias_grad_kernel<<<1, 32, 0, st>>>(w.dz, B, kMlpBins, g + kB3);
+    ERQ_TRY(mlp_mm(w.dz, kMlpBins, 1, m->wb + kW3, kMlpHidden, 1, w.dh2, B, kMlpHidden, kMlpBins,
+                   (const float*)nullptr, false, st));
+    mlp_relu_grad_kernel<<<(unsigned)div_up((uint64_t)B * kMlpHidden, 256), 256, 0, st>>>(
+        w.dh2, w.h2, B * kMlpHidden);
+    // second layer
+    ERQ_TRY(mlp_mm(w.dh2, 1, kMlpHidden, w.h1, kMlpHidden, 1, g + kW2, kMlpHidden, kMlpHidden, B,
+                   (const float*)nullptr, false, st));
+    mlp_bias_grad_kernel<<<1, kMlpHidden, 0, st>>>(w.dh2, B, kMlpHidden, g + kB2);
+    ERQ_TRY(mlp_mm(w.dh2, kMlpHidden, 1, m->wb + kW2, kMlpHidden, 1, w.dh1, B, kMlpHidden,
+                   kMlpHidden, (const float*)nullptr, false, st));
+    mlp_relu_grad_kernel<<<(unsigned)div_up((uint64_t)B * kMlpHidden, 256), 256, 0, st>>>(
+        w.dh1, w.h1, B * kMlpHidden);
+    // first layer
+    ERQ_TRY(mlp_mm(w.dh1, 1, kMlpHidden, w.x, kMlpIn, 1, g + kW1, kMlpHidden, kMlpIn, B,
+                   (const float*)nullptr, false, st));
+    mlp_bias_grad_kernel<<<1, kMlpHidden, 0, st>>>(w.dh1, B, kMlpHidden, g + kB1);
+    ERQ_CUDA(cudaGetLastError());
+    return ERQ_OK;
+}
+
+__global__ void mlp_gather_rows_kernel(const float* __restrict__ X, const uint8_t* __restrict__ y,
+                                       const uint32_t* __restrict__ perm, int B,
+                                       float* __restrict__ xb, uint8_t* __restrict__ yb) {
+    const int r = blockIdx.x;
+    if (r >= B) return;
+    const uint32_t src = perm[r];
+    for (int c = threadIdx.x; c < kMlpIn; c += blockDim.x)
+        xb[(size_t)r * kMlpIn + c] = X[(size_t)src * kMlpIn + c];
+    if (threadIdx.x == 0) yb[r] = y[src];
+}
+
+erq_status model_alloc(erq_probe_model* m) {
+    ERQ_CUDA(cudaMalloc(&m->w, sizeof(float) * kMlpParams));
+    ERQ_CUDA(cudaMalloc(&m->wb, sizeof(__nv_bfloat16) * kMlpParams));
+    ERQ_CUDA(cudaMalloc(&m->mean, sizeof(float) * kMlpIn));
+    ERQ_CUDA(cudaMalloc(&m->stdv, sizeof(float) * kMlpIn));
+    ERQ_CUDA(cudaMalloc(&m->bins_dev, sizeof(int) * kMlpBins));
+    return ERQ_OK;
+}
+
+erq_status model_upload(erq_probe_model* m, const std::vector<float>& w,
+                        const std::vector<float>& mean, const std::vector<float>& stdv) {
+    ERQ_CUDA(cudaMemcpy(m->w, w.data(), sizeof(float) * kMlpParams, cudaMemcpyHostToDevice));
+    ERQ_CUDA(cudaMemcpy(m->mean, mean.data(), sizeof(float) * kMlpIn, cudaMemcpyHostToDevice));
+    ERQ_CUDA(cudaMemcpy(m->stdv, stdv.data(), sizeof(float) * kMlpIn, cudaMemcpyHostToDevice));
+    ERQ_CUDA(cudaMemcpy(m->bins_dev, m->bins, sizeof(int) * kMlpBins, cudaMemcpyHostToDevice));
+    mlp_to_bf16_kernel<<<(unsigned)div_up(kMlpParams, 256), 256>>>(m->w, m->wb, kMlpParams);
+    ERQ_CUDA(cudaGetLastError());
+    ERQ_CUDA(cudaDeviceSynchronize());
+    return ERQ_OK;
+}
+
+// Probe features of a batch of rotated queries on the device.
+erq_status features_device(const erq_index* idx, const Batch& b, uint64_t nprobe, float* near_d,
+                           float* feats, cudaStream_t st) {
+    ERQ_TRY(launch_probe_tc(idx, b, nprobe, st, near_d));
+    probe_features_kernel<<<(unsigned)b.nq, 128, 0, st>>>(b.qrot, (int)idx->D, near_d,
+                                                         (int)b.nq, feats);
+    ERQ_CUDA(cudaGetLastError());
     return ERQ_OK;
 }
 
@@ -977,6 +1131,414 @@ erq_status erq_debug_scan(const erq_index* idx, const float* qrot, uint64_t nq, 
     ERQ_CUDA(cudaMemcpyAsync(s_offsets, b.s_off, np * 8, cudaMemcpyDeviceToHost, st));
     ERQ_CUDA(cudaMemcpyAsync(S, b.S, need * 4, cudaMemcpyDeviceToHost, st));
     ERQ_CUDA(cudaStreamSynchronize(st));
+    return ERQ_OK;
+}
+
+
+// ------------------------------------------------------------ learned probing
+erq_status erq_probe_features(const erq_index* idx, const float* rotated_queries, uint64_t nq,
+                              float* features, void* stream) {
+    if (!idx || !rotated_queries || !features) return fail(ERQ_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (nq == 0) return ERQ_OK;
+    DeviceGuard guard;
+    ERQ_TRY(guard.set(idx->device));
+    ERQ_TRY(configure_kernels((int)idx->D, (int)idx->K, 1));
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const bool q_dev = is_device_ptr(rotated_queries), f_dev = is_device_ptr(features);
+    Scratch s(st, idx->pool);
+    const float* q = rotated_queries;
+    if (!q_dev || (reinterpret_cast<uintptr_t>(q) & 15)) {
+        float* tmp = nullptr;
+        ERQ_TRY(s.alloc(&tmp, nq * idx->D));
+        ERQ_CUDA(cudaMemcpyAsync(tmp, rotated_queries, nq * idx->D * 4, cudaMemcpyDefault, st));
+        q = tmp;
+    }
+    float* fout = features;
+    if (!f_dev) ERQ_TRY(s.alloc(&fout, nq * kMlpIn));
+    const uint64_t nprobe = 1;
+    const uint64_t bq = batch_queries(idx, std::max<uint64_t>(nprobe, 1), nq);
+    Batch b;
+    ERQ_TRY(alloc_batch(s, idx, bq, nprobe, b));
+    float* near_d = nullptr;
+    ERQ_TRY(s.alloc(&near_d, bq * kFeatDists));
+    for (uint64_t q0 = 0; q0 < nq; q0 += bq) {
+        b.nq = std::min(bq, nq - q0);
+        b.qrot = q + q0 * idx->D;
+        ERQ_TRY(features_device(idx, b, nprobe, near_d, fout + q0 * kMlpIn, st));
+    }
+    if (!f_dev) {
+        ERQ_CUDA(cudaMemcpyAsync(features, fout, nq * kMlpIn * 4, cudaMemcpyDeviceToHost, st));
+        ERQ_CUDA(cudaStreamSynchronize(st));
+    } else if (!q_dev) {
+        ERQ_CUDA(cudaStreamSynchronize(st));
+    }
+    return ERQ_OK;
+}
+
+erq_status erq_probe_model_train(const float* features, const uint8_t* labels, uint64_t n,
+                                 const uint32_t* bin_nprobe, int epochs, int batch, float lr,
+                                 uint64_t seed, int device, erq_probe_model** out,
+                                 float* final_loss) {
+    if (!features || !labels || !bin_nprobe || !out) return fail(ERQ_ERR_INVALID_ARGUMENT, "NULL argument");
+    *out = nullptr;
+    if (n < 2 || epochs < 1 || batch < 1 || !(lr > 0.f))
+        return fail(ERQ_ERR_INVALID_ARGUMENT, "need n >= 2, epochs >= 1, batch >= 1, lr > 0");
+    for (int j = 0; j < kMlpBins; ++j)
+        if (bin_nprobe[j] < 1 || (j > 0 && bin_nprobe[j] <= bin_nprobe[j - 1]))
+            return fail(ERQ_ERR_INVALID_ARGUMENT, "bin_nprobe must be increasing and >= 1");
+    for (uint64_t i = 0; i < n; ++i)
+        if (labels[i] >= kMlpBins) return fail(ERQ_ERR_INVALID_ARGUMENT, "label >= %d", kMlpBins);
+    DeviceGuard guard;
+    ERQ_TRY(guard.set(device));
+    std::unique_ptr<erq_probe_model> m(new (std::nothrow) erq_probe_model());
+    if (!m) return fail(ERQ_ERR_OUT_OF_MEMORY, "host allocation failed");
+    m->device = device;
+    for (int j = 0; j < kMlpBins; ++j) m->bins[j] = (int)bin_nprobe[j];
+    ERQ_TRY(model_alloc(m.get()));
+    // standardisation statistics (float64 on the host)
+    std::vector<double> mu(kMlpIn, 0.0), var(kMlpIn, 0.0);
+    for (uint64_t i = 0; i < n; ++i)
+        for (int c = 0; c < kMlpIn; ++c) mu[c] += features[i * kMlpIn + c];
+    for (int c = 0; c < kMlpIn; ++c) mu[c] /= (double)n;
+    for (uint64_t i = 0; i < n; ++i)
+        for (int c = 0; c < kMlpIn; ++c) {
+            const double d = features[i * kMlpIn + c] - mu[c];
+            var[c] += d * d;
+        }
+    std::vector<float> mean(kMlpIn), stdv(kMlpIn);
+    for (int c = 0; c < kMlpIn; ++c) {
+        mean[c] = (float)mu[c];
+        stdv[c] = (float)std::max(std::sqrt(var[c] / (double)n), 1e-6);
+    }
+    // initial weights: uniform(-1/sqrt(fan_in), 1/sqrt(fan_in)), zero biases
+    std::mt19937_64 rng(seed);
+    std::vector<float> w(kMlpParams, 0.f);
+    auto init = [&](int off, int rows, int cols) {
+        std::uniform_real_distribution<float> u(-1.f / std::sqrt((float)cols), 1.f / std::sqrt((float)cols));
+        for (int i = 0; i < rows * cols; ++i) w[off + i] = u(rng);
+    };
+    init(kW1, kMlpHidden, kMlpIn);
+    init(kW2, kMlpHidden, kMlpHidden);
+    init(kW3, kMlpBins, kMlpHidden);
+    ERQ_TRY(model_upload(m.get(), w, mean, stdv));
+    // the whole standardised training set on the device
+    cudaStream_t st = nullptr;
+    ERQ_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    struct StreamCloser {
+        cudaStream_t s;
+        ~StreamCloser() { cudaStreamDestroy(s); }
+    } closer{st};
+    float *X = nullptr, *Xraw = nullptr, *g = nullptr, *m1 = nullptr, *m2 = nullptr;
+    uint8_t *Y = nullptr, *yb = nullptr;
+    uint32_t* perm_d = nullptr;
+    struct Frees {
+        std::vector<void*> p;
+        ~Frees() {
+            for (void* x : p) cudaFree(x);
+        }
+    } frees;
+    auto dmalloc = [&](void** p, size_t bytes) -> erq_status {
+        ERQ_CUDA(cudaMalloc(p, std::max<size_t>(bytes, 16)));
+        frees.p.push_back(*p);
+        return ERQ_OK;
+    };
+    ERQ_TRY(dmalloc((void**)&Xraw, n * kMlpIn * 4));
+    ERQ_TRY(dmalloc((void**)&X, n * kMlpIn * 4));
+    ERQ_TRY(dmalloc((void**)&Y, n));
+    ERQ_TRY(dmalloc((void**)&g, kMlpParams * 4));
+    ERQ_TRY(dmalloc((void**)&m1, kMlpParams * 4));
+    ERQ_TRY(dmalloc((void**)&m2, kMlpParams * 4));
+    ERQ_TRY(dmalloc((void**)&perm_d, n * 4));
+    ERQ_TRY(dmalloc((void**)&yb, (size_t)batch));
+    ERQ_CUDA(cudaMemcpy(Xraw, features, n * kMlpIn * 4, cudaMemcpyHostToDevice));
+    ERQ_CUDA(cudaMemcpy(Y, labels, n, cudaMemcpyHostToDevice));
+    ERQ_CUDA(cudaMemsetAsync(m1, 0, kMlpParams * 4, st));
+    ERQ_CUDA(cudaMemsetAsync(m2, 0, kMlpParams * 4, st));
+    mlp_standardise_kernel<<<(unsigned)div_up(n * kMlpIn, 256), 256, 0, st>>>(Xraw, m->mean, m->stdv,
+                                                                            X, (int)(n * kMlpIn));
+    ERQ_CUDA(cudaGetLastError());
+    MlpWork wk;
+    {
+        float* p = nullptr;
+        ERQ_TRY(dmalloc((void**)&p, (size_t)batch * kMlpIn * 4)); wk.x = p;
+        ERQ_TRY(dmalloc((void**)&p, (size_t)batch * kMlpHidden * 4)); wk.h1 = p;
+        ERQ_TRY(dmalloc((void**)&p, (size_t)batch * kMlpHidden * 4)); wk.h2 = p;
+        ERQ_TRY(dmalloc((void**)&p, (size_t)batch * kMlpBins * 4)); wk.z = p;
+        ERQ_TRY(dmalloc((void**)&p, (size_t)batch * kMlpBins * 4)); wk.probs = p;
+        ERQ_TRY(dmalloc((void**)&p, (size_t)batch * kMlpBins * 4)); wk.dz = p;
+        ERQ_TRY(dmalloc((void**)&p, (size_t)batch * kMlpHidden * 4)); wk.dh2 = p;
+        ERQ_TRY(dmalloc((void**)&p, (size_t)batch * kMlpHidden * 4)); wk.dh1 = p;
+        ERQ_TRY(dmalloc((void**)&p, (size_t)batch * 4)); wk.loss = p;
+    }
+    std::vector<uint32_t> perm(n);
+    std::vector<float> loss_h(batch);
+    const float beta1 = 0.9f, beta2 = 0.999f, eps = 1e-8f;
+    int t = 0;
+    double last = 0.0;
+    for (int e = 0; e < epochs; ++e) {
+        std::iota(perm.begin(), perm.end(), 0u);
+        std::shuffle(perm.begin(), perm.end(), rng);
+        ERQ_CUDA(cudaMemcpyAsync(perm_d, perm.data(), n * 4, cudaMemcpyHostToDevice, st));
+        double sum = 0.0;
+        uint64_t seen = 0;
+        for (uint64_t b0 = 0; b0 + 1 < n; b0 += batch) {
+            const int B = (int)std::min<uint64_t>(batch, n - b0);
+            mlp_gather_rows_kernel<<<B, 128, 0, st>>>(X, Y, perm_d + b0, B, wk.x, yb);
+            ERQ_TRY(mlp_forward(m.get(), wk, B, st));
+            mlp_softmax_xent_kernel<<<(unsigned)div_up(B, 128), 128, 0, st>>>(wk.z, yb, B, wk.probs,
+                                                                             wk.dz, wk.loss);
+            ERQ_TRY(mlp_backward(m.get(), wk, B, g, st));
+            ++t;
+            const float bc1 = 1.f - std::pow(beta1, (float)t), bc2 = 1.f - std::pow(beta2, (float)t);
+            mlp_adam_kernel<<<(unsigned)div_up(kMlpParams, 256), 256, 0, st>>>(
+                m->w, g, m1, m2, m->wb, kMlpParams, lr, beta1, beta2, eps, bc1, bc2);
+            ERQ_CUDA(cudaGetLastError());
+            if (e == epochs - 1) {
+                ERQ_CUDA(cudaMemcpyAsync(loss_h.data(), wk.loss, B * 4, cudaMemcpyDeviceToHost, st));
+                ERQ_CUDA(cudaStreamSynchronize(st));
+                for (int r = 0; r < B; ++r) sum += loss_h[r];
+                seen += B;
+            }
+        }
+        if (e == epochs - 1) last = seen ? sum / seen : 0.0;
+    }
+    ERQ_CUDA(cudaStreamSynchronize(st));
+    if (final_loss) *final_loss = (float)last;
+    *out = m.release();
+    return ERQ_OK;
+}
+
+static const char kModelMagic[8] = {'E', 'R', 'Q', 'P', 'R', 'O', 'B', '1'};
+
+erq_status erq_probe_model_save(const erq_probe_model* m, const char* path) {
+    if (!m || !path) return fail(ERQ_ERR_INVALID_ARGUMENT, "NULL argument");
+    DeviceGuard guard;
+    ERQ_TRY(guard.set(m->device));
+    std::vector<float> w(kMlpParams), mean(kMlpIn), stdv(kMlpIn);
+    ERQ_CUDA(cudaMemcpy(w.data(), m->w, kMlpParams * 4, cudaMemcpyDeviceToHost));
+    ERQ_CUDA(cudaMemcpy(mean.data(), m->mean, kMlpIn * 4, cudaMemcpyDeviceToHost));
+    ERQ_CUDA(cudaMemcpy(stdv.data(), m->stdv, kMlpIn * 4, cudaMemcpyDeviceToHost));
+    std::unique_ptr<FILE, FileCloser> f(fopen(path, "wb"));
+    if (!f) return fail(ERQ_ERR_IO, "cannot write '%s'", path);
+    const int32_t dims[3] = {kMlpIn, kMlpHidden, kMlpBins};
+    bool ok = fwrite(kModelMagic, 1, 8, f.get()) == 8 && fwrite(dims, 4, 3, f.get()) == 3 &&
+              fwrite(m->bins, 4, kMlpBins, f.get()) == (size_t)kMlpBins &&
+              fwrite(mean.data(), 4, kMlpIn, f.get()) == (size_t)kMlpIn &&
+              fwrite(stdv.data(), 4, kMlpIn, f.get()) == (size_t)kMlpIn &&
+              fwrite(w.data(), 4, kMlpParams, f.get()) == (size_t)kMlpParams;
+    return ok ? ERQ_OK : fail(ERQ_ERR_IO, "short write to '%s'", path);
+}
+
+erq_status erq_probe_model_load(const char* path, int device, erq_probe_model** out) {
+    if (!path || !out) return fail(ERQ_ERR_INVALID_ARGUMENT, "NULL argument");
+    *out = nullptr;
+    std::unique_ptr<FILE, FileCloser> f(fopen(path, "rb"));
+    if (!f) return fail(ERQ_ERR_IO, "cannot open '%s'", path);
+    char magic[8];
+    int32_t dims[3];
+    std::unique_ptr<erq_probe_model> m(new (std::nothrow) erq_probe_model());
+    if (!m) return fail(ERQ_ERR_OUT_OF_MEMORY, "host allocation failed");
+    std::vector<float> w(kMlpParams), mean(kMlpIn), stdv(kMlpIn);
+    if (fread(magic, 1, 8, f.get()) != 8 || memcmp(magic, kModelMagic, 8) != 0)
+        return fail(ERQ_ERR_FORMAT, "'%s' is not a probe model", path);
+    if (fread(dims, 4, 3, f.get()) != 3 || dims[0] != kMlpIn || dims[1] != kMlpHidden ||
+        dims[2] != kMlpBins)
+        return fail(ERQ_ERR_FORMAT, "probe model dimensions do not match");
+    if (fread(m->bins, 4, kMlpBins, f.get()) != (size_t)kMlpBins ||
+        fread(mean.data(), 4, kMlpIn, f.get()) != (size_t)kMlpIn ||
+        fread(stdv.data(), 4, kMlpIn, f.get()) != (size_t)kMlpIn ||
+        fread(w.data(), 4, kMlpParams, f.get()) != (size_t)kMlpParams)
+        return fail(ERQ_ERR_FORMAT, "probe model file truncated");
+    DeviceGuard guard;
+    ERQ_TRY(guard.set(device));
+    m->device = device;
+    ERQ_TRY(model_alloc(m.get()));
+    ERQ_TRY(model_upload(m.get(), w, mean, stdv));
+    *out = m.release();
+    return ERQ_OK;
+}
+
+void erq_probe_model_free(erq_probe_model* m) { delete m; }
+
+erq_status erq_probe_model_predict(const erq_probe_model* m, const float* features, uint64_t n,
+                                   float* probs, void* stream) {
+    if (!m || !features || !probs) return fail(ERQ_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (n == 0) return ERQ_OK;
+    DeviceGuard guard;
+    ERQ_TRY(guard.set(m->device));
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    float *fin = nullptr, *pout = nullptr;
+    std::vector<void*> owned;
+    struct Frees {
+        std::vector<void*>& p;
+        ~Frees() {
+            for (void* x : p) cudaFree(x);
+        }
+    } frees{owned};
+    const bool f_dev = is_device_ptr(features), p_dev = is_device_ptr(probs);
+    if (!f_dev) {
+        ERQ_CUDA(cudaMalloc(&fin, n * kMlpIn * 4));
+        owned.push_back(fin);
+        ERQ_CUDA(cudaMemcpyAsync(fin, features, n * kMlpIn * 4, cudaMemcpyHostToDevice, st));
+    } else {
+        fin = const_cast<float*>(features);
+    }
+    if (!p_dev) {
+        ERQ_CUDA(cudaMalloc(&pout, n * kMlpBins * 4));
+        owned.push_back(pout);
+    } else {
+        pout = probs;
+    }
+    MlpWork wk;
+    for (float** p : {&wk.x, &wk.h1, &wk.h2, &wk.z}) {
+        const size_t cols = p == &wk.x ? kMlpIn : (p == &wk.z ? kMlpBins : kMlpHidden);
+        ERQ_CUDA(cudaMalloc(p, n * cols * 4));
+        owned.push_back(*p);
+    }
+    mlp_standardise_kernel<<<(unsigned)div_up(n * kMlpIn, 256), 256, 0, st>>>(fin, m->mean, m->stdv,
+                                                                            wk.x, (int)(n * kMlpIn));
+    ERQ_TRY(mlp_forward(m, wk, (int)n, st));
+    mlp_softmax_xent_kernel<<<(unsigned)div_up(n, 128), 128, 0, st>>>(wk.z, nullptr, (int)n, pout,
+                                                                     nullptr, nullptr);
+    ERQ_CUDA(cudaGetLastError());
+    if (!p_dev) ERQ_CUDA(cudaMemcpyAsync(probs, pout, n * kMlpBins * 4, cudaMemcpyDeviceToHost, st));
+    ERQ_CUDA(cudaStreamSynchronize(st));
+    return ERQ_OK;
+}
+
+erq_status erq_search_learned(const erq_index* idx, const erq_probe_model* m,
+                              const float* rotated_queries, uint64_t nq, uint64_t k,
+                              uint64_t nprobe_fallback, float confidence, float min_prob,
+                              uint32_t* ids, float* dists, uint32_t* nprobe_used, void* stream) {
+    if (!m) return fail(ERQ_ERR_INVALID_ARGUMENT, "model is NULL");
+    ERQ_TRY(check_search_args(idx, nq, k, nprobe_fallback, rotated_queries, ids));
+    if (nq == 0) return ERQ_OK;
+    if (m->device != idx->device)
+        return fail(ERQ_ERR_INVALID_ARGUMENT, "model and index are on different devices");
+    if (!(confidence > 0.f && confidence <= 1.f))
+        return fail(ERQ_ERR_INVALID_ARGUMENT, "confidence must be in (0, 1]");
+    DeviceGuard guard;
+    ERQ_TRY(guard.set(idx->device));
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const uint64_t nprobe_max =
+        std::min<uint64_t>(idx->K, std::max<uint64_t>(nprobe_fallback, (uint64_t)m->bins[kMlpBins - 1]));
+    ERQ_TRY(configure_kernels((int)idx->D, (int)idx->K, (int)k));
+    const bool q_dev = is_device_ptr(rotated_queries), ids_dev = is_device_ptr(ids);
+    const bool d_dev = dists == nullptr || is_device_ptr(dists);
+    const bool u_dev = nprobe_used == nullptr || is_device_ptr(nprobe_used);
+    Scratch s(st, idx->pool);
+    const float* q = rotated_queries;
+    if (!q_dev || (reinterpret_cast<uintptr_t>(q) & 15)) {
+        float* tmp = nullptr;
+        ERQ_TRY(s.alloc(&tmp, nq * idx->D));
+        ERQ_CUDA(cudaMemcpyAsync(tmp, rotated_queries, nq * idx->D * 4, cudaMemcpyDefault, st));
+        q = tmp;
+    }
+    uint32_t* ids_out = ids;
+    float* d_out = dists;
+    int* used = nullptr;
+    if (!ids_dev) ERQ_TRY(s.alloc(&ids_out, nq * k));
+    if (!d_dev) ERQ_TRY(s.alloc(&d_out, nq * k));
+    ERQ_TRY(s.alloc(&used, nq));
+    const uint64_t bq = batch_queries(idx, nprobe_max, nq);
+    Batch b;
+    ERQ_TRY(alloc_batch(s, idx, bq, nprobe_max, b));
+    float *near_d = nullptr, *feats = nullptr;
+    ERQ_TRY(s.alloc(&near_d, bq * kFeatDists));
+    ERQ_TRY(s.alloc(&feats, bq * kMlpIn));
+    MlpWork wk;
+    ERQ_TRY(mlp_alloc(s, (int)bq, false, wk));
+    for (uint64_t q0 = 0; q0 < nq; q0 += bq) {
+        b.nq = std::min(bq, nq - q0);
+        b.qrot = q + q0 * idx->D;
+        const int B = (int)b.nq;
+        ERQ_TRY(features_device(idx, b, nprobe_max, near_d, feats, st));
+        mlp_standardise_kernel<<<(unsigned)div_up((uint64_t)B * kMlpIn, 256), 256, 0, st>>>(
+            feats, m->mean, m->stdv, wk.x, B * kMlpIn);
+        ERQ_TRY(mlp_forward(m, wk, B, st));
+        mlp_softmax_xent_kernel<<<(unsigned)div_up(B, 128), 128, 0, st>>>(wk.z, nullptr, B,
+                                                                         wk.probs, nullptr, nullptr);
+        mlp_choose_nprobe_kernel<<<(unsigned)div_up(B, 128), 128, 0, st>>>(
+            wk.probs, B, m->bins_dev, confidence, min_prob, (int)nprobe_fallback, (int)nprobe_max,
+            used + q0);
+        ERQ_CUDA(cudaGetLastError());
+        ERQ_TRY(launch_scan(idx, b, nprobe_max, st, used + q0));
+        ERQ_TRY(launch_refine(idx, b, nprobe_max, k, ids_out + q0 * k,
+                              d_out ? d_out + q0 * k : nullptr, st, used + q0));
+    }
+    if (nprobe_used)
+        ERQ_CUDA(cudaMemcpyAsync(nprobe_used, used, nq * 4, cudaMemcpyDefault, st));
+    if (!ids_dev)
+        ERQ_CUDA(cudaMemcpyAsync(ids, ids_out, nq * k * 4, cudaMemcpyDeviceToHost, st));
+    if (!d_dev)
+        ERQ_CUDA(cudaMemcpyAsync(dists, d_out, nq * k * 4, cudaMemcpyDeviceToHost, st));
+    if (!q_dev || !ids_dev || !d_dev || !u_dev) ERQ_CUDA(cudaStreamSynchronize(st));
+    return ERQ_OK;
+}
+
+erq_status erq_debug_probe_model_grads(const erq_probe_model* m, const float* features,
+                                       const uint8_t* labels, uint64_t n, float* loss,
+                                       float* grads) {
+    if (!m || !features || !labels || !loss || !grads)
+        return fail(ERQ_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (n == 0 || n > 65536) return fail(ERQ_ERR_INVALID_ARGUMENT, "n must be in [1, 65536]");
+    DeviceGuard guard;
+    ERQ_TRY(guard.set(m->device));
+    std::vector<void*> owned;
+    struct Frees {
+        std::vector<void*>& p;
+        ~Frees() {
+            for (void* x : p) cudaFree(x);
+        }
+    } frees{owned};
+    auto dm = [&](void** p, size_t bytes) -> erq_status {
+        ERQ_CUDA(cudaMalloc(p, std::max<size_t>(bytes, 16)));
+        owned.push_back(*p);
+        return ERQ_OK;
+    };
+    float *fin = nullptr, *g = nullptr;
+    uint8_t* y = nullptr;
+    MlpWork wk;
+    ERQ_TRY(dm((void**)&fin, n * kMlpIn * 4));
+    ERQ_TRY(dm((void**)&y, n));
+    ERQ_TRY(dm((void**)&g, kMlpParams * 4));
+    ERQ_TRY(dm((void**)&wk.x, n * kMlpIn * 4));
+    ERQ_TRY(dm((void**)&wk.h1, n * kMlpHidden * 4));
+    ERQ_TRY(dm((void**)&wk.h2, n * kMlpHidden * 4));
+    ERQ_TRY(dm((void**)&wk.z, n * kMlpBins * 4));
+    ERQ_TRY(dm((void**)&wk.probs, n * kMlpBins * 4));
+    ERQ_TRY(dm((void**)&wk.dz, n * kMlpBins * 4));
+    ERQ_TRY(dm((void**)&wk.dh2, n * kMlpHidden * 4));
+    ERQ_TRY(dm((void**)&wk.dh1, n * kMlpHidden * 4));
+    ERQ_TRY(dm((void**)&wk.loss, n * 4));
+    ERQ_CUDA(cudaMemcpy(fin, features, n * kMlpIn * 4, cudaMemcpyHostToDevice));
+    ERQ_CUDA(cudaMemcpy(y, labels, n, cudaMemcpyHostToDevice));
+    cudaStream_t st = nullptr;
+    mlp_standardise_kernel<<<(unsigned)div_up(n * kMlpIn, 256), 256, 0, st>>>(fin, m->mean, m->stdv,
+                                                                            wk.x, (int)(n * kMlpIn));
+    ERQ_TRY(mlp_forward(m, wk, (int)n, st));
+    mlp_softmax_xent_kernel<<<(unsigned)div_up(n, 128), 128, 0, st>>>(wk.z, y, (int)n, wk.probs, wk.dz,
+                                                                     wk.loss);
+    ERQ_TRY(mlp_backward(m, wk, (int)n, g, st));
+    std::vector<float> lh(n);
+    ERQ_CUDA(cudaMemcpy(lh.data(), wk.loss, n * 4, cudaMemcpyDeviceToHost));
+    ERQ_CUDA(cudaMemcpy(grads, g, kMlpParams * 4, cudaMemcpyDeviceToHost));
+    double sum = 0.0;
+    for (float v : lh) sum += v;
+    *loss = (float)(sum / n);
+    return ERQ_OK;
+}
+
+erq_status erq_debug_probe_model_params(const erq_probe_model* m, float* params, float* mean,
+                                        float* stdv, uint32_t* bin_nprobe) {
+    if (!m) return fail(ERQ_ERR_INVALID_ARGUMENT, "NULL argument");
+    DeviceGuard guard;
+    ERQ_TRY(guard.set(m->device));
+    if (params) ERQ_CUDA(cudaMemcpy(params, m->w, kMlpParams * 4, cudaMemcpyDeviceToHost));
+    if (mean) ERQ_CUDA(cudaMemcpy(mean, m->mean, kMlpIn * 4, cudaMemcpyDeviceToHost));
+    if (stdv) ERQ_CUDA(cudaMemcpy(stdv, m->stdv, kMlpIn * 4, cudaMemcpyDeviceToHost));
+    if (bin_nprobe)
+        for (int j = 0; j < kMlpBins; ++j) bin_nprobe[j] = (uint32_t)m->bins[j];
     return ERQ_OK;
 }
 

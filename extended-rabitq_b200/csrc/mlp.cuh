@@ -1,0 +1,200 @@
+// Learned probing: a small MLP that predicts, per query, how many clusters the
+// plain search must probe before its top-k stops changing.
+//
+//   features (320) -> 256 -> ReLU -> 256 -> ReLU -> 8 logits -> softmax
+//
+// Weights are kept as FP32 master copies for training and as BF16 copies for
+// the forward pass; every product accumulates in FP32.  The forward, backward
+// and Adam kernels are written here (no library).  The model only chooses how
+// many of the probe list's clusters each query scans; the distance arithmetic
+// of the search is unchanged.
+#pragma once
+
+#include <cuda_bf16.h>
+
+#include "common.cuh"
+
+namespace erq {
+
+constexpr int kMlpIn = 320;      // 256 sketch dims + 64 centroid distances
+constexpr int kMlpHidden = 256;
+constexpr int kMlpBins = 8;
+constexpr int kSketchDims = 256;
+constexpr int kFeatDists = 64;
+
+// Parameter layout (one flat FP32 array; the BF16 copy mirrors W1, W2, W3).
+constexpr int kW1 = 0;                                  // [256][320]
+constexpr int kB1 = kW1 + kMlpHidden * kMlpIn;          // [256]
+constexpr int kW2 = kB1 + kMlpHidden;                   // [256][256]
+constexpr int kB2 = kW2 + kMlpHidden * kMlpHidden;      // [256]
+constexpr int kW3 = kB2 + kMlpHidden;                   // [8][256]
+constexpr int kB3 = kW3 + kMlpBins * kMlpHidden;        // [8]
+constexpr int kMlpParams = kB3 + kMlpBins;
+
+// C[m][n] (+)= sum_k A(m,k) * B(k,n) with A(m,k) = A[m*sam + k*sak] and
+// B(k,n) = B[k*sbk + n*sbn]; 16x16 tiles through shared memory.  TB is float
+// or __nv_bfloat16.  Optional bias[n] and ReLU on the result.
+template <typename TB>
+__global__ void mlp_matmul_kernel(const float* __restrict__ A, long sam, long sak,
+                                  const TB* __restrict__ B, long sbk, long sbn,
+                                  float* __restrict__ C, int M, int N, int K,
+                                  const float* __restrict__ bias, bool relu, bool accumulate) {
+    __shared__ float As[16][17];
+    __shared__ float Bs[16][17];
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    const int m = blockIdx.y * 16 + ty, n = blockIdx.x * 16 + tx;
+    float acc = 0.f;
+    for (int k0 = 0; k0 < K; k0 += 16) {
+        const int ka = k0 + tx, kb = k0 + ty;
+        const int am = blockIdx.y * 16 + ty, bn = blockIdx.x * 16 + tx;
+        As[ty][tx] = (am < M && ka < K) ? A[am * sam + (long)ka * sak] : 0.f;
+        float bv = 0.f;
+        if (kb < K && bn < N) {
+            if constexpr (sizeof(TB) == 2)
+                bv = __bfloat162float(B[(long)kb * sbk + (long)bn * sbn]);
+            else
+                bv = (float)B[(long)kb * sbk + (long)bn * sbn];
+        }
+        Bs[ty][tx] = bv;
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < 16; ++kk) acc = fmaf(As[ty][kk], Bs[kk][tx], acc);
+        __syncthreads();
+    }
+    if (m < M && n < N) {
+        float v = acc + (bias ? bias[n] : 0.f);
+        if (relu) v = fmaxf(v, 0.f);
+        C[(size_t)m * N + n] = accumulate ? C[(size_t)m * N + n] + v : v;
+    }
+}
+
+// Softmax cross-entropy on logits [B][8]: dlogits = (softmax - onehot) / B,
+// probabilities out, per-row loss into loss_rows.
+__global__ void mlp_softmax_xent_kernel(const float* __restrict__ logits,
+                                        const uint8_t* __restrict__ labels, int B,
+                                        float* __restrict__ probs, float* __restrict__ dlogits,
+                                        float* __restrict__ loss_rows) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= B) return;
+    const float* z = logits + (size_t)r * kMlpBins;
+    float mx = z[0];
+    for (int j = 1; j < kMlpBins; ++j) mx = fmaxf(mx, z[j]);
+    float e[kMlpBins], s = 0.f;
+    for (int j = 0; j < kMlpBins; ++j) {
+        e[j] = expf(z[j] - mx);
+        s += e[j];
+    }
+    const float inv = 1.f / s;
+    for (int j = 0; j < kMlpBins; ++j) {
+        const float p = e[j] * inv;
+        if (probs) probs[(size_t)r * kMlpBins + j] = p;
+        if (dlogits) dlogits[(size_t)r * kMlpBins + j] = (p - (labels && labels[r] == j ? 1.f : 0.f)) / B;
+    }
+    if (loss_rows && labels) loss_rows[r] = -(z[labels[r]] - mx - logf(s));
+}
+
+// dH *= (H > 0), elementwise.
+__global__ void mlp_relu_grad_kernel(float* __restrict__ dH, const float* __restrict__ H, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n && H[i] <= 0.f) dH[i] = 0.f;
+}
+
+// db[n] = sum_r dY[r][n]
+__global__ void mlp_bias_grad_kernel(const float* __restrict__ dY, int B, int N,
+                                     float* __restrict__ db) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    float s = 0.f;
+    for (int r = 0; r < B; ++r) s += dY[(size_t)r * N + n];
+    db[n] = s;
+}
+
+// Adam on the FP32 master weights, refreshing the BF16 copies of W1..W3.
+__global__ void mlp_adam_kernel(float* __restrict__ w, const float* __restrict__ g,
+                                float* __restrict__ m1, float* __restrict__ m2,
+                                __nv_bfloat16* __restrict__ wb, int n, float lr, float beta1,
+                                float beta2, float eps, float bc1, float bc2) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float gi = g[i];
+    const float a = beta1 * m1[i] + (1.f - beta1) * gi;
+    const float b = beta2 * m2[i] + (1.f - beta2) * gi * gi;
+    m1[i] = a;
+    m2[i] = b;
+    const float v = w[i] - lr * (a / bc1) / (sqrtf(b / bc2) + eps);
+    w[i] = v;
+    wb[i] = __float2bfloat16_rn(v);
+}
+
+__global__ void mlp_to_bf16_kernel(const float* __restrict__ w, __nv_bfloat16* __restrict__ wb,
+                                   int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) wb[i] = __float2bfloat16_rn(w[i]);
+}
+
+// Standardise raw features: x = (f - mean) / std.
+__global__ void mlp_standardise_kernel(const float* __restrict__ f, const float* __restrict__ mean,
+                                       const float* __restrict__ stdv, float* __restrict__ x,
+                                       int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        const int c = i % kMlpIn;
+        x[i] = (f[i] - mean[c]) / stdv[c];
+    }
+}
+
+// Raw features of one query: 256 sketch dims (the first rotated coordinates,
+// a random projection, scaled by 16/||q_r||) and 64 values of its nearest
+// centroid distances e_0 <= e_1 <= ...: log(e_0 / ||q_r||^2 + 1e-12) and
+// e_j / e_0 - 1 for j >= 1.
+__global__ void probe_features_kernel(const float* __restrict__ qrot, int D,
+                                      const float* __restrict__ near_d, int nq,
+                                      float* __restrict__ feats) {
+    const int q = blockIdx.x;
+    if (q >= nq) return;
+    __shared__ float red[8];
+    const float* v = qrot + (size_t)q * D;
+    float s = 0.f;
+    for (int i = threadIdx.x; i < D; i += blockDim.x) s = fmaf(v[i], v[i], s);
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    float qn = 0.f;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) qn += red[w];
+    const float inv = qn > 0.f ? 16.f / sqrtf(qn) : 0.f;
+    float* f = feats + (size_t)q * kMlpIn;
+    for (int i = threadIdx.x; i < kSketchDims; i += blockDim.x) f[i] = i < D ? v[i] * inv : 0.f;
+    const float* d = near_d + (size_t)q * kFeatDists;
+    const float d0 = d[0];
+    for (int j = threadIdx.x; j < kFeatDists; j += blockDim.x) {
+        float x;
+        if (j == 0)
+            x = logf(d0 / fmaxf(qn, 1e-30f) + 1e-12f);
+        else
+            x = d0 > 0.f ? d[j] / d0 - 1.f : 0.f;
+        f[kSketchDims + j] = x;
+    }
+}
+
+// Per-query probe count from the class probabilities: the smallest bin whose
+// cumulative probability reaches `confidence`; queries whose most likely bin
+// has probability below `min_prob` fall back to `fallback`.
+__global__ void mlp_choose_nprobe_kernel(const float* __restrict__ probs, int nq,
+                                         const int* __restrict__ bin_nprobe, float confidence,
+                                         float min_prob, int fallback, int nprobe_cap,
+                                         int* __restrict__ q_nprobe) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nq) return;
+    const float* p = probs + (size_t)q * kMlpBins;
+    float mx = 0.f, cum = 0.f;
+    int chosen = -1;
+    for (int j = 0; j < kMlpBins; ++j) {
+        mx = fmaxf(mx, p[j]);
+        cum += p[j];
+        if (chosen < 0 && cum >= confidence) chosen = j;
+    }
+    int np = (chosen < 0 || mx < min_prob) ? fallback : bin_nprobe[chosen];
+    q_nprobe[q] = min(max(np, 1), nprobe_cap);
+}
+
+}  // namespace erq

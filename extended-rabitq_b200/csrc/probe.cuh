@@ -31,7 +31,9 @@ struct ProbeArgs {
     float* probe_sqy;         // [nq][nprobe]
     uint64_t* s_off;          // [nq][nprobe]
     uint32_t* fallbacks;      // optional counter of queries that took step 4
+    float* near_d;            // optional [nq][64]: the 64 nearest exact distances
     int nq, K, Kpow2, D, nprobe, M;
+    int check_rank;           // rank whose exactness the bound check proves (>= nprobe)
 };
 
 constexpr int kProbeThreads = 256;
@@ -174,9 +176,9 @@ __global__ void __launch_bounds__(kProbeThreads) probe_kernel(ProbeArgs a) {
     block_bitonic_sort(sk, nsort);
     // bound check
     if (tid == 0) {
-        bool ok = ns >= a.nprobe;
+        bool ok = ns >= a.check_rank;
         if (ok && !select_all) {
-            const float e_n = __uint_as_float((uint32_t)(sk[a.nprobe - 1] >> 32));
+            const float e_n = __uint_as_float((uint32_t)(sk[a.check_rank - 1] >> 32));
             const float eps = a.eps_rel * (a.qn[q] + a.cn_max);
             const float A = order_key_value(kstar);
             ok = (A - eps > e_n) && (e_n == e_n);
@@ -196,6 +198,12 @@ __global__ void __launch_bounds__(kProbeThreads) probe_kernel(ProbeArgs a) {
         for (int i = K + tid; i < a.Kpow2; i += blockDim.x) sk[i] = ~0ull;
         __syncthreads();
         block_bitonic_sort(sk, a.Kpow2);
+    }
+    if (a.near_d) {
+        const int avail = misc[3] ? ns : K;
+        for (int j = tid; j < 64; j += blockDim.x)
+            a.near_d[(size_t)q * 64 + j] =
+                __uint_as_float((uint32_t)(sk[j < avail ? j : avail - 1] >> 32));
     }
     // outputs + exclusive prefix of 32*nblocks over the probe order (warp 0)
     if (warp == 0) {

@@ -40,11 +40,10 @@ struct RefineArgs {
     const uint32_t* c_size;        // [K]
     uint32_t* out_ids;            // [nq][k]
     float* out_dists;             // [nq][k] or null
+    const int* q_nprobe;          // optional [nq]: clusters probed by each query
     int nq, D, EX, nprobe, k;
 };
 
-constexpr int kRefineWarps = 4;
-constexpr int kChunkBlocks = 4;  // blocks whose candidates are refined together
 
 // float(v) for 0 <= v < 256 held in byte `i` of `w`: 0x4B0000vv is 2^23 + v.
 __device__ __forceinline__ float byte_to_float(uint32_t w, int i) {
@@ -174,43 +173,57 @@ __device__ __forceinline__ void pool_insert(float* pool_d, uint32_t* pool_id, in
     distk = size == k ? pool_d[k - 1] : FLT_MAX;
 }
 
-// Shared memory of one warp: unit_q[D] | ipq, onorm, ex_dist, id [128 each] |
-// candidate list [128 bytes] | pool_d[kpad] | pool_id[kpad]
-__host__ __device__ constexpr size_t refine_warp_smem_bytes(int D, int kpad) {
-    return (size_t)D * 4 + (size_t)kChunkBlocks * 32 * 16 + kChunkBlocks * 32 + (size_t)kpad * 8;
+constexpr int kRefineThreads = 128;     // 4 warps per query
+constexpr int kWindowBlocks = 16;       // blocks whose candidates are refined together
+constexpr int kWindowLanes = kWindowBlocks * 32;
+
+// Shared memory of one block: unit_q[D] | per window lane: lb, ipq, onorm,
+// ex_dist, id, list | pool_d[kpad] | pool_id[kpad] | misc
+__host__ __device__ constexpr size_t refine_smem_bytes_per_query(int D, int kpad) {
+    return (size_t)D * 4 + (size_t)kWindowLanes * (5 * 4 + 2) + (size_t)kpad * 8 + 64;
 }
 
+// One block of 4 warps per query.  Per window of 16 blocks of the current
+// cluster: every warp computes the lower bounds of 4 blocks and lists the
+// lanes below the threshold as it stands at the window's start (a superset of
+// the exact candidates, because the threshold only falls); all 128 threads
+// refine the listed candidates, one each; warp 0 then replays the window in
+// the reference's order - each block's mask against the threshold at that
+// block's start, candidates in ascending lane order - inserting into the pool.
 template <int EX>
-__global__ void __launch_bounds__(kRefineWarps * 32) refine_kernel(RefineArgs a) {
+__global__ void __launch_bounds__(kRefineThreads) refine_kernel(RefineArgs a) {
     extern __shared__ __align__(16) uint8_t smem_raw[];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int q = blockIdx.x * kRefineWarps + warp;
-    if (q >= a.nq) return;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int q = blockIdx.x;
     const int D = a.D, k = a.k;
     const int kpad = (k + 31) & ~31;
-    uint8_t* base = smem_raw + (size_t)warp * refine_warp_smem_bytes(D, kpad);
-    float* uq = reinterpret_cast<float*>(base);
-    float* c_ipq = uq + D;
-    float* c_on = c_ipq + kChunkBlocks * 32;
-    float* c_ed = c_on + kChunkBlocks * 32;
-    uint32_t* c_id = reinterpret_cast<uint32_t*>(c_ed + kChunkBlocks * 32);
-    uint8_t* c_list = reinterpret_cast<uint8_t*>(c_id + kChunkBlocks * 32);
-    float* pool_d = reinterpret_cast<float*>(c_list + kChunkBlocks * 32);
+    float* uq = reinterpret_cast<float*>(smem_raw);
+    float* w_lb = uq + D;
+    float* w_ipq = w_lb + kWindowLanes;
+    float* w_on = w_ipq + kWindowLanes;
+    float* w_ed = w_on + kWindowLanes;
+    uint32_t* w_id = reinterpret_cast<uint32_t*>(w_ed + kWindowLanes);
+    uint16_t* w_list = reinterpret_cast<uint16_t*>(w_id + kWindowLanes);
+    float* pool_d = reinterpret_cast<float*>(w_list + kWindowLanes);
     uint32_t* pool_id = reinterpret_cast<uint32_t*>(pool_d + kpad);
+    int* misc = reinterpret_cast<int*>(pool_id + kpad);  // [0] list count
+    float* s_distk = reinterpret_cast<float*>(misc + 1);
     const int code_len = D * EX / 8;
     const int fac_rescale = 1 << EX;
     const float one_over_sqrtD = recip_via_double(__fsqrt_rn((float)D));
     const float* qv = a.qrot + (size_t)q * D;
 
-    for (int i = lane; i < kpad; i += 32) {
+    for (int i = tid; i < kpad; i += blockDim.x) {
         pool_d[i] = 0.f;
         pool_id[i] = 0u;
     }
-    __syncwarp();
-    int size = 0;
+    if (tid == 0) *s_distk = FLT_MAX;
+    int size = 0;         // pool state, maintained by warp 0
     float distk = FLT_MAX;
+    __syncthreads();
 
-    for (int p = 0; p < a.nprobe; ++p) {
+    const int np_q = a.q_nprobe ? a.q_nprobe[q] : a.nprobe;
+    for (int p = 0; p < np_q; ++p) {
         const size_t qp = (size_t)q * a.nprobe + p;
         const uint32_t cid = a.probe_cid[qp];
         const float sqy = a.probe_sqy[qp];
@@ -228,89 +241,94 @@ __global__ void __launch_bounds__(kRefineWarps * 32) refine_kernel(RefineArgs a)
         const int32_t* S = a.S + a.s_off[qp];
         const uint32_t nblocks = (n + 31) >> 5;
         bool uq_ready = false;
-        for (uint32_t cb = 0; cb < nblocks; cb += kChunkBlocks) {
-            const int nbc = (int)min((uint32_t)kChunkBlocks, nblocks - cb);
-            float lb[kChunkBlocks];
-            bool valid[kChunkBlocks];
+        for (uint32_t wb = 0; wb < nblocks; wb += kWindowBlocks) {
+            const int nbw = (int)min((uint32_t)kWindowBlocks, nblocks - wb);
+            const float d0 = *s_distk;
+            if (tid == 0) misc[0] = 0;
+            __syncthreads();
+            // lower bounds and the candidate superset, 4 blocks per warp
 #pragma unroll
-            for (int b = 0; b < kChunkBlocks; ++b) {
-                valid[b] = false;
-                lb[b] = 0.f;
-                if (b < nbc) {
-                    const uint32_t blk = cb + b;
+            for (int i = 0; i < kWindowBlocks / 4; ++i) {
+                const int b = warp * (kWindowBlocks / 4) + i;
+                if (b < nbw) {  // uniform per warp
+                    const uint32_t blk = wb + b;
                     const float ipq = __fmul_rn(__int2float_rn(S[32 * blk + lane]), delta);
                     const float on = a.onorm[(size_t)(fb + blk) * 32 + lane];
                     float t = __fsub_rn(ipq, c1);
                     t = __fmul_rn(t, c2);
                     t = __fmul_rn(t, on);
                     t = __fadd_rn(t, c3);
-                    lb[b] = __fadd_rn(t, __fmul_rn(on, on));
-                    valid[b] = 32 * blk + lane < n;
-                    c_ipq[32 * b + lane] = ipq;
-                    c_on[32 * b + lane] = on;
+                    t = __fadd_rn(t, __fmul_rn(on, on));
+                    const bool valid = 32 * blk + lane < n;
+                    // padding lanes never pass (NaN compares false)
+                    w_lb[32 * b + lane] = valid ? t : __int_as_float(0x7fc00000);
+                    w_ipq[32 * b + lane] = ipq;
+                    w_on[32 * b + lane] = on;
+                    const uint32_t m = __ballot_sync(0xffffffffu, valid && t < d0);
+                    int base = 0;
+                    if (lane == 0 && m) base = atomicAdd(&misc[0], __popc(m));
+                    base = __shfl_sync(0xffffffffu, base, 0);
+                    if ((m >> lane) & 1u)
+                        w_list[base + __popc(m & ((1u << lane) - 1u))] = (uint16_t)(32 * b + lane);
                 }
             }
-            // Every candidate of these blocks has lb < distk at its block's
-            // start <= distk now, so {lb < distk now} holds them all.
-            int cnt = 0;
-#pragma unroll
-            for (int b = 0; b < kChunkBlocks; ++b) {
-                const uint32_t m = __ballot_sync(0xffffffffu, valid[b] && lb[b] < distk);
-                if ((m >> lane) & 1u) c_list[cnt + __popc(m & ((1u << lane) - 1u))] = (uint8_t)(32 * b + lane);
-                cnt += __popc(m);
-            }
-            if (cnt == 0) continue;
+            __syncthreads();
+            const int cnt = misc[0];
+            if (cnt == 0) continue;  // uniform: nothing in this window can pass
             if (!uq_ready) {
                 const float* cv = a.centroids + (size_t)cid * D;
                 if (y > kNormEps) {
                     const float fac = recip_via_double(y);
-                    for (int i = lane; i < D; i += 32) uq[i] = __fmul_rn(__fsub_rn(qv[i], cv[i]), fac);
+                    for (int i = tid; i < D; i += blockDim.x) uq[i] = __fmul_rn(__fsub_rn(qv[i], cv[i]), fac);
                 } else {
                     const float fill = recip_via_double(__fsqrt_rn((float)D));
-                    for (int i = lane; i < D; i += 32) uq[i] = fill;
+                    for (int i = tid; i < D; i += blockDim.x) uq[i] = fill;
                 }
                 uq_ready = true;
+                __syncthreads();
             }
-            __syncwarp();
-            // refine the candidates, one per lane (inactive lanes repeat the
-            // first one so the warp stays converged on the broadcast reads)
-            for (int r = 0; r < cnt; r += 32) {
-                const int i = r + lane;
-                const int slot = c_list[i < cnt ? i : 0];
-                const size_t pos = (size_t)first_vec + 32 * cb + slot;
+            // refine the listed candidates, one per thread (idle threads repeat
+            // the first so each warp stays converged on the broadcast reads)
+            for (int r = 0; r < cnt; r += blockDim.x) {
+                const int i = r + tid;
+                const int slot = w_list[i < cnt ? i : 0];
+                const size_t pos = (size_t)first_vec + 32 * wb + slot;
                 const float ip = ex_ip_thread<EX>(uq, a.excode + pos * code_len, D);
                 if (i < cnt) {
                     // inc/index/HASearcher.hpp:225-232
-                    const float on = c_on[slot];
+                    const float on = w_on[slot];
                     const float sqr_x = __fmul_rn(on, on);
-                    const float t = __fadd_rn(__fmul_rn((float)fac_rescale, c_ipq[slot]), ip);
+                    const float t = __fadd_rn(__fmul_rn((float)fac_rescale, w_ipq[slot]), ip);
                     const double br = __dsub_rn((double)t, ex_sub);
                     const float xy = __fmul_rn(a.xipnorm[pos], y);
                     const float f = __fadd_rn(sqr_x, sqy);
-                    c_ed[slot] = __double2float_rn(__dsub_rn((double)f, __dmul_rn((double)xy, br)));
-                    c_id[slot] = a.ids[pos];
+                    w_ed[slot] = __double2float_rn(__dsub_rn((double)f, __dmul_rn((double)xy, br)));
+                    w_id[slot] = a.ids[pos];
                 }
             }
-            __syncwarp();
-            // exact replay: the mask of each block against the threshold at
-            // the block's start, candidates in ascending lane order
-#pragma unroll
-            for (int b = 0; b < kChunkBlocks; ++b) {
-                uint32_t mask = __ballot_sync(0xffffffffu, valid[b] && lb[b] < distk);
-                while (mask) {
-                    const int j = __ffs(mask) - 1;
-                    mask &= mask - 1;
-                    pool_insert(pool_d, pool_id, size, k, distk, c_ed[32 * b + j], c_id[32 * b + j],
-                                lane);
+            __syncthreads();
+            if (warp == 0) {
+                for (int b = 0; b < nbw; ++b) {
+                    uint32_t mask = __ballot_sync(0xffffffffu, w_lb[32 * b + lane] < distk);
+                    while (mask) {
+                        const int j = __ffs(mask) - 1;
+                        mask &= mask - 1;
+                        pool_insert(pool_d, pool_id, size, k, distk, w_ed[32 * b + j],
+                                    w_id[32 * b + j], lane);
+                    }
                 }
+                if (lane == 0) *s_distk = distk;
             }
-            __syncwarp();
+            __syncthreads();
         }
     }
-    uint32_t* oid = a.out_ids + (size_t)q * k;
-    for (int i = lane; i < k; i += 32) {
-        oid[i] = i < size ? pool_id[i] : 0u;
-        if (a.out_dists) a.out_dists[(size_t)q * k + i] = i < size ? pool_d[i] : __int_as_float(0x7f800000);
+    if (warp == 0) {
+        uint32_t* oid = a.out_ids + (size_t)q * k;
+        for (int i = lane; i < k; i += 32) {
+            oid[i] = i < size ? pool_id[i] : 0u;
+            if (a.out_dists)
+                a.out_dists[(size_t)q * k + i] = i < size ? pool_d[i] : __int_as_float(0x7f800000);
+        }
     }
 }
 

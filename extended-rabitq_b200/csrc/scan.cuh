@@ -40,6 +40,7 @@ struct ScanArgs {
     int32_t* S;               // output sums
     float* qp_delta;          // [nq][nprobe]
     float* qp_sumq;           // [nq][nprobe]
+    const int* q_nprobe;      // optional [nq]: probe only the first q_nprobe[q] clusters
     int D;
     int nprobe;
 };
@@ -93,6 +94,7 @@ __global__ void __launch_bounds__(kScanWarps * 32) scan_kernel(ScanArgs a) {
 
     const uint32_t pair = blockIdx.x;
     const uint32_t q = pair / (uint32_t)a.nprobe;
+    if (a.q_nprobe && (int)(pair - q * (uint32_t)a.nprobe) >= a.q_nprobe[q]) return;
     const uint32_t cid = a.probe_cid[pair];
     const float sqy = a.probe_sqy[pair];
     const float y = __fsqrt_rn(sqy);

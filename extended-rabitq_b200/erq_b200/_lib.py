@@ -31,6 +31,9 @@ EXPORTED_SYMBOLS = (
     "erq_search_noalloc",
     "erq_debug_scan_capacity", "erq_debug_centroid_dists", "erq_debug_probe", "erq_debug_scan",
     "erq_profile_enable", "erq_profile_reset", "erq_profile_read",
+    "erq_probe_features", "erq_probe_model_train", "erq_probe_model_save", "erq_probe_model_load",
+    "erq_probe_model_free", "erq_probe_model_predict", "erq_search_learned",
+    "erq_debug_probe_model_grads", "erq_debug_probe_model_params",
 )
 
 
@@ -98,6 +101,26 @@ def load_library(path: str | None = None) -> C.CDLL:
     lib.erq_profile_reset.restype = None
     lib.erq_profile_read.argtypes = [C.c_char_p, C.POINTER(C.c_uint64), C.POINTER(C.c_double)]
     lib.erq_profile_read.restype = C.c_int
+    lib.erq_probe_features.argtypes = [vp, f32p, u64, f32p, vp]
+    lib.erq_probe_features.restype = C.c_int
+    lib.erq_probe_model_train.argtypes = [vp, vp, u64, vp, C.c_int, C.c_int, C.c_float, u64,
+                                          C.c_int, C.POINTER(C.c_void_p), C.POINTER(C.c_float)]
+    lib.erq_probe_model_train.restype = C.c_int
+    lib.erq_probe_model_save.argtypes = [vp, C.c_char_p]
+    lib.erq_probe_model_save.restype = C.c_int
+    lib.erq_probe_model_load.argtypes = [C.c_char_p, C.c_int, C.POINTER(C.c_void_p)]
+    lib.erq_probe_model_load.restype = C.c_int
+    lib.erq_probe_model_free.argtypes = [vp]
+    lib.erq_probe_model_free.restype = None
+    lib.erq_probe_model_predict.argtypes = [vp, vp, u64, vp, vp]
+    lib.erq_probe_model_predict.restype = C.c_int
+    lib.erq_search_learned.argtypes = [vp, vp, f32p, u64, u64, u64, C.c_float, C.c_float, u32p,
+                                       f32p, vp, vp]
+    lib.erq_search_learned.restype = C.c_int
+    lib.erq_debug_probe_model_grads.argtypes = [vp, vp, vp, u64, C.POINTER(C.c_float), vp]
+    lib.erq_debug_probe_model_grads.restype = C.c_int
+    lib.erq_debug_probe_model_params.argtypes = [vp, vp, vp, vp, vp]
+    lib.erq_debug_probe_model_params.restype = C.c_int
     _lib = lib
     return lib
 

@@ -92,6 +92,47 @@ ERQ_API erq_status erq_search_raw(const erq_index* index, const float* queries, 
                           uint64_t k, uint64_t nprobe, uint32_t* ids, float* dists,
                           void* stream);
 
+/* ---------------------------------------------------------------------------
+ * Learned probing.  Has no counterpart in the reference (IVF::search probes a
+ * fixed nprobe, inc/index/IVF.hpp:295-324).  A small MLP predicts, per query,
+ * after how many clusters of its probe list the plain search's top-k stops
+ * changing; the search then scans only those clusters, with the reference's
+ * arithmetic unchanged.  Training uses labels produced by the plain search. */
+typedef struct erq_probe_model erq_probe_model;
+#define ERQ_PROBE_FEATURES 320 /* 256 sketch dims + 64 nearest-centroid terms */
+#define ERQ_PROBE_BINS 8
+
+/* features[nq][320] of rotated queries: the first 256 rotated coordinates
+ * scaled by 16/||q||, log(e_0/||q||^2) and e_j/e_0 - 1 (j = 1..63) of the 64
+ * nearest exact centroid distances e_0 <= e_1 <= ... */
+ERQ_API erq_status erq_probe_features(const erq_index* index, const float* rotated_queries,
+                                      uint64_t nq, float* features, void* stream);
+
+/* Train on host features[n][320] and labels[n] in [0, 8); bin_nprobe[8]
+ * (increasing) is the probe count of each class.  Adam, cross-entropy,
+ * mini-batches of `batch`, on CUDA device `device`. */
+ERQ_API erq_status erq_probe_model_train(const float* features, const uint8_t* labels, uint64_t n,
+                                         const uint32_t* bin_nprobe, int epochs, int batch,
+                                         float lr, uint64_t seed, int device,
+                                         erq_probe_model** out, float* final_loss);
+ERQ_API erq_status erq_probe_model_save(const erq_probe_model* model, const char* path);
+ERQ_API erq_status erq_probe_model_load(const char* path, int device, erq_probe_model** out);
+ERQ_API void erq_probe_model_free(erq_probe_model* model);
+/* probs[n][8] = softmax of the model on raw features[n][320]. */
+ERQ_API erq_status erq_probe_model_predict(const erq_probe_model* model, const float* features,
+                                           uint64_t n, float* probs, void* stream);
+
+/* IVF::search where each query scans the first c clusters of its probe list:
+ * c = bin_nprobe of the smallest class whose cumulative probability reaches
+ * `confidence`, or nprobe_fallback when the most likely class has probability
+ * below `min_prob`.  nprobe_used[nq] (may be NULL) receives c per query.  The
+ * results equal erq_search's with nprobe = c for each query. */
+ERQ_API erq_status erq_search_learned(const erq_index* index, const erq_probe_model* model,
+                                      const float* rotated_queries, uint64_t nq, uint64_t k,
+                                      uint64_t nprobe_fallback, float confidence, float min_prob,
+                                      uint32_t* ids, float* dists, uint32_t* nprobe_used,
+                                      void* stream);
+
 /* erq_search without any memory allocation.  Has no counterpart in the
  * reference: it is for callers that cannot allocate device memory while a
  * query runs - engines that hand all GPU memory to their own allocator up

@@ -41,6 +41,18 @@ ERQ_API erq_status erq_debug_scan(const erq_index* index, const float* rotated_q
                           uint64_t nprobe, uint32_t* cids, float* sqr_y, float* delta,
                           float* sumq, uint64_t* s_offsets, int32_t* S, uint64_t s_capacity);
 
+/* Gradient of the mean cross-entropy of a probe model on host features[n][320]
+ * and labels[n], in the parameter order W1[256][320], b1, W2[256][256], b2,
+ * W3[8][256], b3 (grads holds ERQ_PROBE_PARAMS floats); loss = mean loss. */
+#define ERQ_PROBE_PARAMS 150024
+ERQ_API erq_status erq_debug_probe_model_grads(const erq_probe_model* model, const float* features,
+                                               const uint8_t* labels, uint64_t n, float* loss,
+                                               float* grads);
+/* Copies of the FP32 parameters, standardisation and class probe counts
+ * (any pointer may be NULL). */
+ERQ_API erq_status erq_debug_probe_model_params(const erq_probe_model* model, float* params,
+                                                float* mean, float* stdv, uint32_t* bin_nprobe);
+
 /* Kernel timing.  While enabled, every kernel launch of the search and
  * rotation entry points is bracketed by CUDA events recorded on the stream
  * the kernel runs on.  erq_profile_read waits for the recorded events and
