@@ -45,12 +45,15 @@ CONFIGS = {
     "sphere1536-1M-8bit": dict(
         gen="sphere", n=1_000_000, dim=1536, comps=4096, sigma=0.05, zipf=None, K=4096,
         bits=8, nq=10_000, k=100, seed=20241, nprobe=None, recall_target=0.95,
+        train_queries=200_000,
         data="synthetic: seeded 4096-component unit-sphere mixture, tangent sigma 0.05, "
-             "1M base + 10k queries, d=1536 (openai1536 stand-in)"),
+             "1M base + 10k queries (+200k training queries for the probe model), d=1536 "
+             "(openai1536 stand-in)"),
     # the small CPU-runnable case
     "gauss128-100k-4bit": dict(
         gen="gauss", n=100_000, dim=128, comps=256, sigma=0.3, zipf=None, K=1024,
         bits=4, nq=1000, k=100, seed=11, nprobe=None, recall_target=0.95,
+        train_queries=20_000,
         data="synthetic: seeded 256-component Gaussian mixture, sigma 0.3, 100k base + 1k "
              "queries, d=128"),
 }
@@ -65,7 +68,8 @@ def log(*a):
 
 # ------------------------------------------------------------------ data prep
 def cache_dir(name, cfg):
-    key = f"{name}-{cfg['n']}-{cfg['dim']}-{cfg['K']}-{cfg['bits']}-{cfg['nq']}-{cfg['seed']}"
+    key = (f"{name}-{cfg['n']}-{cfg['dim']}-{cfg['K']}-{cfg['bits']}-{cfg['nq']}-{cfg['seed']}"
+           f"-{cfg.get('train_queries', 0)}")
     return os.path.join(os.environ.get("ERQ_BENCH_CACHE", "/tmp/erq_bench"), key)
 
 
@@ -82,14 +86,19 @@ def prepare(name, cfg, device="cuda"):
 
     os.makedirs(d, exist_ok=True)
     t0 = time.time()
+    nq_all = cfg["nq"] + cfg.get("train_queries", 0)
     if cfg["gen"] == "sphere":
         base, query = datasets.sphere_mixture_torch(cfg["n"], cfg["dim"], cfg["comps"],
-                                                    cfg["sigma"], cfg["seed"], cfg["nq"],
+                                                    cfg["sigma"], cfg["seed"], nq_all,
                                                     cfg["zipf"], device=device)
     else:
         base, query = datasets.gaussian_mixture_torch(cfg["n"], cfg["dim"], cfg["comps"],
-                                                      cfg["sigma"], cfg["seed"], cfg["nq"],
+                                                      cfg["sigma"], cfg["seed"], nq_all,
                                                       device=device)
+    train_q = query[cfg["nq"]:]
+    query = query[:cfg["nq"]]
+    np.save(os.path.join(d, "train_query.npy"), train_q.cpu().numpy())
+    del train_q
     log(f"generated {cfg['n']}x{cfg['dim']} in {time.time() - t0:.1f}s")
     cent, ids = datasets.kmeans_torch(base, cfg["K"], iters=20, seed=cfg["seed"] + 1)
     log(f"k-means K={cfg['K']} done at {time.time() - t0:.1f}s")
@@ -231,44 +240,68 @@ def choose_nprobe(idx, qraw, gt, cfg):
     return best
 
 
-def run_e2e(idx, query, k, nprobe, ids0, stream, args, world):
-    """The same steps through the C ABI with pinned host buffers: the H2D
-    copy of the raw queries and the D2H copy of ids + distances are inside
-    the timed region (the call returns when the results are on the host)."""
+def timed(step, steps, warmup, world, stream, clock_gpu=None):
+    """`warmup` untimed calls, then `steps` calls between CUDA events on
+    `stream` bracketed by barrier + synchronize; returns (max-over-ranks ms,
+    per-kernel profile of the timed calls, clock samples)."""
     import torch
 
-    nq = query.shape[0]
-    qh = torch.from_numpy(query).pin_memory()
-    ids_h = torch.empty((nq, k), dtype=torch.int32).pin_memory()
-    dist_h = torch.empty((nq, k), dtype=torch.float32).pin_memory()
+    from erq_b200 import _lib as L
 
-    def step_host():
-        idx.search_raw(qh, k, nprobe, ids=ids_h, dists=dist_h, stream=stream)
-
-    for _ in range(args.warmup):
-        step_host()
-    barrier(world)
-    torch.cuda.synchronize()
-    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    f0.record(stream)
-    for _ in range(args.steps):
-        step_host()
-    f1.record(stream)
+    for _ in range(warmup):
+        step()
     torch.cuda.synchronize()
     barrier(world)
-    e2e_ms = max_over_ranks(f0.elapsed_time(f1), world)
-    assert (ids_h.numpy().view(np.uint32) == ids0).all()
-    return {"value": round(world * nq * args.steps / (e2e_ms / 1e3), 1), "unit": "queries/s",
-            "h2d_bytes_per_step": int(nq * query.shape[1] * 4),
-            "d2h_bytes_per_step": int(nq * k * 8)}
+    torch.cuda.synchronize()
+    sampler = ClockSampler(clock_gpu) if clock_gpu is not None else None
+    L.profile_reset()
+    L.profile_enable(True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    L.profile_enable(False)
+    barrier(world)
+    clocks = sampler.stop() if sampler else None
+    prof = L.profile_read()
+    return max_over_ranks(e0.elapsed_time(e1), world), prof, clocks
+
+
+def learned_model(idx, d, cfg, plain_nprobe):
+    """The probe model of this workload, trained once and cached: labels from
+    the plain search on the training queries, features from the probe kernel,
+    training on the GPU by the library's kernels."""
+    from erq_b200 import learned
+
+    path = os.path.join(d, "probe.model")
+    if os.path.exists(path):
+        return learned.ProbeModel.load(path), json.load(open(path + ".json"))
+    t0 = time.time()
+    train_q = np.load(os.path.join(d, "train_query.npy"))
+    rot = idx.rotate(train_q)
+    del train_q
+    bins = learned.DEFAULT_BINS
+    labels = learned.make_labels(idx, rot, cfg["k"], bins)
+    feats = learned.probe_features(idx, rot)
+    del rot
+    model = learned.ProbeModel.train(feats, labels, bins, epochs=8, batch=1024, lr=1e-3,
+                                     seed=cfg["seed"] + 3)
+    hist = np.bincount(labels, minlength=len(bins)).tolist()
+    meta = {"train_queries": int(labels.size), "label_hist": hist, "bins": list(bins),
+            "final_loss": round(model.final_loss, 4), "train_s": round(time.time() - t0, 1)}
+    model.save(path)
+    json.dump(meta, open(path + ".json", "w"))
+    log(f"probe model: {meta}")
+    return model, meta
 
 
 # ------------------------------------------------------------------ our arm
 def run_ours(args, cfg, name):
     import torch
 
-    from erq_b200 import IVF, indexfile, metrics
-    from erq_b200 import _lib as L
+    from erq_b200 import IVF, indexfile, learned, metrics
 
     world, rank, local = dist_setup(args)
     torch.cuda.set_device(local)
@@ -282,60 +315,100 @@ def run_ours(args, cfg, name):
     if args.queries:
         query, gt = query[:args.queries], gt[:args.queries]
     nq, k = query.shape[0], cfg["k"]
+    target = cfg["recall_target"]
 
     idx = IVF(index_path, device=local)
     if args.nprobe:
         cfg = dict(cfg, nprobe=args.nprobe)
     nprobe, recall, ids0 = choose_nprobe(idx, query, gt, cfg)
-    # distance ratio on the first 1000 queries (get_ratio, inc/utils/tools.hpp:16-51)
     base = np.load(os.path.join(d, "base.npy"), mmap_mode="r")
     sub = min(1000, nq)
-    ratio = metrics.average_distance_ratio(query[:sub], base, ids0[:sub].astype(np.int64),
-                                           gt[:sub].astype(np.int64), k)
-    # algorithmic bytes of the scan kernel: every probed block's codes read
-    # and its 32 int32 sums written, (4D + 128) bytes per block
     arr = indexfile.read_index(index_path)
     nblocks = (arr.sizes.astype(np.int64) + 31) // 32
-    qrot = idx.rotate(query)
-    cids, _ = idx.debug_probe(qrot, nprobe)
-    scan_bytes_per_step = int(nblocks[cids.astype(np.int64)].sum()) * (4 * arr.D + 128)
-    del arr, qrot
+    block_bytes = 4 * arr.D + 128
+    qrot_h = idx.rotate(query)
+    cids, _ = idx.debug_probe(qrot_h, max(nprobe, learned.DEFAULT_BINS[-1]))
+    del arr
 
     stream = torch.cuda.current_stream()
     qd = torch.from_numpy(query).cuda()
     ids_d = torch.empty((nq, k), dtype=torch.int32, device="cuda")
     dist_d = torch.empty((nq, k), dtype=torch.float32, device="cuda")
+    qh = torch.from_numpy(query).pin_memory()
+    ids_h = torch.empty((nq, k), dtype=torch.int32).pin_memory()
+    dist_h = torch.empty((nq, k), dtype=torch.float32).pin_memory()
 
-    def step_device():
+    # --- plain fixed-nprobe search
+    def plain_dev():
         idx.search_raw(qd, k, nprobe, ids=ids_d, dists=dist_d, stream=stream)
 
-    for _ in range(args.warmup):
-        step_device()
-    torch.cuda.synchronize()
-    # device results equal the host-path results used for recall
+    def plain_host():
+        idx.search_raw(qh, k, nprobe, ids=ids_h, dists=dist_h, stream=stream)
+
+    ms_p, prof_p, clocks_p = timed(plain_dev, args.steps, args.warmup, world, stream, local)
     assert (ids_d.cpu().numpy().view(np.uint32) == ids0).all()
-    barrier(world)
-    torch.cuda.synchronize()
-    sampler = ClockSampler(local)
-    L.profile_reset()
-    L.profile_enable(True)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        step_device()
-    e1.record(stream)
-    torch.cuda.synchronize()
-    L.profile_enable(False)
-    barrier(world)
-    clocks = sampler.stop()
-    ms = max_over_ranks(e0.elapsed_time(e1), world)
-    prof = L.profile_read()
-    value = world * nq * args.steps / (ms / 1e3)
-
-    e2e_block = None
+    plain = {"value": round(world * nq * args.steps / (ms_p / 1e3), 1), "nprobe": nprobe,
+             "recall@100": round(recall, 5), "ms_per_step": round(ms_p / args.steps, 4)}
+    ms_pe = None
     if not args.no_e2e:
-        e2e_block = run_e2e(idx, query, k, nprobe, ids0, stream, args, world)
+        ms_pe, _, _ = timed(plain_host, args.steps, args.warmup, world, stream)
+        assert (ids_h.numpy().view(np.uint32) == ids0).all()
+        plain["e2e"] = round(world * nq * args.steps / (ms_pe / 1e3), 1)
+    scan_bytes_plain = int(nblocks[cids[:, :nprobe].astype(np.int64)].sum()) * block_bytes
 
+    # --- learned per-query depth
+    mode = "plain"
+    chosen = {"ms": ms_p, "prof": prof_p, "clocks": clocks_p, "recall": recall, "ids": ids0,
+              "scan_bytes": scan_bytes_plain, "e2e_ms": None}
+    learned_info = None
+    if not args.no_learned and cfg.get("train_queries"):
+        model, meta = learned_model(idx, d, cfg, nprobe)
+        used_h = np.empty(nq, np.uint32)
+        best = None
+        for conf in (0.5, 0.6, 0.7, 0.8, 0.9, 0.95, 0.99):
+            ids_l, _, used = learned.search_learned(idx, model, qrot_h, k, nprobe, conf)
+            r = metrics.recall_at_k(ids_l, gt, k)
+            log(f"learned confidence={conf}: recall@{k}={r:.4f}, mean nprobe "
+                f"{used.mean():.3f}")
+            if r >= target:
+                best = (conf, r, ids_l, used)
+                break
+        if best is not None:
+            conf, r_l, ids_l, used = best
+            used_d = torch.empty(nq, dtype=torch.int32, device="cuda")
+
+            def learned_dev():
+                learned.search_learned_buffers(idx, model, qd, k, nprobe, conf, ids_d, dist_d,
+                                               used_d, raw=True, stream=stream)
+
+            def learned_host():
+                learned.search_learned_buffers(idx, model, qh, k, nprobe, conf, ids_h, dist_h,
+                                               None, raw=True, stream=stream)
+
+            ms_l, prof_l, clocks_l = timed(learned_dev, args.steps, args.warmup, world, stream,
+                                           local)
+            assert (ids_d.cpu().numpy().view(np.uint32) == ids_l).all()
+            e2e_l = None
+            if not args.no_e2e:
+                e2e_l, _, _ = timed(learned_host, args.steps, args.warmup, world, stream)
+                assert (ids_h.numpy().view(np.uint32) == ids_l).all()
+            take = np.arange(cids.shape[1])[None, :] < used.astype(np.int64)[:, None]
+            scan_bytes_l = int(nblocks[cids.astype(np.int64)][take].sum()) * block_bytes
+            learned_info = {"value": round(world * nq * args.steps / (ms_l / 1e3), 1),
+                            "confidence": conf, "mean_nprobe": round(float(used.mean()), 4),
+                            "recall@100": round(r_l, 5),
+                            "ms_per_step": round(ms_l / args.steps, 4), "model": meta}
+            if e2e_l is not None:
+                learned_info["e2e"] = round(world * nq * args.steps / (e2e_l / 1e3), 1)
+            if ms_l < ms_p:
+                mode = "learned"
+                chosen = {"ms": ms_l, "prof": prof_l, "clocks": clocks_l, "recall": r_l,
+                          "ids": ids_l, "scan_bytes": scan_bytes_l, "e2e_ms": e2e_l}
+        model.free()
+
+    ratio = metrics.average_distance_ratio(query[:sub], base, chosen["ids"][:sub].astype(np.int64),
+                                           gt[:sub].astype(np.int64), k)
+    prof = chosen["prof"]
     scan_n, scan_ms = prof["scan"]
     launches = sum(v[0] for v in prof.values())
     peaks = {}
@@ -348,8 +421,9 @@ def run_ours(args, cfg, name):
     peak = peak or 6650.0
     achieved = None
     if scan_n:
-        per_launch_bytes = scan_bytes_per_step * args.steps / scan_n
+        per_launch_bytes = chosen["scan_bytes"] * args.steps / scan_n
         achieved = per_launch_bytes / (scan_ms / scan_n / 1e3) / 1e9
+    e2e_ms = chosen["e2e_ms"] if mode == "learned" else ms_pe
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         searcher, kind, note = cpu_searcher(index_path)
@@ -362,31 +436,39 @@ def run_ours(args, cfg, name):
                          f"{srch_s:.2f}s)" + (f"; {note}" if note else "")}
         searcher.close()
     if rank == 0:
+        ms = chosen["ms"]
         out = {
-            "metric": METRIC, "value": round(value, 1), "unit": "queries/s", "n_gpus": world,
+            "metric": METRIC, "value": round(world * nq * args.steps / (ms / 1e3), 1),
+            "unit": "queries/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(ms / args.steps, 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int32",
             "data": cfg["data"],
-            "config": {"workload": f"{name}: plain fixed-nprobe GPU search, "
-                                   f"{cfg['n']}x{cfg['dim']}, K={cfg['K']}, {cfg['bits']}-bit, "
-                                   f"{nq} queries per step, top-{k}",
-                       "nprobe": nprobe, "recall@100": round(recall, 5),
+            "config": {"workload": f"{name}: {'learned-probe' if mode == 'learned' else 'plain'} "
+                                   f"GPU search, {cfg['n']}x{cfg['dim']}, K={cfg['K']}, "
+                                   f"{cfg['bits']}-bit, {nq} queries per step, top-{k}",
+                       "mode": mode, "nprobe": nprobe, "recall@100": round(chosen["recall"], 5),
                        "distance_ratio": round(ratio, 5), "queries_per_step": nq,
                        "parallelism": f"replicas x{world} (queries replicated per GPU)",
                        "l2": "inputs larger than L2: every step streams "
-                             f"{scan_bytes_per_step / 1e9:.1f} GB of packed codes from a "
+                             f"{chosen['scan_bytes'] / 1e9:.1f} GB of packed codes from a "
                              f"{os.path.getsize(index_path) / 1e9:.2f} GB index"},
-            "e2e": e2e_block,
+            "plain_gpu": plain,
+            "learned_gpu": learned_info,
+            "e2e": None if e2e_ms is None else {
+                "value": round(world * nq * args.steps / (e2e_ms / 1e3), 1), "unit": "queries/s",
+                "h2d_bytes_per_step": int(nq * query.shape[1] * 4),
+                "d2h_bytes_per_step": int(nq * k * 8)},
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1) if achieved else None,
                          "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4) if achieved else None,
                          "traffic": None, "kernel": "scan_kernel",
                          "peak_source": f"{peak_src} hbm_gbs (copy)"},
-            "kernels_ms_per_step": {kk: round(v[1] / args.steps, 4) for kk, v in prof.items()},
+            "kernels_ms_per_step": {kk: round(v[1] / args.steps, 4) for kk, v in prof.items()
+                                    if v[0]},
             "cpu_baseline": cpu,
-            "clocks": clocks,
+            "clocks": chosen["clocks"],
         }
         print(json.dumps(out), flush=True)
     idx.free()
@@ -473,6 +555,7 @@ def main():
                     help="seconds of CPU search per step of the reference arm")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer e2e timing")
+    ap.add_argument("--no-learned", action="store_true", help="plain fixed-nprobe search only")
     ap.add_argument("--queries", type=int, default=0,
                     help="use only the first N queries of the batch (profiling cases)")
     ap.add_argument("--nprobe", type=int, default=0,

@@ -1406,12 +1406,14 @@ erq_status erq_probe_model_predict(const erq_probe_model* m, const float* featur
     return ERQ_OK;
 }
 
-erq_status erq_search_learned(const erq_index* idx, const erq_probe_model* m,
-                              const float* rotated_queries, uint64_t nq, uint64_t k,
-                              uint64_t nprobe_fallback, float confidence, float min_prob,
-                              uint32_t* ids, float* dists, uint32_t* nprobe_used, void* stream) {
+static erq_status search_learned_entry(const erq_index* idx, const erq_probe_model* m,
+                                       const float* queries, bool rotated, uint64_t nq,
+                                       uint64_t k, uint64_t nprobe_fallback, float confidence,
+                                       float min_prob, uint32_t* ids, float* dists,
+                                       uint32_t* nprobe_used, void* stream) {
     if (!m) return fail(ERQ_ERR_INVALID_ARGUMENT, "model is NULL");
-    ERQ_TRY(check_search_args(idx, nq, k, nprobe_fallback, rotated_queries, ids));
+    const float* rotated_queries = queries;
+    ERQ_TRY(check_search_args(idx, nq, k, nprobe_fallback, queries, ids));
     if (nq == 0) return ERQ_OK;
     if (m->device != idx->device)
         return fail(ERQ_ERR_INVALID_ARGUMENT, "model and index are on different devices");
@@ -1427,11 +1429,18 @@ erq_status erq_search_learned(const erq_index* idx, const erq_probe_model* m,
     const bool d_dev = dists == nullptr || is_device_ptr(dists);
     const bool u_dev = nprobe_used == nullptr || is_device_ptr(nprobe_used);
     Scratch s(st, idx->pool);
+    const uint64_t in_cols = rotated ? idx->D : idx->DIM;
     const float* q = rotated_queries;
     if (!q_dev || (reinterpret_cast<uintptr_t>(q) & 15)) {
         float* tmp = nullptr;
+        ERQ_TRY(s.alloc(&tmp, nq * in_cols));
+        ERQ_CUDA(cudaMemcpyAsync(tmp, rotated_queries, nq * in_cols * 4, cudaMemcpyDefault, st));
+        q = tmp;
+    }
+    if (!rotated) {
+        float* tmp = nullptr;
         ERQ_TRY(s.alloc(&tmp, nq * idx->D));
-        ERQ_CUDA(cudaMemcpyAsync(tmp, rotated_queries, nq * idx->D * 4, cudaMemcpyDefault, st));
+        ERQ_TRY(rotate_device(idx, q, nq, tmp, st));
         q = tmp;
     }
     uint32_t* ids_out = ids;
@@ -1474,6 +1483,23 @@ erq_status erq_search_learned(const erq_index* idx, const erq_probe_model* m,
         ERQ_CUDA(cudaMemcpyAsync(dists, d_out, nq * k * 4, cudaMemcpyDeviceToHost, st));
     if (!q_dev || !ids_dev || !d_dev || !u_dev) ERQ_CUDA(cudaStreamSynchronize(st));
     return ERQ_OK;
+}
+
+erq_status erq_search_learned(const erq_index* idx, const erq_probe_model* m,
+                              const float* rotated_queries, uint64_t nq, uint64_t k,
+                              uint64_t nprobe_fallback, float confidence, float min_prob,
+                              uint32_t* ids, float* dists, uint32_t* nprobe_used, void* stream) {
+    return search_learned_entry(idx, m, rotated_queries, true, nq, k, nprobe_fallback, confidence,
+                                min_prob, ids, dists, nprobe_used, stream);
+}
+
+erq_status erq_search_learned_raw(const erq_index* idx, const erq_probe_model* m,
+                                  const float* queries, uint64_t nq, uint64_t k,
+                                  uint64_t nprobe_fallback, float confidence, float min_prob,
+                                  uint32_t* ids, float* dists, uint32_t* nprobe_used,
+                                  void* stream) {
+    return search_learned_entry(idx, m, queries, false, nq, k, nprobe_fallback, confidence,
+                                min_prob, ids, dists, nprobe_used, stream);
 }
 
 erq_status erq_debug_probe_model_grads(const erq_probe_model* m, const float* features,

@@ -133,46 +133,6 @@ __device__ __forceinline__ float ex_ip_thread(const float* __restrict__ uq,
     return __fadd_rn(__fadd_rn(t6[0], t6[2]), __fadd_rn(t6[1], t6[3]));
 }
 
-// ResultPool::insert + distk (inc/index/Pool.hpp:15-31) on a pool held in
-// shared memory, executed by the whole warp.
-__device__ __forceinline__ void pool_insert(float* pool_d, uint32_t* pool_id, int& size, int k,
-                                            float& distk, float dnew, uint32_t inew, int lane) {
-    if (size == k && dnew > pool_d[size - 1]) return;
-    // lower_bound: number of entries < dnew
-    int lo = 0;
-    for (int i0 = 0; i0 < size; i0 += 32) {
-        const int i = i0 + lane;
-        const bool lt = i < size && pool_d[i] < dnew;
-        lo += __popc(__ballot_sync(0xffffffffu, lt));
-    }
-    // shift [lo, last) up by one; when full the entry at k-1 falls off.
-    // Chunks of 32 from the top down: each chunk is read before the chunk
-    // below writes into its first slot.
-    const int last = size < k ? size : k - 1;
-    for (int i0 = lo + ((last - lo - 1) >> 5) * 32; last > lo && i0 >= lo; i0 -= 32) {
-        const int i = i0 + lane;
-        float sv = 0.f;
-        uint32_t si = 0u;
-        if (i < last) {
-            sv = pool_d[i];
-            si = pool_id[i];
-        }
-        __syncwarp();
-        if (i < last) {
-            pool_d[i + 1] = sv;
-            pool_id[i + 1] = si;
-        }
-        __syncwarp();
-    }
-    if (lane == 0) {
-        pool_d[lo] = dnew;
-        pool_id[lo] = inew;
-    }
-    __syncwarp();
-    size += size < k;
-    distk = size == k ? pool_d[k - 1] : FLT_MAX;
-}
-
 constexpr int kRefineThreads = 128;     // 4 warps per query
 constexpr int kWindowBlocks = 16;       // blocks whose candidates are refined together
 constexpr int kWindowLanes = kWindowBlocks * 32;
@@ -180,13 +140,102 @@ constexpr int kWindowLanes = kWindowBlocks * 32;
 // Shared memory of one block: unit_q[D] | per window lane: lb, ipq, onorm,
 // ex_dist, id, list | pool_d[kpad] | pool_id[kpad] | misc
 __host__ __device__ constexpr size_t refine_smem_bytes_per_query(int D, int kpad) {
-    return (size_t)D * 4 + (size_t)kWindowLanes * (5 * 4 + 2) + (size_t)kpad * 8 + 64;
+    return (size_t)D * 4 + (size_t)kWindowLanes * (5 * 4 + 2) + (size_t)kpad * 8 + 64 + 128;
 }
 
-// One block of 4 warps per query.  Per window of 16 blocks of the current
-// cluster: every warp computes the lower bounds of 4 blocks and lists the
-// lanes below the threshold as it stands at the window's start (a superset of
-// the exact candidates, because the threshold only falls); all 128 threads
+// Order key: ascending distance (-0 equal to +0, as float compares see it);
+// among equal distances the higher lane, offered to the pool later, first.
+// Non-candidates sort last.
+__device__ __forceinline__ uint64_t merge_key(float d, int lane, bool cand) {
+    const uint32_t b = __float_as_uint(d == 0.f ? 0.f : d);
+    const uint32_t o = (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+    return cand ? (((uint64_t)o << 32) | (uint32_t)(31 - lane)) : ~0ull;
+}
+
+// Offers one block's candidates (lanes with `cand`, distance d, id) to the
+// pool in ascending lane order, as ResultPool::insert does one at a time
+// (inc/index/Pool.hpp:15-26), in one parallel step.  Each insert keeps the k
+// smallest entries under the order (distance, newer first): lower_bound
+// places a new value before equal ones, an equal value still enters a full
+// pool and pushes the last one out, a larger one is rejected.  A sequence of
+// inserts therefore leaves the k smallest of (pool + sequence) in that order:
+// sort the candidates by (distance, later lane first); pool entry i moves to
+// i + #(candidates <= it), candidate j goes to j + #(pool entries < it), and
+// ranks >= k fall off.  Executed by one whole warp; `cs` is 32 floats of
+// scratch.
+__device__ __forceinline__ void pool_merge_block(float* pool_d, uint32_t* pool_id, int& size, int k,
+                                                 float& distk, bool cand, float d, uint32_t id,
+                                                 float* cs, int lane) {
+    const int nc = __popc(__ballot_sync(0xffffffffu, cand));
+    uint64_t key = merge_key(d, lane, cand);
+    uint32_t val = id;
+    float dv = d;
+#pragma unroll
+    for (int sz = 2; sz <= 32; sz <<= 1) {
+#pragma unroll
+        for (int st = sz >> 1; st > 0; st >>= 1) {
+            const uint64_t ok = __shfl_xor_sync(0xffffffffu, key, st);
+            const uint32_t ov = __shfl_xor_sync(0xffffffffu, val, st);
+            const float od = __shfl_xor_sync(0xffffffffu, dv, st);
+            const bool take_min = ((lane & st) == 0) == ((lane & sz) == 0);
+            if (take_min ? (ok < key) : (ok > key)) {
+                key = ok;
+                val = ov;
+                dv = od;
+            }
+        }
+    }
+    // lane j holds the j-th candidate
+    cs[lane] = dv;
+    int lo = 0;
+    if (lane < nc) {
+        int hi = size;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (pool_d[mid] < dv) lo = mid + 1; else hi = mid;
+        }
+    }
+    const int rc = lane < nc ? lane + lo : k;
+    const int first = __shfl_sync(0xffffffffu, lo, 0);  // entries below it stay put
+    __syncwarp();
+    // move pool entries, top chunk first: entry i goes to i + c(i) >= i, and
+    // i + c(i) strictly increases with i, so no chunk overwrites an entry
+    // that has not been read or one already moved
+    for (int i0 = ((size - 1) >> 5) << 5; i0 >= 0 && i0 + 31 >= first; i0 -= 32) {
+        const int i = i0 + lane;
+        float pd = 0.f;
+        uint32_t pid = 0u;
+        int pr = k;
+        if (i < size) {
+            pd = pool_d[i];
+            pid = pool_id[i];
+            int l2 = 0, h2 = nc;
+            while (l2 < h2) {
+                const int mid = (l2 + h2) >> 1;
+                if (cs[mid] <= pd) l2 = mid + 1; else h2 = mid;
+            }
+            pr = i + l2;
+        }
+        __syncwarp();
+        if (pr < k) {
+            pool_d[pr] = pd;
+            pool_id[pr] = pid;
+        }
+        __syncwarp();
+    }
+    if (rc < k) {
+        pool_d[rc] = dv;
+        pool_id[rc] = val;
+    }
+    __syncwarp();
+    size = min(k, size + nc);
+    distk = size == k ? pool_d[k - 1] : FLT_MAX;
+}
+
+// One block of 4 warps per query.  Per window of up to 16 blocks of the
+// current cluster: every warp computes the lower bounds of 4 blocks and lists
+// the lanes below the threshold as it stands at the window's start (a superset
+// of the exact candidates, because the threshold only falls); all 128 threads
 // refine the listed candidates, one each; warp 0 then replays the window in
 // the reference's order - each block's mask against the threshold at that
 // block's start, candidates in ascending lane order - inserting into the pool.
@@ -206,8 +255,9 @@ __global__ void __launch_bounds__(kRefineThreads) refine_kernel(RefineArgs a) {
     uint16_t* w_list = reinterpret_cast<uint16_t*>(w_id + kWindowLanes);
     float* pool_d = reinterpret_cast<float*>(w_list + kWindowLanes);
     uint32_t* pool_id = reinterpret_cast<uint32_t*>(pool_d + kpad);
-    int* misc = reinterpret_cast<int*>(pool_id + kpad);  // [0] list count
-    float* s_distk = reinterpret_cast<float*>(misc + 1);
+    int* misc = reinterpret_cast<int*>(pool_id + kpad);  // [0] list count [1] pool size
+    float* s_distk = reinterpret_cast<float*>(misc + 2);
+    float* cs = reinterpret_cast<float*>(misc + 16);  // 32 floats of merge scratch
     const int code_len = D * EX / 8;
     const int fac_rescale = 1 << EX;
     const float one_over_sqrtD = recip_via_double(__fsqrt_rn((float)D));
@@ -217,7 +267,10 @@ __global__ void __launch_bounds__(kRefineThreads) refine_kernel(RefineArgs a) {
         pool_d[i] = 0.f;
         pool_id[i] = 0u;
     }
-    if (tid == 0) *s_distk = FLT_MAX;
+    if (tid == 0) {
+        *s_distk = FLT_MAX;
+        misc[1] = 0;  // pool size as seen by all warps
+    }
     int size = 0;         // pool state, maintained by warp 0
     float distk = FLT_MAX;
     __syncthreads();
@@ -241,15 +294,21 @@ __global__ void __launch_bounds__(kRefineThreads) refine_kernel(RefineArgs a) {
         const int32_t* S = a.S + a.s_off[qp];
         const uint32_t nblocks = (n + 31) >> 5;
         bool uq_ready = false;
-        for (uint32_t wb = 0; wb < nblocks; wb += kWindowBlocks) {
-            const int nbw = (int)min((uint32_t)kWindowBlocks, nblocks - wb);
+        for (uint32_t wb = 0; wb < nblocks;) {
             const float d0 = *s_distk;
+            const int filled = misc[1];
+            // While the pool is filling every lane is a candidate: take just
+            // enough blocks to fill it, so few lanes are refined in vain.
+            const int want = filled < k ? min(kWindowBlocks, max(1, (k - filled + 31) / 32))
+                                        : kWindowBlocks;
+            const int nbw = (int)min((uint32_t)want, nblocks - wb);
+            __syncthreads();
             if (tid == 0) misc[0] = 0;
             __syncthreads();
             // lower bounds and the candidate superset, 4 blocks per warp
 #pragma unroll
-            for (int i = 0; i < kWindowBlocks / 4; ++i) {
-                const int b = warp * (kWindowBlocks / 4) + i;
+            for (int i = 0; i < kWindowBlocks / (kRefineThreads / 32); ++i) {
+                const int b = warp * (kWindowBlocks / (kRefineThreads / 32)) + i;
                 if (b < nbw) {  // uniform per warp
                     const uint32_t blk = wb + b;
                     const float ipq = __fmul_rn(__int2float_rn(S[32 * blk + lane]), delta);
@@ -274,7 +333,10 @@ __global__ void __launch_bounds__(kRefineThreads) refine_kernel(RefineArgs a) {
             }
             __syncthreads();
             const int cnt = misc[0];
-            if (cnt == 0) continue;  // uniform: nothing in this window can pass
+            if (cnt == 0) {  // uniform: nothing in this window can pass
+                wb += nbw;
+                continue;
+            }
             if (!uq_ready) {
                 const float* cv = a.centroids + (size_t)cid * D;
                 if (y > kNormEps) {
@@ -309,17 +371,18 @@ __global__ void __launch_bounds__(kRefineThreads) refine_kernel(RefineArgs a) {
             __syncthreads();
             if (warp == 0) {
                 for (int b = 0; b < nbw; ++b) {
-                    uint32_t mask = __ballot_sync(0xffffffffu, w_lb[32 * b + lane] < distk);
-                    while (mask) {
-                        const int j = __ffs(mask) - 1;
-                        mask &= mask - 1;
-                        pool_insert(pool_d, pool_id, size, k, distk, w_ed[32 * b + j],
-                                    w_id[32 * b + j], lane);
-                    }
+                    const bool cand = w_lb[32 * b + lane] < distk;
+                    if (__ballot_sync(0xffffffffu, cand))
+                        pool_merge_block(pool_d, pool_id, size, k, distk, cand, w_ed[32 * b + lane],
+                                         w_id[32 * b + lane], cs, lane);
                 }
-                if (lane == 0) *s_distk = distk;
+                if (lane == 0) {
+                    *s_distk = distk;
+                    misc[1] = size;
+                }
             }
             __syncthreads();
+            wb += nbw;
         }
     }
     if (warp == 0) {

@@ -33,6 +33,7 @@ EXPORTED_SYMBOLS = (
     "erq_profile_enable", "erq_profile_reset", "erq_profile_read",
     "erq_probe_features", "erq_probe_model_train", "erq_probe_model_save", "erq_probe_model_load",
     "erq_probe_model_free", "erq_probe_model_predict", "erq_search_learned",
+    "erq_search_learned_raw",
     "erq_debug_probe_model_grads", "erq_debug_probe_model_params",
 )
 
@@ -117,6 +118,8 @@ def load_library(path: str | None = None) -> C.CDLL:
     lib.erq_search_learned.argtypes = [vp, vp, f32p, u64, u64, u64, C.c_float, C.c_float, u32p,
                                        f32p, vp, vp]
     lib.erq_search_learned.restype = C.c_int
+    lib.erq_search_learned_raw.argtypes = lib.erq_search_learned.argtypes
+    lib.erq_search_learned_raw.restype = C.c_int
     lib.erq_debug_probe_model_grads.argtypes = [vp, vp, vp, u64, C.POINTER(C.c_float), vp]
     lib.erq_debug_probe_model_grads.restype = C.c_int
     lib.erq_debug_probe_model_params.argtypes = [vp, vp, vp, vp, vp]

@@ -131,3 +131,16 @@ def search_learned(ivf, model: ProbeModel, rotated_queries, k: int, nprobe_fallb
                                             nprobe_fallback, confidence, min_prob, ids.ctypes.data,
                                             d.ctypes.data, used.ctypes.data, st))
     return ids, d, used
+
+
+def search_learned_buffers(ivf, model: ProbeModel, queries, k: int, nprobe_fallback: int,
+                           confidence: float, ids, dists, used=None, raw: bool = True,
+                           min_prob: float = 0.0, stream=None) -> None:
+    """Learned search into caller buffers (numpy arrays or torch tensors, host
+    or device): raw DIM-float queries when `raw`, else rotated ones."""
+    ptr = lambda t: None if t is None else C.c_void_p(  # noqa: E731
+        t.data_ptr() if hasattr(t, "data_ptr") else t.ctypes.data)
+    fn = load_library().erq_search_learned_raw if raw else load_library().erq_search_learned
+    st = None if stream is None else C.c_void_p(stream.cuda_stream)
+    check(fn(ivf._h, model._h, ptr(queries), int(queries.shape[0]), k, nprobe_fallback,
+             confidence, min_prob, ptr(ids), ptr(dists), ptr(used), st))

@@ -133,6 +133,13 @@ ERQ_API erq_status erq_search_learned(const erq_index* index, const erq_probe_mo
                                       uint32_t* ids, float* dists, uint32_t* nprobe_used,
                                       void* stream);
 
+/* The same with raw DIM-float queries, rotated inside (test_search's sequence). */
+ERQ_API erq_status erq_search_learned_raw(const erq_index* index, const erq_probe_model* model,
+                                          const float* queries, uint64_t nq, uint64_t k,
+                                          uint64_t nprobe_fallback, float confidence,
+                                          float min_prob, uint32_t* ids, float* dists,
+                                          uint32_t* nprobe_used, void* stream);
+
 /* erq_search without any memory allocation.  Has no counterpart in the
  * reference: it is for callers that cannot allocate device memory while a
  * query runs - engines that hand all GPU memory to their own allocator up
