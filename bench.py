@@ -26,6 +26,7 @@ import json
 import os
 import statistics
 import subprocess
+import threading
 import sys
 import time
 
@@ -126,8 +127,13 @@ CLOCK_FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.a
 
 
 class ClockSampler:
+    """nvidia-smi samples every 100 ms on a reader thread; only samples taken
+    between mark_start() and mark_end() (the timed region) are summarised."""
+
     def __init__(self, gpu_index: int):
         self.proc = None
+        self.samples = []
+        self.t0 = self.t1 = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={CLOCK_FIELDS}", "--format=csv,noheader,nounits",
@@ -135,15 +141,37 @@ class ClockSampler:
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
+            return
+        self.first = threading.Event()
+        self.reader = threading.Thread(target=self._read, daemon=True)
+        self.reader.start()
+        self.first.wait(timeout=10.0)
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append((time.monotonic(), line))
+            self.first.set()
+
+    def mark_start(self):
+        self.t0 = time.monotonic()
+
+    def mark_end(self):
+        self.t1 = time.monotonic()
 
     def stop(self):
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
         self.proc.terminate()
-        out, _ = self.proc.communicate(timeout=10)
+        self.proc.wait(timeout=10)
+        self.reader.join(timeout=5)
         sm, smax, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in out.strip().splitlines():
+        t0 = self.t0 if self.t0 is not None else 0.0
+        t1 = (self.t1 if self.t1 is not None else time.monotonic()) + 0.15
+        for t, line in self.samples:
+            if not (t0 <= t <= t1):
+                continue
             f = [x.strip() for x in line.split(",")]
             if len(f) < 9:
                 continue
@@ -257,11 +285,15 @@ def timed(step, steps, warmup, world, stream, clock_gpu=None):
     L.profile_reset()
     L.profile_enable(True)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if sampler:
+        sampler.mark_start()
     e0.record(stream)
     for _ in range(steps):
         step()
     e1.record(stream)
     torch.cuda.synchronize()
+    if sampler:
+        sampler.mark_end()
     L.profile_enable(False)
     barrier(world)
     clocks = sampler.stop() if sampler else None
@@ -513,9 +545,11 @@ def run_reference(args, cfg, name):
     per_step = []
     samples = []
     offset = 0
+    # each step a bounded sample, so that the whole run stays near two minutes
+    step_s = min(args.ref_step_s, max(0.3, 120.0 / (args.warmup + args.steps)))
     for s in range(args.warmup + args.steps):
         qs = np.roll(query, -offset, axis=0)
-        qps, n, sec, _, _ = time_cpu(searcher, kind, qs, k, nprobe, threads, args.ref_step_s, nq)
+        qps, n, sec, _, _ = time_cpu(searcher, kind, qs, k, nprobe, threads, step_s, nq)
         offset = (offset + n) % nq
         if s >= args.warmup:
             per_step.append(sec)
@@ -532,7 +566,7 @@ def run_reference(args, cfg, name):
                                f"of the {nq}-query batch, top-{k}", "nprobe": nprobe},
         "cpu_baseline": {"value": round(value, 2), "unit": "queries/s", "cores": threads,
                          "kind": kind,
-                         "sample": f"{args.steps} steps of ~{args.ref_step_s:.0f}s each, "
+                         "sample": f"{args.steps} steps of ~{step_s:.2f}s each, "
                                    f"{total_q} queries total at nprobe={nprobe} incl. the "
                                    "reference's own query rotation" + (f"; {note}" if note else "")},
         "e2e": {"value": round(value, 2), "unit": "queries/s", "h2d_bytes_per_step": 0,
@@ -545,7 +579,7 @@ def run_reference(args, cfg, name):
 def main():
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--config", choices=sorted(CONFIGS), default=DEFAULT_CONFIG)

@@ -194,7 +194,8 @@ struct erq_index {
     float* centroids = nullptr;
     uint8_t* codes = nullptr;
     float* onorm = nullptr;
-    uint8_t* excode = nullptr;
+    uint8_t* excode = nullptr;      // device layout, ex_row bytes per vector
+    uint64_t ex_row = 0;
     float* xipnorm = nullptr;
     uint32_t* ids = nullptr;
     uint32_t* c_first_block = nullptr;
@@ -343,8 +344,31 @@ erq_status load_impl(const char* path, erq_index* idx) {
         cudaFree(raw);
         if (s != ERQ_OK) return s;
     }
-    ERQ_TRY(dev_alloc(idx, &idx->excode, N * code_len + 64));
-    ERQ_TRY(read_to_device(f.get(), idx->excode, N * code_len, staging, "the EX-bit codes"));
+    idx->ex_row = ex_row_bytes((int)D, (int)EX);
+    ERQ_TRY(dev_alloc(idx, &idx->excode, std::max<uint64_t>(N * idx->ex_row, 64)));
+    {
+        uint8_t* raw = nullptr;
+        cudaError_t e = cudaMalloc(&raw, std::max<uint64_t>(N * code_len, 16));
+        if (e != cudaSuccess) return fail(ERQ_ERR_OUT_OF_MEMORY, "cudaMalloc for EX-bit codes failed");
+        erq_status s = read_to_device(f.get(), raw, N * code_len, staging, "the EX-bit codes");
+        if (s == ERQ_OK && N > 0) {
+            uint32_t* dst = reinterpret_cast<uint32_t*>(idx->excode);
+            switch (EX) {
+                case 2: transform_excode_kernel<2><<<2368, 256>>>(raw, dst, N, (int)D); break;
+                case 3: transform_excode_kernel<3><<<2368, 256>>>(raw, dst, N, (int)D); break;
+                case 4: transform_excode_kernel<4><<<2368, 256>>>(raw, dst, N, (int)D); break;
+                case 6: transform_excode_kernel<6><<<2368, 256>>>(raw, dst, N, (int)D); break;
+                case 7: transform_excode_kernel<7><<<2368, 256>>>(raw, dst, N, (int)D); break;
+                default: transform_excode_kernel<8><<<2368, 256>>>(raw, dst, N, (int)D); break;
+            }
+            e = cudaGetLastError();
+            if (e == cudaSuccess) e = cudaDeviceSynchronize();
+            if (e != cudaSuccess)
+                s = fail(ERQ_ERR_CUDA, "EX-code layout kernel failed: %s", cudaGetErrorString(e));
+        }
+        cudaFree(raw);
+        if (s != ERQ_OK) return s;
+    }
     ERQ_TRY(dev_alloc(idx, &idx->xipnorm, N));
     ERQ_TRY(read_to_device(f.get(), idx->xipnorm, N * sizeof(float), staging, "the EX factors"));
     ERQ_TRY(dev_alloc(idx, &idx->ids, N));
@@ -586,6 +610,7 @@ erq_status launch_refine(const erq_index* idx, const Batch& b, uint64_t nprobe, 
     a.qp_sumq = b.sumq;
     a.onorm = idx->onorm;
     a.excode = idx->excode;
+    a.ex_row = idx->ex_row;
     a.xipnorm = idx->xipnorm;
     a.ids = idx->ids;
     a.c_first_block = idx->c_first_block;

@@ -19,6 +19,7 @@
 #include <cfloat>
 
 #include "common.cuh"
+#include "layout.cuh"
 
 namespace erq {
 
@@ -32,7 +33,8 @@ struct RefineArgs {
     const float* qp_delta;        // [nq][nprobe]
     const float* qp_sumq;         // [nq][nprobe]
     const float* onorm;           // [blocks*32]
-    const uint8_t* excode;        // [N][D*EX/8]
+    const uint8_t* excode;        // [N][ex_row] device layout (layout.cuh)
+    uint64_t ex_row;              // bytes per EX-code row
     const float* xipnorm;         // [N]
     const uint32_t* ids;          // [N]
     const uint32_t* c_first_block; // [K]
@@ -45,92 +47,102 @@ struct RefineArgs {
 };
 
 
-// float(v) for 0 <= v < 256 held in byte `i` of `w`: 0x4B0000vv is 2^23 + v.
-__device__ __forceinline__ float byte_to_float(uint32_t w, int i) {
-    return __fsub_rn(__int_as_float((int)__byte_perm(w, 0x4B000000u, 0x7540u | (uint32_t)i)),
-                     8388608.f);
+// Packed FP32 pairs (sm_100a f32x2): two independent IEEE round-to-nearest
+// operations per instruction, each equal to its scalar counterpart.
+__device__ __forceinline__ float2 ffma2(float2 a, float2 b, float2 c) {
+    uint64_t d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;"
+        : "=l"(d)
+        : "l"(*reinterpret_cast<const uint64_t*>(&a)), "l"(*reinterpret_cast<const uint64_t*>(&b)),
+          "l"(*reinterpret_cast<const uint64_t*>(&c)));
+    return *reinterpret_cast<float2*>(&d);
+}
+__device__ __forceinline__ float2 fsub2(float2 a, float2 b) {
+    uint64_t d;
+    asm("sub.rn.f32x2 %0, %1, %2;"
+        : "=l"(d)
+        : "l"(*reinterpret_cast<const uint64_t*>(&a)), "l"(*reinterpret_cast<const uint64_t*>(&b)));
+    return *reinterpret_cast<float2*>(&d);
 }
 
-// Four consecutive dims (16*sub + 4*qd .. +3 of a 64-dim group) of one EX-bit
-// code as bytes of a word.  `w` holds the group's 8*EX bytes as 2*EX words.
-// Layouts: store_compacted_code, inc/index/Quantizer.hpp:491-631.
-template <int EX>
-__device__ __forceinline__ uint32_t ex_quad(const uint32_t* w, int sub, int qd) {
-    if (EX == 8) {
-        return w[4 * sub + qd];
-    } else if (EX == 4) {  // per 32 dims: 16 bytes, low nibble = dims 0-15
-        const uint32_t c = w[4 * (sub >> 1) + qd];
-        return (sub & 1) ? ((c >> 4) & 0x0F0F0F0Fu) : (c & 0x0F0F0F0Fu);
-    } else if (EX == 2 || EX == 3) {  // 2 bits at 2*sub of bytes 0-15
-        uint32_t v = (w[qd] >> (2 * sub)) & 0x03030303u;
-        if (EX == 3) {
-            // bit j of byte m of the top word = bit 2 of dim 8j + m; these
-            // dims have m = (4qd .. 4qd+3) % 8 and j = 2*sub + qd/2
-            const uint32_t t = w[4 + (qd & 1)];
-            const int j = 2 * sub + (qd >> 1);
-            v |= ((j <= 2) ? (t << (2 - j)) : (t >> (j - 2))) & 0x04040404u;
-        }
-        return v;
-    } else {  // EX == 6 || EX == 7: c1 = bytes 0-15, c2 = 16-31, c3 = 32-47
-        const uint32_t c1 = w[qd], c2 = w[4 + qd], c3 = w[8 + qd];
-        uint32_t v;
-        if (sub == 0) {
-            v = c1 & 0x3F3F3F3Fu;
-        } else if (sub == 1) {
-            v = c2 & 0x3F3F3F3Fu;
-        } else if (sub == 2) {
-            v = ((c1 >> 2) & 0x30303030u) | (c3 & 0x0F0F0F0Fu);
-        } else {
-            v = ((c2 >> 2) & 0x30303030u) | ((c3 >> 4) & 0x0F0F0F0Fu);
-        }
-        if (EX == 7) {  // bit 6 from the top word (after 48 bytes)
-            const uint32_t t = w[12 + (qd & 1)];
-            const int j = 2 * sub + (qd >> 1);
-            v |= ((j <= 6) ? (t << (6 - j)) : (t >> (j - 6))) & 0x40404040u;
-        }
-        return v;
-    }
+// Codes of bytes (lo, lo+1) of w as exact floats: 0x4B0000vv is 2^23 + v.
+__device__ __forceinline__ float2 code_pair(uint32_t w, int lo) {
+    const float2 big = make_float2(__int_as_float((int)__byte_perm(w, 0x4B000000u, 0x7540u | (uint32_t)lo)),
+                                   __int_as_float((int)__byte_perm(w, 0x4B000000u, 0x7540u | (uint32_t)(lo + 1))));
+    return fsub2(big, make_float2(8388608.f, 8388608.f));
 }
 
-// <unit_q, ex code> computed by one thread in the reference's order:
-// accumulator l takes fma(unit_q[16s+l], code[16s+l], acc[l]) for s = 0,1,...
-// then the reduce tree (IP*_fxu* in inc/utils/space.hpp).  unit_q is in
-// shared memory and read as broadcasts (all lanes walk the same dims).
-template <int EX>
-__device__ __forceinline__ float ex_ip_thread(const float* __restrict__ uq,
-                                              const uint8_t* __restrict__ code, int D) {
-    float acc[16];
+// Codes of step t (0 <= t < 32/SB) of a lane's uint4 as 4 bytes.
+template <int SB>
+__device__ __forceinline__ uint32_t step_word(const uint4& v, int t) {
+    const uint32_t c[4] = {v.x, v.y, v.z, v.w};
+    if (SB == 8) return c[t];
+    if (SB == 4) return (c[t >> 1] >> (4 * (t & 1))) & 0x0F0F0F0Fu;
+    return (c[t >> 2] >> (2 * (t & 3))) & 0x03030303u;
+}
+
+// One step of one candidate: accumulators 4r+0..4r+3 of the reference's 16
+// (as two pairs) take fma(unit_q[16s + 4r + i], code, acc).
+__device__ __forceinline__ void ip_step(float2 acc[2], const float4& u, uint32_t w) {
+    acc[0] = ffma2(make_float2(u.x, u.y), code_pair(w, 0), acc[0]);
+    acc[1] = ffma2(make_float2(u.z, u.w), code_pair(w, 2), acc[1]);
+}
+
+// <unit_q, ex code> of NC (1 or 2) candidates by the 4 lanes r = 0..3 of a
+// quad, in the reference's order (IP*_fxu* in inc/utils/space.hpp): the 16
+// accumulators acc[l] take the dims l, l+16, l+32, ... in turn; lane r holds
+// acc[4r..4r+3].  Rows are in the lane-interleaved layout of layout.cuh;
+// each lane streams its own uint4s, two ahead.  uq4 = unit_q as float4.
+// Returns the sums (the reduce tree: acc[l] + acc[l+8], then + 4, then
+// (0 + 2) + (1 + 3)) in every lane of the quad.
+template <int SB, int NC>
+__device__ __forceinline__ void ex_ip_quad(const float4* __restrict__ uq4, const uint4* __restrict__ row0,
+                                           const uint4* __restrict__ row1, int r, int steps,
+                                           float out[2]) {
+    constexpr int SPU = 32 / SB;  // steps per uint4
+    const int U = (steps + SPU - 1) / SPU;
+    float2 acc[NC][2];
 #pragma unroll
-    for (int l = 0; l < 16; ++l) acc[l] = 0.f;
-    const uint2* src = reinterpret_cast<const uint2*>(code);
-    for (int t = 0; t < (D >> 6); ++t) {
-        uint32_t w[2 * EX];
+    for (int c = 0; c < NC; ++c) acc[c][0] = acc[c][1] = make_float2(0.f, 0.f);
+    const uint4* rows[2] = {row0 + r, row1 + r};
+    uint4 cur[NC], nxt[NC];
 #pragma unroll
-        for (int i = 0; i < EX; ++i) {
-            const uint2 x = __ldg(src + EX * t + i);
-            w[2 * i] = x.x;
-            w[2 * i + 1] = x.y;
+    for (int c = 0; c < NC; ++c) {
+        cur[c] = __ldg(rows[c]);
+        nxt[c] = U > 1 ? __ldg(rows[c] + 4) : make_uint4(0, 0, 0, 0);
+    }
+    const int Uf = steps / SPU;  // uint4s whose steps are all real
+    for (int u = 0; u < Uf; ++u) {
+        uint4 nn[NC];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) nn[c] = u + 2 < U ? __ldg(rows[c] + 4 * (u + 2)) : make_uint4(0, 0, 0, 0);
+#pragma unroll
+        for (int t = 0; t < SPU; ++t) {
+            const float4 q = uq4[4 * (u * SPU + t) + r];
+#pragma unroll
+            for (int c = 0; c < NC; ++c) ip_step(acc[c], q, step_word<SB>(cur[c], t));
         }
-        const float4* u4 = reinterpret_cast<const float4*>(uq + 64 * t);
 #pragma unroll
-        for (int sub = 0; sub < 4; ++sub) {
-#pragma unroll
-            for (int qd = 0; qd < 4; ++qd) {
-                const uint32_t v = ex_quad<EX>(w, sub, qd);
-                const float4 u = u4[4 * sub + qd];
-                acc[4 * qd + 0] = __fmaf_rn(u.x, byte_to_float(v, 0), acc[4 * qd + 0]);
-                acc[4 * qd + 1] = __fmaf_rn(u.y, byte_to_float(v, 1), acc[4 * qd + 1]);
-                acc[4 * qd + 2] = __fmaf_rn(u.z, byte_to_float(v, 2), acc[4 * qd + 2]);
-                acc[4 * qd + 3] = __fmaf_rn(u.w, byte_to_float(v, 3), acc[4 * qd + 3]);
-            }
+        for (int c = 0; c < NC; ++c) {
+            cur[c] = nxt[c];
+            nxt[c] = nn[c];
         }
     }
-    float t3[8], t6[4];
+    for (int t = 0; t < steps - Uf * SPU; ++t) {  // a partly filled last uint4
+        const float4 q = uq4[4 * (Uf * SPU + t) + r];
 #pragma unroll
-    for (int l = 0; l < 8; ++l) t3[l] = __fadd_rn(acc[l + 8], acc[l]);
+        for (int c = 0; c < NC; ++c) ip_step(acc[c], q, step_word<SB>(cur[c], t));
+    }
 #pragma unroll
-    for (int m = 0; m < 4; ++m) t6[m] = __fadd_rn(t3[m + 4], t3[m]);
-    return __fadd_rn(__fadd_rn(t6[0], t6[2]), __fadd_rn(t6[1], t6[3]));
+    for (int c = 0; c < NC; ++c) {
+        float t3[4], t6[4];
+        const float a4[4] = {acc[c][0].x, acc[c][0].y, acc[c][1].x, acc[c][1].y};
+#pragma unroll
+        for (int i = 0; i < 4; ++i) t3[i] = __fadd_rn(__shfl_xor_sync(0xffffffffu, a4[i], 2), a4[i]);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) t6[i] = __fadd_rn(__shfl_xor_sync(0xffffffffu, t3[i], 1), t3[i]);
+        out[c] = __fadd_rn(__fadd_rn(t6[0], t6[2]), __fadd_rn(t6[1], t6[3]));
+    }
 }
 
 constexpr int kRefineThreads = 128;     // 4 warps per query
@@ -258,7 +270,6 @@ __global__ void __launch_bounds__(kRefineThreads) refine_kernel(RefineArgs a) {
     int* misc = reinterpret_cast<int*>(pool_id + kpad);  // [0] list count [1] pool size
     float* s_distk = reinterpret_cast<float*>(misc + 2);
     float* cs = reinterpret_cast<float*>(misc + 16);  // 32 floats of merge scratch
-    const int code_len = D * EX / 8;
     const int fac_rescale = 1 << EX;
     const float one_over_sqrtD = recip_via_double(__fsqrt_rn((float)D));
     const float* qv = a.qrot + (size_t)q * D;
@@ -349,23 +360,42 @@ __global__ void __launch_bounds__(kRefineThreads) refine_kernel(RefineArgs a) {
                 uq_ready = true;
                 __syncthreads();
             }
-            // refine the listed candidates, one per thread (idle threads repeat
-            // the first so each warp stays converged on the broadcast reads)
-            for (int r = 0; r < cnt; r += blockDim.x) {
-                const int i = r + tid;
-                const int slot = w_list[i < cnt ? i : 0];
-                const size_t pos = (size_t)first_vec + 32 * wb + slot;
-                const float ip = ex_ip_thread<EX>(uq, a.excode + pos * code_len, D);
-                if (i < cnt) {
-                    // inc/index/HASearcher.hpp:225-232
-                    const float on = w_on[slot];
-                    const float sqr_x = __fmul_rn(on, on);
-                    const float t = __fadd_rn(__fmul_rn((float)fac_rescale, w_ipq[slot]), ip);
-                    const double br = __dsub_rn((double)t, ex_sub);
-                    const float xy = __fmul_rn(a.xipnorm[pos], y);
-                    const float f = __fadd_rn(sqr_x, sqy);
-                    w_ed[slot] = __double2float_rn(__dsub_rn((double)f, __dmul_rn((double)xy, br)));
-                    w_id[slot] = a.ids[pos];
+            // refine the listed candidates: quad g (lanes 4g..4g+3) takes two
+            // per round while at least 33 remain, else one; quads past the
+            // end repeat the list's first so every warp stays converged
+            {
+                const int g = tid >> 2, r = tid & 3;
+                const float4* uq4 = reinterpret_cast<const float4*>(uq);
+                for (int base = 0; base < cnt;) {
+                    const int two = cnt - base > kRefineThreads / 4;
+                    const int i0 = base + g, i1 = base + kRefineThreads / 4 + g;
+                    const int s0 = w_list[i0 < cnt ? i0 : 0];
+                    const int s1 = w_list[two && i1 < cnt ? i1 : 0];
+                    const size_t pos0 = (size_t)first_vec + 32 * wb + s0;
+                    const size_t pos1 = (size_t)first_vec + 32 * wb + s1;
+                    const uint4* row0 = reinterpret_cast<const uint4*>(a.excode + pos0 * a.ex_row);
+                    const uint4* row1 = reinterpret_cast<const uint4*>(a.excode + pos1 * a.ex_row);
+                    float ip[2];
+                    if (two)
+                        ex_ip_quad<ex_storage_bits(EX), 2>(uq4, row0, row1, r, D / 16, ip);
+                    else
+                        ex_ip_quad<ex_storage_bits(EX), 1>(uq4, row0, row0, r, D / 16, ip);
+                    // lane 0 of the quad finishes the first, lane 1 the second
+                    const int i = r == 0 ? i0 : i1;
+                    if (r < 2 && (r == 0 || two) && i < cnt) {
+                        const int slot = r == 0 ? s0 : s1;
+                        const size_t pos = r == 0 ? pos0 : pos1;
+                        // inc/index/HASearcher.hpp:225-232
+                        const float on = w_on[slot];
+                        const float sqr_x = __fmul_rn(on, on);
+                        const float t = __fadd_rn(__fmul_rn((float)fac_rescale, w_ipq[slot]), r == 0 ? ip[0] : ip[1]);
+                        const double br = __dsub_rn((double)t, ex_sub);
+                        const float xy = __fmul_rn(a.xipnorm[pos], y);
+                        const float f = __fadd_rn(sqr_x, sqy);
+                        w_ed[slot] = __double2float_rn(__dsub_rn((double)f, __dmul_rn((double)xy, br)));
+                        w_id[slot] = a.ids[pos];
+                    }
+                    base += two ? kRefineThreads / 2 : kRefineThreads / 4;
                 }
             }
             __syncthreads();
