@@ -31,6 +31,7 @@
 #include "probe.cuh"
 #include "layout.cuh"
 #include "refine.cuh"
+#include "order.cuh"
 #include "scan.cuh"
 
 using namespace erq;
@@ -126,10 +127,13 @@ enum KernelId {
     kSplit,
     kGemm,
     kProbe,
+    kOrder,
+    kMlp,
     kNumKernels
 };
 const char* const kKernelNames[kNumKernels] = {"rotate", "centroid_dist", "select_probe", "scan",
-                                               "refine", "split",  "gemm",          "probe"};
+                                               "refine", "split",  "gemm",          "probe",
+                                               "order", "mlp"};
 
 struct Profiler {
     std::mutex mu;
@@ -468,6 +472,11 @@ struct Batch {
     float* sumq = nullptr;
     __nv_bfloat16* qsplit = nullptr;  // [nq][3D] split rotated queries
     float* qn = nullptr;              // [nq]
+    // work order (order.cuh)
+    uint32_t* keys = nullptr;         // [nq * nprobe]
+    uint32_t* buckets = nullptr;      // [K + 1]
+    uint32_t* order_pairs = nullptr;  // [nq * nprobe]
+    uint32_t* order_q = nullptr;      // [nq]
 };
 
 // Largest query batch whose scan workspace fits the budget.
@@ -490,7 +499,61 @@ erq_status alloc_batch(Scratch& s, const erq_index* idx, uint64_t nq, uint64_t n
     ERQ_TRY(s.alloc(&b.sumq, nq * nprobe));
     ERQ_TRY(s.alloc(&b.qsplit, nq * 3 * idx->D));
     ERQ_TRY(s.alloc(&b.qn, nq));
+    ERQ_TRY(s.alloc(&b.keys, nq * nprobe));
+    ERQ_TRY(s.alloc(&b.buckets, idx->K + 1));
+    ERQ_TRY(s.alloc(&b.order_pairs, nq * nprobe));
+    ERQ_TRY(s.alloc(&b.order_q, nq));
     return ERQ_OK;
+}
+
+// Orders of the scan's (query, probe) pairs and the refinement's queries by
+// cluster (order.cuh).  Small batches gain nothing from reuse and keep the
+// identity order (returns false).
+bool launch_order(const erq_index* idx, const Batch& b, uint64_t nprobe, cudaStream_t st,
+                  const int* q_nprobe, erq_status* err) {
+    *err = ERQ_OK;
+    const uint64_t pairs = b.nq * nprobe;
+    if (pairs < 1024 || !b.order_pairs) return false;
+    const uint32_t nb = (uint32_t)idx->K + 1;
+    const unsigned gp = (unsigned)div_up(pairs, 256), gq = (unsigned)div_up(b.nq, 256);
+    auto sort = [&](uint32_t n, uint32_t* order) -> erq_status {
+        ERQ_CUDA(cudaMemsetAsync(b.buckets, 0, nb * sizeof(uint32_t), st));
+        {
+            LaunchTimer t(kOrder, st);
+            bucket_count_kernel<<<(unsigned)div_up(n, 256), 256, 0, st>>>(b.keys, n, b.buckets);
+            t.finish();
+        }
+        {
+            LaunchTimer t(kOrder, st);
+            bucket_scan_kernel<<<1, kBucketScanThreads, 0, st>>>(b.buckets, nb);
+            t.finish();
+        }
+        {
+            LaunchTimer t(kOrder, st);
+            bucket_scatter_kernel<<<(unsigned)div_up(n, 256), 256, 0, st>>>(b.keys, n, b.buckets, order);
+            t.finish();
+        }
+        return ERQ_OK;
+    };
+    {
+        LaunchTimer t(kOrder, st);
+        pair_keys_kernel<<<gp, 256, 0, st>>>(b.probe_cid, (uint32_t)pairs, (int)nprobe, q_nprobe,
+                                             (uint32_t)idx->K, b.keys);
+        t.finish();
+    }
+    if ((*err = sort((uint32_t)pairs, b.order_pairs)) != ERQ_OK) return false;
+    {
+        LaunchTimer t(kOrder, st);
+        query_keys_kernel<<<gq, 256, 0, st>>>(b.probe_cid, (uint32_t)b.nq, (int)nprobe, b.keys);
+        t.finish();
+    }
+    if ((*err = sort((uint32_t)b.nq, b.order_q)) != ERQ_OK) return false;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        *err = fail(ERQ_ERR_CUDA, "order kernels: %s", cudaGetErrorString(e));
+        return false;
+    }
+    return true;
 }
 
 // Candidate count for the probe: nprobe plus a margin (probe.cuh).
@@ -571,8 +634,9 @@ erq_status launch_probe(const erq_index* idx, const Batch& b, uint64_t nprobe, c
 }
 
 erq_status launch_scan(const erq_index* idx, const Batch& b, uint64_t nprobe, cudaStream_t st,
-                       const int* q_nprobe = nullptr) {
+                       const int* q_nprobe = nullptr, const uint32_t* order = nullptr) {
     ScanArgs a;
+    a.order = order;
     a.qrot = b.qrot;
     a.centroids = idx->centroids;
     a.probe_cid = b.probe_cid;
@@ -598,8 +662,9 @@ erq_status launch_scan(const erq_index* idx, const Batch& b, uint64_t nprobe, cu
 
 erq_status launch_refine(const erq_index* idx, const Batch& b, uint64_t nprobe, uint64_t k,
                          uint32_t* out_ids, float* out_dists, cudaStream_t st,
-                         const int* q_nprobe = nullptr) {
+                         const int* q_nprobe = nullptr, const uint32_t* order = nullptr) {
     RefineArgs a;
+    a.order = order;
     a.qrot = b.qrot;
     a.centroids = idx->centroids;
     a.probe_cid = b.probe_cid;
@@ -667,9 +732,13 @@ erq_status search_device(const erq_index* idx, const float* qrot_dev, uint64_t n
         b.nq = std::min(bq, nq - q0);
         b.qrot = qrot_dev + q0 * idx->D;
         ERQ_TRY(launch_probe_tc(idx, b, nprobe, st));
-        ERQ_TRY(launch_scan(idx, b, nprobe, st));
+        erq_status oe;
+        const bool ordered = launch_order(idx, b, nprobe, st, nullptr, &oe);
+        ERQ_TRY(oe);
+        ERQ_TRY(launch_scan(idx, b, nprobe, st, nullptr, ordered ? b.order_pairs : nullptr));
         ERQ_TRY(launch_refine(idx, b, nprobe, k, ids_dev + q0 * k,
-                              dists_dev ? dists_dev + q0 * k : nullptr, st));
+                              dists_dev ? dists_dev + q0 * k : nullptr, st, nullptr,
+                              ordered ? b.order_q : nullptr));
     }
     return ERQ_OK;
 }
@@ -773,8 +842,10 @@ template <typename TB>
 erq_status mlp_mm(const float* A, long sam, long sak, const TB* B, long sbk, long sbn, float* C,
                   int M, int N, int K, const float* bias, bool relu, cudaStream_t st) {
     dim3 grid((unsigned)div_up(N, 16), (unsigned)div_up(M, 16));
+    LaunchTimer t(kMlp, st);
     mlp_matmul_kernel<TB><<<grid, 256, 0, st>>>(A, sam, sak, B, sbk, sbn, C, M, N, K, bias, relu,
                                                 false);
+    t.finish();
     ERQ_CUDA(cudaGetLastError());
     return ERQ_OK;
 }
@@ -881,8 +952,10 @@ erq_status model_upload(erq_probe_model* m, const std::vector<float>& w,
 erq_status features_device(const erq_index* idx, const Batch& b, uint64_t nprobe, float* near_d,
                            float* feats, cudaStream_t st) {
     ERQ_TRY(launch_probe_tc(idx, b, nprobe, st, near_d));
+    LaunchTimer t(kMlp, st);
     probe_features_kernel<<<(unsigned)b.nq, 128, 0, st>>>(b.qrot, (int)idx->D, near_d,
                                                          (int)b.nq, feats);
+    t.finish();
     ERQ_CUDA(cudaGetLastError());
     return ERQ_OK;
 }
@@ -1487,18 +1560,34 @@ static erq_status search_learned_entry(const erq_index* idx, const erq_probe_mod
         b.qrot = q + q0 * idx->D;
         const int B = (int)b.nq;
         ERQ_TRY(features_device(idx, b, nprobe_max, near_d, feats, st));
-        mlp_standardise_kernel<<<(unsigned)div_up((uint64_t)B * kMlpIn, 256), 256, 0, st>>>(
-            feats, m->mean, m->stdv, wk.x, B * kMlpIn);
+        {
+            LaunchTimer t(kMlp, st);
+            mlp_standardise_kernel<<<(unsigned)div_up((uint64_t)B * kMlpIn, 256), 256, 0, st>>>(
+                feats, m->mean, m->stdv, wk.x, B * kMlpIn);
+            t.finish();
+        }
         ERQ_TRY(mlp_forward(m, wk, B, st));
-        mlp_softmax_xent_kernel<<<(unsigned)div_up(B, 128), 128, 0, st>>>(wk.z, nullptr, B,
-                                                                         wk.probs, nullptr, nullptr);
-        mlp_choose_nprobe_kernel<<<(unsigned)div_up(B, 128), 128, 0, st>>>(
-            wk.probs, B, m->bins_dev, confidence, min_prob, (int)nprobe_fallback, (int)nprobe_max,
-            used + q0);
+        {
+            LaunchTimer t(kMlp, st);
+            mlp_softmax_xent_kernel<<<(unsigned)div_up(B, 128), 128, 0, st>>>(wk.z, nullptr, B,
+                                                                             wk.probs, nullptr, nullptr);
+            t.finish();
+        }
+        {
+            LaunchTimer t(kMlp, st);
+            mlp_choose_nprobe_kernel<<<(unsigned)div_up(B, 128), 128, 0, st>>>(
+                wk.probs, B, m->bins_dev, confidence, min_prob, (int)nprobe_fallback, (int)nprobe_max,
+                used + q0);
+            t.finish();
+        }
         ERQ_CUDA(cudaGetLastError());
-        ERQ_TRY(launch_scan(idx, b, nprobe_max, st, used + q0));
+        erq_status oe;
+        const bool ordered = launch_order(idx, b, nprobe_max, st, used + q0, &oe);
+        ERQ_TRY(oe);
+        ERQ_TRY(launch_scan(idx, b, nprobe_max, st, used + q0, ordered ? b.order_pairs : nullptr));
         ERQ_TRY(launch_refine(idx, b, nprobe_max, k, ids_out + q0 * k,
-                              d_out ? d_out + q0 * k : nullptr, st, used + q0));
+                              d_out ? d_out + q0 * k : nullptr, st, used + q0,
+                              ordered ? b.order_q : nullptr));
     }
     if (nprobe_used)
         ERQ_CUDA(cudaMemcpyAsync(nprobe_used, used, nq * 4, cudaMemcpyDefault, st));

@@ -43,6 +43,7 @@ struct RefineArgs {
     uint32_t* out_ids;            // [nq][k]
     float* out_dists;             // [nq][k] or null
     const int* q_nprobe;          // optional [nq]: clusters probed by each query
+    const uint32_t* order;        // optional: block i refines query order[i]
     int nq, D, EX, nprobe, k;
 };
 
@@ -174,37 +175,58 @@ __device__ __forceinline__ uint64_t merge_key(float d, int lane, bool cand) {
 // sort the candidates by (distance, later lane first); pool entry i moves to
 // i + #(candidates <= it), candidate j goes to j + #(pool entries < it), and
 // ranks >= k fall off.  Executed by one whole warp; `cs` is 32 floats of
-// scratch.
+// scratch.  The caller may drop candidates that cannot enter a full pool
+// (distance > its k-th): they would rank >= k and move no other entry.
 __device__ __forceinline__ void pool_merge_block(float* pool_d, uint32_t* pool_id, int& size, int k,
                                                  float& distk, bool cand, float d, uint32_t id,
                                                  float* cs, int lane) {
-    const int nc = __popc(__ballot_sync(0xffffffffu, cand));
-    uint64_t key = merge_key(d, lane, cand);
-    uint32_t val = id;
+    const uint32_t cm = __ballot_sync(0xffffffffu, cand);
+    const int nc = __popc(cm);
     float dv = d;
+    uint32_t val = id;
+    if (nc == 1) {
+        const int src = __ffs(cm) - 1;
+        dv = __shfl_sync(0xffffffffu, d, src);
+        val = __shfl_sync(0xffffffffu, id, src);
+    } else {
+        uint64_t key = merge_key(d, lane, cand);
 #pragma unroll
-    for (int sz = 2; sz <= 32; sz <<= 1) {
+        for (int sz = 2; sz <= 32; sz <<= 1) {
 #pragma unroll
-        for (int st = sz >> 1; st > 0; st >>= 1) {
-            const uint64_t ok = __shfl_xor_sync(0xffffffffu, key, st);
-            const uint32_t ov = __shfl_xor_sync(0xffffffffu, val, st);
-            const float od = __shfl_xor_sync(0xffffffffu, dv, st);
-            const bool take_min = ((lane & st) == 0) == ((lane & sz) == 0);
-            if (take_min ? (ok < key) : (ok > key)) {
-                key = ok;
-                val = ov;
-                dv = od;
+            for (int st = sz >> 1; st > 0; st >>= 1) {
+                const uint64_t ok = __shfl_xor_sync(0xffffffffu, key, st);
+                const uint32_t ov = __shfl_xor_sync(0xffffffffu, val, st);
+                const float od = __shfl_xor_sync(0xffffffffu, dv, st);
+                const bool take_min = ((lane & st) == 0) == ((lane & sz) == 0);
+                if (take_min ? (ok < key) : (ok > key)) {
+                    key = ok;
+                    val = ov;
+                    dv = od;
+                }
             }
         }
     }
-    // lane j holds the j-th candidate
-    cs[lane] = dv;
+    // lane j (< nc) holds the j-th candidate
+    constexpr int kFew = 8;  // up to this many: counts by broadcast, else binary search
     int lo = 0;
-    if (lane < nc) {
-        int hi = size;
-        while (lo < hi) {
-            const int mid = (lo + hi) >> 1;
-            if (pool_d[mid] < dv) lo = mid + 1; else hi = mid;
+    if (nc <= kFew) {
+        for (int i0 = 0; i0 < size; i0 += 32) {
+            const int i = i0 + lane;
+            const float pdv = i < size ? pool_d[i] : 0.f;
+            for (int j = 0; j < nc; ++j) {
+                const float dj = __shfl_sync(0xffffffffu, dv, j);
+                const int c = __popc(__ballot_sync(0xffffffffu, i < size && pdv < dj));
+                if (lane == j) lo += c;
+            }
+        }
+    } else {
+        cs[lane] = dv;
+        if (lane < nc) {
+            int hi = size;
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (pool_d[mid] < dv) lo = mid + 1; else hi = mid;
+            }
         }
     }
     const int rc = lane < nc ? lane + lo : k;
@@ -217,17 +239,21 @@ __device__ __forceinline__ void pool_merge_block(float* pool_d, uint32_t* pool_i
         const int i = i0 + lane;
         float pd = 0.f;
         uint32_t pid = 0u;
-        int pr = k;
         if (i < size) {
             pd = pool_d[i];
             pid = pool_id[i];
-            int l2 = 0, h2 = nc;
-            while (l2 < h2) {
-                const int mid = (l2 + h2) >> 1;
-                if (cs[mid] <= pd) l2 = mid + 1; else h2 = mid;
-            }
-            pr = i + l2;
         }
+        int c = 0;
+        if (nc <= kFew) {
+            for (int j = 0; j < nc; ++j) c += __shfl_sync(0xffffffffu, dv, j) <= pd;
+        } else if (i < size) {
+            int h2 = nc;
+            while (c < h2) {
+                const int mid = (c + h2) >> 1;
+                if (cs[mid] <= pd) c = mid + 1; else h2 = mid;
+            }
+        }
+        const int pr = i < size ? i + c : k;
         __syncwarp();
         if (pr < k) {
             pool_d[pr] = pd;
@@ -255,7 +281,7 @@ template <int EX>
 __global__ void __launch_bounds__(kRefineThreads) refine_kernel(RefineArgs a) {
     extern __shared__ __align__(16) uint8_t smem_raw[];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int q = blockIdx.x;
+    const int q = a.order ? (int)a.order[blockIdx.x] : (int)blockIdx.x;
     const int D = a.D, k = a.k;
     const int kpad = (k + 31) & ~31;
     float* uq = reinterpret_cast<float*>(smem_raw);
@@ -338,8 +364,15 @@ __global__ void __launch_bounds__(kRefineThreads) refine_kernel(RefineArgs a) {
                     int base = 0;
                     if (lane == 0 && m) base = atomicAdd(&misc[0], __popc(m));
                     base = __shfl_sync(0xffffffffu, base, 0);
-                    if ((m >> lane) & 1u)
+                    if ((m >> lane) & 1u) {
                         w_list[base + __popc(m & ((1u << lane) - 1u))] = (uint16_t)(32 * b + lane);
+                        // start the candidate's EX-code row on its way to L2
+                        const size_t pos = (size_t)first_vec + 32 * blk + lane;
+                        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(
+                                         a.excode + pos * a.ex_row),
+                                     "r"((uint32_t)a.ex_row)
+                                     : "memory");
+                    }
                 }
             }
             __syncthreads();
@@ -375,25 +408,32 @@ __global__ void __launch_bounds__(kRefineThreads) refine_kernel(RefineArgs a) {
                     const size_t pos1 = (size_t)first_vec + 32 * wb + s1;
                     const uint4* row0 = reinterpret_cast<const uint4*>(a.excode + pos0 * a.ex_row);
                     const uint4* row1 = reinterpret_cast<const uint4*>(a.excode + pos1 * a.ex_row);
+                    // lane 0 of the quad finishes the first, lane 1 the second
+                    const int i = r == 0 ? i0 : i1;
+                    const bool fin = r < 2 && (r == 0 || two) && i < cnt;
+                    const int slot = r == 0 ? s0 : s1;
+                    const size_t pos = r == 0 ? pos0 : pos1;
+                    float xipn = 0.f;
+                    uint32_t vid = 0u;
+                    if (fin) {
+                        xipn = __ldg(a.xipnorm + pos);
+                        vid = __ldg(a.ids + pos);
+                    }
                     float ip[2];
                     if (two)
                         ex_ip_quad<ex_storage_bits(EX), 2>(uq4, row0, row1, r, D / 16, ip);
                     else
                         ex_ip_quad<ex_storage_bits(EX), 1>(uq4, row0, row0, r, D / 16, ip);
-                    // lane 0 of the quad finishes the first, lane 1 the second
-                    const int i = r == 0 ? i0 : i1;
-                    if (r < 2 && (r == 0 || two) && i < cnt) {
-                        const int slot = r == 0 ? s0 : s1;
-                        const size_t pos = r == 0 ? pos0 : pos1;
+                    if (fin) {
                         // inc/index/HASearcher.hpp:225-232
                         const float on = w_on[slot];
                         const float sqr_x = __fmul_rn(on, on);
                         const float t = __fadd_rn(__fmul_rn((float)fac_rescale, w_ipq[slot]), r == 0 ? ip[0] : ip[1]);
                         const double br = __dsub_rn((double)t, ex_sub);
-                        const float xy = __fmul_rn(a.xipnorm[pos], y);
+                        const float xy = __fmul_rn(xipn, y);
                         const float f = __fadd_rn(sqr_x, sqy);
                         w_ed[slot] = __double2float_rn(__dsub_rn((double)f, __dmul_rn((double)xy, br)));
-                        w_id[slot] = a.ids[pos];
+                        w_id[slot] = vid;
                     }
                     base += two ? kRefineThreads / 2 : kRefineThreads / 4;
                 }
@@ -401,9 +441,12 @@ __global__ void __launch_bounds__(kRefineThreads) refine_kernel(RefineArgs a) {
             __syncthreads();
             if (warp == 0) {
                 for (int b = 0; b < nbw; ++b) {
-                    const bool cand = w_lb[32 * b + lane] < distk;
-                    if (__ballot_sync(0xffffffffu, cand))
-                        pool_merge_block(pool_d, pool_id, size, k, distk, cand, w_ed[32 * b + lane],
+                    // candidates of the block against the threshold at its
+                    // start; those above a full pool's k-th cannot enter
+                    const float ed = w_ed[32 * b + lane];
+                    const bool enter = w_lb[32 * b + lane] < distk && (size < k || !(ed > distk));
+                    if (__ballot_sync(0xffffffffu, enter))
+                        pool_merge_block(pool_d, pool_id, size, k, distk, enter, ed,
                                          w_id[32 * b + lane], cs, lane);
                 }
                 if (lane == 0) {

@@ -41,6 +41,7 @@ struct ScanArgs {
     float* qp_delta;          // [nq][nprobe]
     float* qp_sumq;           // [nq][nprobe]
     const int* q_nprobe;      // optional [nq]: probe only the first q_nprobe[q] clusters
+    const uint32_t* order;    // optional: block i scans pair order[i]
     int D;
     int nprobe;
 };
@@ -92,7 +93,7 @@ __global__ void __launch_bounds__(kScanWarps * 32) scan_kernel(ScanArgs a) {
     float* unit_q = reinterpret_cast<float*>(tables + nchunk * 512);
     float* red = unit_q + D;
 
-    const uint32_t pair = blockIdx.x;
+    const uint32_t pair = a.order ? a.order[blockIdx.x] : blockIdx.x;
     const uint32_t q = pair / (uint32_t)a.nprobe;
     if (a.q_nprobe && (int)(pair - q * (uint32_t)a.nprobe) >= a.q_nprobe[q]) return;
     const uint32_t cid = a.probe_cid[pair];

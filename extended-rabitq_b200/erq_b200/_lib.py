@@ -135,7 +135,7 @@ def check(status: int) -> None:
 
 
 KERNELS = ("rotate", "centroid_dist", "select_probe", "scan", "refine", "split", "gemm",
-           "probe")
+           "probe", "order", "mlp")
 
 
 def profile_enable(on: bool = True) -> None:

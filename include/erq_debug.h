@@ -57,7 +57,7 @@ ERQ_API erq_status erq_debug_probe_model_params(const erq_probe_model* model, fl
  * rotation entry points is bracketed by CUDA events recorded on the stream
  * the kernel runs on.  erq_profile_read waits for the recorded events and
  * returns, for one kernel ("rotate", "centroid_dist", "select_probe", "scan",
- * "refine", "split", "gemm", "probe"), the number of launches and their summed device time since the
+ * "refine", "split", "gemm", "probe", "order", "mlp"), the number of launches and their summed device time since the
  * last reset.  Process-wide; meant for benchmarks. */
 ERQ_API void erq_profile_enable(int on);
 ERQ_API void erq_profile_reset(void);
