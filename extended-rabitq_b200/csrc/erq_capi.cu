@@ -18,6 +18,7 @@
 #include <numeric>
 #include <random>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -33,6 +34,7 @@
 #include "refine.cuh"
 #include "order.cuh"
 #include "scan.cuh"
+#include "scan_batch.cuh"
 
 using namespace erq;
 
@@ -165,6 +167,12 @@ struct LaunchTimer {
             active = p.on;
         }
         if (!active) return;
+        // launches recorded into a CUDA graph are not timed one by one
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        if (cudaStreamIsCapturing(stream, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+            active = false;
+            return;
+        }
         if (cudaEventCreate(&start) != cudaSuccess || cudaEventCreate(&stop) != cudaSuccess) {
             active = false;
             return;
@@ -474,7 +482,8 @@ struct Batch {
     float* qn = nullptr;              // [nq]
     // work order (order.cuh)
     uint32_t* keys = nullptr;         // [nq * nprobe]
-    uint32_t* buckets = nullptr;      // [K + 1]
+    uint32_t* buckets = nullptr;      // [K + 1] pair sort; ends of each cluster's run after it
+    uint32_t* buckets_q = nullptr;    // [K + 1] query sort
     uint32_t* order_pairs = nullptr;  // [nq * nprobe]
     uint32_t* order_q = nullptr;      // [nq]
 };
@@ -488,7 +497,8 @@ uint64_t batch_queries(const erq_index* idx, uint64_t nprobe, uint64_t nq) {
     return std::min(b, nq);
 }
 
-erq_status alloc_batch(Scratch& s, const erq_index* idx, uint64_t nq, uint64_t nprobe, Batch& b) {
+template <class Alloc>
+erq_status alloc_batch(Alloc& s, const erq_index* idx, uint64_t nq, uint64_t nprobe, Batch& b) {
     b.nq = nq;
     ERQ_TRY(s.alloc(&b.dist, nq * idx->K));
     ERQ_TRY(s.alloc(&b.probe_cid, nq * nprobe));
@@ -501,58 +511,73 @@ erq_status alloc_batch(Scratch& s, const erq_index* idx, uint64_t nq, uint64_t n
     ERQ_TRY(s.alloc(&b.qn, nq));
     ERQ_TRY(s.alloc(&b.keys, nq * nprobe));
     ERQ_TRY(s.alloc(&b.buckets, idx->K + 1));
+    ERQ_TRY(s.alloc(&b.buckets_q, idx->K + 1));
     ERQ_TRY(s.alloc(&b.order_pairs, nq * nprobe));
     ERQ_TRY(s.alloc(&b.order_q, nq));
     return ERQ_OK;
 }
 
-// Orders of the scan's (query, probe) pairs and the refinement's queries by
-// cluster (order.cuh).  Small batches gain nothing from reuse and keep the
-// identity order (returns false).
+// Counting sort of keys[0, n) over K + 1 buckets into order; afterwards
+// buckets[c] is the end of bucket c's run (order.cuh).
+erq_status bucket_sort(const erq_index* idx, const uint32_t* keys, uint32_t n, uint32_t* buckets,
+                       uint32_t* order, cudaStream_t st) {
+    const uint32_t nb = (uint32_t)idx->K + 1;
+    ERQ_CUDA(cudaMemsetAsync(buckets, 0, nb * sizeof(uint32_t), st));
+    if (n == 0) return ERQ_OK;
+    {
+        LaunchTimer t(kOrder, st);
+        bucket_count_kernel<<<(unsigned)div_up(n, 256), 256, 0, st>>>(keys, n, buckets);
+        t.finish();
+    }
+    {
+        LaunchTimer t(kOrder, st);
+        bucket_scan_kernel<<<1, kBucketScanThreads, 0, st>>>(buckets, nb);
+        t.finish();
+    }
+    {
+        LaunchTimer t(kOrder, st);
+        bucket_scatter_kernel<<<(unsigned)div_up(n, 256), 256, 0, st>>>(keys, n, buckets, order);
+        t.finish();
+    }
+    ERQ_CUDA(cudaGetLastError());
+    return ERQ_OK;
+}
+
+// (query, probe) pairs by cluster into b.order_pairs (pairs a per-query probe
+// count leaves out go last), runs delimited by b.buckets.
+erq_status order_pairs(const erq_index* idx, const Batch& b, uint64_t nprobe, cudaStream_t st,
+                       const int* q_nprobe) {
+    const uint64_t pairs = b.nq * nprobe;
+    if (pairs == 0) return ERQ_OK;
+    {
+        LaunchTimer t(kOrder, st);
+        pair_keys_kernel<<<(unsigned)div_up(pairs, 256), 256, 0, st>>>(
+            b.probe_cid, (uint32_t)pairs, (int)nprobe, q_nprobe, (uint32_t)idx->K, b.keys);
+        t.finish();
+    }
+    return bucket_sort(idx, b.keys, (uint32_t)pairs, b.buckets, b.order_pairs, st);
+}
+
+// queries by their nearest cluster into b.order_q.
+erq_status order_queries(const erq_index* idx, const Batch& b, uint64_t nprobe, cudaStream_t st) {
+    if (b.nq == 0) return ERQ_OK;
+    {
+        LaunchTimer t(kOrder, st);
+        query_keys_kernel<<<(unsigned)div_up(b.nq, 256), 256, 0, st>>>(b.probe_cid, (uint32_t)b.nq,
+                                                                      (int)nprobe, b.keys);
+        t.finish();
+    }
+    return bucket_sort(idx, b.keys, (uint32_t)b.nq, b.buckets_q, b.order_q, st);
+}
+
+// Both orders for the per-pair scan and the refinement.  Small batches gain
+// nothing from reuse and keep the identity order (returns false).
 bool launch_order(const erq_index* idx, const Batch& b, uint64_t nprobe, cudaStream_t st,
                   const int* q_nprobe, erq_status* err) {
     *err = ERQ_OK;
-    const uint64_t pairs = b.nq * nprobe;
-    if (pairs < 1024 || !b.order_pairs) return false;
-    const uint32_t nb = (uint32_t)idx->K + 1;
-    const unsigned gp = (unsigned)div_up(pairs, 256), gq = (unsigned)div_up(b.nq, 256);
-    auto sort = [&](uint32_t n, uint32_t* order) -> erq_status {
-        ERQ_CUDA(cudaMemsetAsync(b.buckets, 0, nb * sizeof(uint32_t), st));
-        {
-            LaunchTimer t(kOrder, st);
-            bucket_count_kernel<<<(unsigned)div_up(n, 256), 256, 0, st>>>(b.keys, n, b.buckets);
-            t.finish();
-        }
-        {
-            LaunchTimer t(kOrder, st);
-            bucket_scan_kernel<<<1, kBucketScanThreads, 0, st>>>(b.buckets, nb);
-            t.finish();
-        }
-        {
-            LaunchTimer t(kOrder, st);
-            bucket_scatter_kernel<<<(unsigned)div_up(n, 256), 256, 0, st>>>(b.keys, n, b.buckets, order);
-            t.finish();
-        }
-        return ERQ_OK;
-    };
-    {
-        LaunchTimer t(kOrder, st);
-        pair_keys_kernel<<<gp, 256, 0, st>>>(b.probe_cid, (uint32_t)pairs, (int)nprobe, q_nprobe,
-                                             (uint32_t)idx->K, b.keys);
-        t.finish();
-    }
-    if ((*err = sort((uint32_t)pairs, b.order_pairs)) != ERQ_OK) return false;
-    {
-        LaunchTimer t(kOrder, st);
-        query_keys_kernel<<<gq, 256, 0, st>>>(b.probe_cid, (uint32_t)b.nq, (int)nprobe, b.keys);
-        t.finish();
-    }
-    if ((*err = sort((uint32_t)b.nq, b.order_q)) != ERQ_OK) return false;
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) {
-        *err = fail(ERQ_ERR_CUDA, "order kernels: %s", cudaGetErrorString(e));
-        return false;
-    }
+    if (b.nq * nprobe < 1024 || !b.order_pairs) return false;
+    if ((*err = order_pairs(idx, b, nprobe, st, q_nprobe)) != ERQ_OK) return false;
+    if ((*err = order_queries(idx, b, nprobe, st)) != ERQ_OK) return false;
     return true;
 }
 
@@ -744,13 +769,10 @@ erq_status search_device(const erq_index* idx, const float* qrot_dev, uint64_t n
 }
 
 // out[nq][D] = pad(q[nq][DIM]) * P on tensor cores (split-BF16, FP32 accumulation).
-erq_status rotate_device(const erq_index* idx, const float* q_dev, uint64_t nq, float* out_dev,
-                         cudaStream_t st) {
+erq_status rotate_into(const erq_index* idx, const float* q_dev, uint64_t nq, float* out_dev,
+                       __nv_bfloat16* qs, cudaStream_t st) {
     if (nq == 0) return ERQ_OK;
     const int D = (int)idx->D;
-    Scratch s(st, idx->pool);
-    __nv_bfloat16* qs = nullptr;
-    ERQ_TRY(s.alloc(&qs, nq * 3 * (uint64_t)D));
     {
         LaunchTimer t(kSplit, st);
         split_rows_kernel<<<(unsigned)nq, 256, 0, st>>>(q_dev, (int)nq, (int)idx->DIM, D, true, qs,
@@ -765,6 +787,15 @@ erq_status rotate_device(const erq_index* idx, const float* q_dev, uint64_t nq, 
     t.finish();
     ERQ_CUDA(cudaGetLastError());
     return ERQ_OK;
+}
+
+erq_status rotate_device(const erq_index* idx, const float* q_dev, uint64_t nq, float* out_dev,
+                         cudaStream_t st) {
+    if (nq == 0) return ERQ_OK;
+    Scratch s(st, idx->pool);
+    __nv_bfloat16* qs = nullptr;
+    ERQ_TRY(s.alloc(&qs, nq * 3 * idx->D));
+    return rotate_into(idx, q_dev, nq, out_dev, qs, st);
 }
 
 // Shared body of erq_search / erq_search_raw.
@@ -863,7 +894,8 @@ struct MlpWork {
     float* loss = nullptr;  // [B]
 };
 
-erq_status mlp_alloc(Scratch& s, int B, bool train, MlpWork& w) {
+template <class Alloc>
+erq_status mlp_alloc(Alloc& s, int B, bool train, MlpWork& w) {
     ERQ_TRY(s.alloc(&w.x, (size_t)B * kMlpIn));
     ERQ_TRY(s.alloc(&w.h1, (size_t)B * kMlpHidden));
     ERQ_TRY(s.alloc(&w.h2, (size_t)B * kMlpHidden));
@@ -1725,5 +1757,440 @@ erq_status erq_profile_read(const char* kernel, uint64_t* launches, double* tota
     *total_ms = p.ms[id];
     return ERQ_OK;
 }
+
+}  // extern "C"
+
+// ------------------------------------------------------------ batched plans
+//
+// A plan holds every buffer a search of up to max_batch queries needs, so a
+// search allocates nothing; the whole pipeline of one batch size is captured
+// once into a CUDA graph and replayed.  The scan runs over the
+// (query block x cluster chunk) work list of scan_batch.cuh with tiles the
+// autotuner picks.
+namespace {
+
+struct Arena {
+    std::vector<void*> ptrs;
+    uint64_t bytes = 0;
+    template <typename T>
+    erq_status alloc(T** out, size_t count) {
+        void* p = nullptr;
+        const size_t b = std::max<size_t>(count * sizeof(T), 16);
+        cudaError_t e = cudaMalloc(&p, b);
+        if (e != cudaSuccess)
+            return fail(e == cudaErrorMemoryAllocation ? ERQ_ERR_OUT_OF_MEMORY : ERQ_ERR_CUDA,
+                        "cudaMalloc(%zu bytes) for a plan failed: %s", b, cudaGetErrorString(e));
+        ptrs.push_back(p);
+        bytes += b;
+        *out = static_cast<T*>(p);
+        return ERQ_OK;
+    }
+    ~Arena() {
+        for (void* p : ptrs) cudaFree(p);
+    }
+};
+
+// Scan tile shapes the autotuner chooses among: (queries per item, warps).
+struct ScanShape {
+    int qb, warps;
+};
+constexpr ScanShape kScanShapes[] = {{1, 4}, {2, 4}, {4, 4}, {2, 8}, {4, 8}, {8, 8}};
+constexpr int kChunkChoices[] = {8, 16, 32, 64};
+
+template <int QB, int W>
+erq_status scan_batched_configure(int D, int* per_sm) {
+    const size_t smem = scan_batch_smem_bytes(QB, D);
+    ERQ_CUDA(cudaFuncSetAttribute(scan_batched_kernel<QB, W>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    ERQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, scan_batched_kernel<QB, W>, W * 32,
+                                                           smem));
+    *per_sm = std::max(1, *per_sm);
+    return ERQ_OK;
+}
+
+template <int QB, int W>
+erq_status scan_batched_launch(const ScanBatchArgs& a, int blocks, cudaStream_t st) {
+    LaunchTimer t(kScan, st);
+    scan_batched_kernel<QB, W><<<(unsigned)blocks, W * 32, scan_batch_smem_bytes(QB, a.D), st>>>(a);
+    t.finish();
+    ERQ_CUDA(cudaGetLastError());
+    return ERQ_OK;
+}
+
+}  // namespace
+
+struct erq_plan {
+    const erq_index* idx = nullptr;
+    const erq_probe_model* model = nullptr;
+    uint64_t max_batch = 0, k = 0, nprobe = 0, nprobe_run = 0;
+    bool raw = false;
+    float confidence = 0.9f, min_prob = 0.f;
+    int sms = 148;
+    int per_sm[6] = {};  // resident scan blocks per SM, by kScanShapes entry
+    std::map<uint64_t, erq_plan_tuning> tunings;  // by the batch size tuned for
+    Arena arena;
+    Batch b;
+    float* qin = nullptr;       // [max_batch][DIM or D] queries as given
+    float* qrot = nullptr;      // [max_batch][D]
+    uint32_t* ids = nullptr;    // [max_batch][k]
+    float* dists = nullptr;     // [max_batch][k]
+    int* used = nullptr;        // [max_batch] clusters probed per query
+    float* near_d = nullptr;    // [max_batch][64]
+    float* feats = nullptr;     // [max_batch][320]
+    MlpWork wk;
+    uint32_t* item_off = nullptr;  // [K + 1]
+    uint32_t* counter = nullptr;
+    cudaStream_t cap = nullptr;
+    std::mutex mu;
+    std::map<uint64_t, cudaGraphExec_t> graphs;
+
+    void drop_graphs() {
+        for (auto& g : graphs) cudaGraphExecDestroy(g.second);
+        graphs.clear();
+    }
+    ~erq_plan() {
+        int prev = -1;
+        cudaGetDevice(&prev);
+        if (idx) cudaSetDevice(idx->device);
+        cudaDeviceSynchronize();
+        drop_graphs();
+        if (cap) cudaStreamDestroy(cap);
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+namespace {
+
+erq_plan_tuning default_tuning(uint64_t nq) {
+    erq_plan_tuning t;
+    t.queries_per_item = nq >= 1024 ? 4 : 1;
+    t.blocks_per_item = 16;
+    t.warps = nq >= 1024 ? 8 : 4;
+    return t;
+}
+
+// Tuning for a batch of nq: the one tuned for the nearest batch size (log
+// scale), else the default.
+erq_plan_tuning plan_tuning(const erq_plan* p, uint64_t nq) {
+    if (p->tunings.empty()) return default_tuning(nq);
+    double best = 1e300;
+    erq_plan_tuning t = p->tunings.begin()->second;
+    for (auto& kv : p->tunings) {
+        const double d = std::fabs(std::log((double)kv.first) - std::log((double)std::max<uint64_t>(nq, 1)));
+        if (d < best) {
+            best = d;
+            t = kv.second;
+        }
+    }
+    return t;
+}
+
+bool tuning_valid(const erq_plan_tuning& t) {
+    bool shape = false;
+    for (auto& sh : kScanShapes) shape |= (int)t.queries_per_item == sh.qb && (int)t.warps == sh.warps;
+    return shape && t.blocks_per_item >= 1 && t.blocks_per_item <= 4096;
+}
+
+erq_status launch_scan_batched(erq_plan* p, uint64_t nq, const erq_plan_tuning& t, cudaStream_t st) {
+    const erq_index* idx = p->idx;
+    const int K = (int)idx->K;
+    {
+        LaunchTimer lt(kOrder, st);
+        scan_items_count_kernel<<<(unsigned)div_up(K, 256), 256, 0, st>>>(
+            p->b.buckets, idx->c_nblocks, K, (int)t.queries_per_item, (int)t.blocks_per_item,
+            p->item_off);
+        lt.finish();
+    }
+    {
+        LaunchTimer lt(kOrder, st);
+        bucket_scan_kernel<<<1, kBucketScanThreads, 0, st>>>(p->item_off, (uint32_t)K + 1);
+        lt.finish();
+    }
+    ERQ_CUDA(cudaMemsetAsync(p->counter, 0, sizeof(uint32_t), st));
+    ScanBatchArgs a;
+    a.qrot = p->b.qrot;
+    a.centroids = idx->centroids;
+    a.probe_cid = p->b.probe_cid;
+    a.probe_sqy = p->b.probe_sqy;
+    a.codes = idx->codes;
+    a.c_first_block = idx->c_first_block;
+    a.c_nblocks = idx->c_nblocks;
+    a.s_off = p->b.s_off;
+    a.S = p->b.S;
+    a.qp_delta = p->b.delta;
+    a.qp_sumq = p->b.sumq;
+    a.order_pairs = p->b.order_pairs;
+    a.bucket_end = p->b.buckets;
+    a.item_off = p->item_off;
+    a.item_counter = p->counter;
+    a.K = K;
+    a.D = (int)idx->D;
+    a.nprobe = (int)p->nprobe_run;
+    a.CB = (int)t.blocks_per_item;
+    (void)nq;
+    const int qb = (int)t.queries_per_item, w = (int)t.warps;
+    auto grid = [&](int i) { return p->sms * p->per_sm[i]; };
+    if (qb == 1 && w == 4) return scan_batched_launch<1, 4>(a, grid(0), st);
+    if (qb == 2 && w == 4) return scan_batched_launch<2, 4>(a, grid(1), st);
+    if (qb == 4 && w == 4) return scan_batched_launch<4, 4>(a, grid(2), st);
+    if (qb == 2 && w == 8) return scan_batched_launch<2, 8>(a, grid(3), st);
+    if (qb == 4 && w == 8) return scan_batched_launch<4, 8>(a, grid(4), st);
+    if (qb == 8 && w == 8) return scan_batched_launch<8, 8>(a, grid(5), st);
+    return fail(ERQ_ERR_INVALID_ARGUMENT, "unsupported scan tile (%d queries, %d warps)", qb, w);
+}
+
+// The device work of one batch of nq queries already in p->qin.
+erq_status plan_pipeline(erq_plan* p, uint64_t nq, const erq_plan_tuning& t, cudaStream_t st) {
+    const erq_index* idx = p->idx;
+    Batch& b = p->b;
+    b.nq = nq;
+    if (p->raw) {
+        ERQ_TRY(rotate_into(idx, p->qin, nq, p->qrot, b.qsplit, st));
+        b.qrot = p->qrot;
+    } else {
+        b.qrot = p->qin;
+    }
+    const int* qnp = nullptr;
+    if (p->model) {
+        const erq_probe_model* m = p->model;
+        const int B = (int)nq;
+        ERQ_TRY(features_device(idx, b, p->nprobe_run, p->near_d, p->feats, st));
+        {
+            LaunchTimer lt(kMlp, st);
+            mlp_standardise_kernel<<<(unsigned)div_up((uint64_t)B * kMlpIn, 256), 256, 0, st>>>(
+                p->feats, m->mean, m->stdv, p->wk.x, B * kMlpIn);
+            lt.finish();
+        }
+        ERQ_TRY(mlp_forward(m, p->wk, B, st));
+        {
+            LaunchTimer lt(kMlp, st);
+            mlp_softmax_xent_kernel<<<(unsigned)div_up(B, 128), 128, 0, st>>>(p->wk.z, nullptr, B,
+                                                                             p->wk.probs, nullptr, nullptr);
+            lt.finish();
+        }
+        {
+            LaunchTimer lt(kMlp, st);
+            mlp_choose_nprobe_kernel<<<(unsigned)div_up(B, 128), 128, 0, st>>>(
+                p->wk.probs, B, m->bins_dev, p->confidence, p->min_prob, (int)p->nprobe,
+                (int)p->nprobe_run, p->used);
+            lt.finish();
+        }
+        ERQ_CUDA(cudaGetLastError());
+        qnp = p->used;
+    } else {
+        ERQ_TRY(launch_probe_tc(idx, b, p->nprobe_run, st));
+    }
+    ERQ_TRY(order_pairs(idx, b, p->nprobe_run, st, qnp));
+    ERQ_TRY(order_queries(idx, b, p->nprobe_run, st));
+    ERQ_TRY(launch_scan_batched(p, nq, t, st));
+    ERQ_TRY(launch_refine(idx, b, p->nprobe_run, p->k, p->ids, p->dists, st, qnp, b.order_q));
+    return ERQ_OK;
+}
+
+// Graph of the pipeline for batch size nq, captured on first use.
+erq_status plan_graph(erq_plan* p, uint64_t nq, cudaGraphExec_t* out) {
+    auto it = p->graphs.find(nq);
+    if (it != p->graphs.end()) {
+        *out = it->second;
+        return ERQ_OK;
+    }
+    const erq_plan_tuning t = plan_tuning(p, nq);
+    cudaGraph_t g = nullptr;
+    ERQ_CUDA(cudaStreamBeginCapture(p->cap, cudaStreamCaptureModeThreadLocal));
+    erq_status s = plan_pipeline(p, nq, t, p->cap);
+    cudaError_t e = cudaStreamEndCapture(p->cap, &g);
+    if (s != ERQ_OK) {
+        if (g) cudaGraphDestroy(g);
+        return s;
+    }
+    if (e != cudaSuccess) return fail(ERQ_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
+    cudaGraphExec_t ge = nullptr;
+    e = cudaGraphInstantiate(&ge, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return fail(ERQ_ERR_CUDA, "graph instantiation failed: %s", cudaGetErrorString(e));
+    p->graphs[nq] = ge;
+    *out = ge;
+    return ERQ_OK;
+}
+
+erq_status plan_stage_queries(erq_plan* p, const float* queries, uint64_t nq, cudaStream_t st) {
+    const uint64_t cols = p->raw ? p->idx->DIM : p->idx->D;
+    ERQ_CUDA(cudaMemcpyAsync(p->qin, queries, nq * cols * sizeof(float), cudaMemcpyDefault, st));
+    return ERQ_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+erq_status erq_plan_create(const erq_index* idx, const erq_probe_model* model, uint64_t max_batch,
+                           uint64_t k, uint64_t nprobe, int raw_queries, erq_plan** out) {
+    if (!out) return fail(ERQ_ERR_INVALID_ARGUMENT, "out is NULL");
+    *out = nullptr;
+    if (!idx) return fail(ERQ_ERR_INVALID_ARGUMENT, "index is NULL");
+    if (max_batch == 0) return fail(ERQ_ERR_INVALID_ARGUMENT, "max_batch must be positive");
+    if (k == 0 || k > (uint64_t)kMaxTopK)
+        return fail(ERQ_ERR_INVALID_ARGUMENT, "k=%llu outside 1..%d", (unsigned long long)k, kMaxTopK);
+    if (nprobe == 0) return fail(ERQ_ERR_INVALID_ARGUMENT, "nprobe must be positive");
+    if (model && model->device != idx->device)
+        return fail(ERQ_ERR_INVALID_ARGUMENT, "model and index live on different devices");
+    DeviceGuard guard;
+    ERQ_TRY(guard.set(idx->device));
+    std::unique_ptr<erq_plan> p(new erq_plan());
+    p->idx = idx;
+    p->model = model;
+    p->max_batch = max_batch;
+    p->k = k;
+    p->nprobe = std::min<uint64_t>(nprobe, idx->K);
+    p->nprobe_run = model ? std::min<uint64_t>(idx->K, std::max<uint64_t>(p->nprobe, (uint64_t)model->bins[kMlpBins - 1]))
+                          : p->nprobe;
+    p->raw = raw_queries != 0;
+    ERQ_CUDA(cudaDeviceGetAttribute(&p->sms, cudaDevAttrMultiProcessorCount, idx->device));
+    ERQ_TRY(configure_kernels((int)idx->D, (int)idx->K, (int)k));
+    {
+        const int D = (int)idx->D;
+        ERQ_TRY((scan_batched_configure<1, 4>(D, &p->per_sm[0])));
+        ERQ_TRY((scan_batched_configure<2, 4>(D, &p->per_sm[1])));
+        ERQ_TRY((scan_batched_configure<4, 4>(D, &p->per_sm[2])));
+        ERQ_TRY((scan_batched_configure<2, 8>(D, &p->per_sm[3])));
+        ERQ_TRY((scan_batched_configure<4, 8>(D, &p->per_sm[4])));
+        ERQ_TRY((scan_batched_configure<8, 8>(D, &p->per_sm[5])));
+    }
+    ERQ_TRY(alloc_batch(p->arena, idx, max_batch, p->nprobe_run, p->b));
+    ERQ_TRY(p->arena.alloc(&p->qin, max_batch * (p->raw ? idx->DIM : idx->D)));
+    ERQ_TRY(p->arena.alloc(&p->qrot, max_batch * idx->D));
+    ERQ_TRY(p->arena.alloc(&p->ids, max_batch * k));
+    ERQ_TRY(p->arena.alloc(&p->dists, max_batch * k));
+    ERQ_TRY(p->arena.alloc(&p->used, max_batch));
+    ERQ_TRY(p->arena.alloc(&p->item_off, idx->K + 1));
+    ERQ_TRY(p->arena.alloc(&p->counter, 1));
+    if (model) {
+        ERQ_TRY(p->arena.alloc(&p->near_d, max_batch * kFeatDists));
+        ERQ_TRY(p->arena.alloc(&p->feats, max_batch * kMlpIn));
+        ERQ_TRY(mlp_alloc(p->arena, (int)max_batch, false, p->wk));
+    }
+    {
+        std::vector<int> np(max_batch, (int)p->nprobe);
+        ERQ_CUDA(cudaMemcpy(p->used, np.data(), max_batch * sizeof(int), cudaMemcpyHostToDevice));
+    }
+    ERQ_CUDA(cudaStreamCreateWithFlags(&p->cap, cudaStreamNonBlocking));
+    *out = p.release();
+    return ERQ_OK;
+}
+
+void erq_plan_free(erq_plan* plan) { delete plan; }
+
+erq_status erq_plan_set_learned(erq_plan* p, float confidence, float min_prob) {
+    if (!p) return fail(ERQ_ERR_INVALID_ARGUMENT, "plan is NULL");
+    if (!p->model) return fail(ERQ_ERR_INVALID_ARGUMENT, "the plan has no probe model");
+    if (!(confidence > 0.f && confidence <= 1.f))
+        return fail(ERQ_ERR_INVALID_ARGUMENT, "confidence must be in (0, 1]");
+    std::lock_guard<std::mutex> g(p->mu);
+    DeviceGuard guard;
+    ERQ_TRY(guard.set(p->idx->device));
+    p->confidence = confidence;
+    p->min_prob = min_prob;
+    p->drop_graphs();
+    return ERQ_OK;
+}
+
+erq_status erq_plan_set_tuning(erq_plan* p, uint64_t batch, const erq_plan_tuning* t) {
+    if (!p || !t) return fail(ERQ_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (!tuning_valid(*t)) return fail(ERQ_ERR_INVALID_ARGUMENT, "unsupported tuning");
+    std::lock_guard<std::mutex> g(p->mu);
+    DeviceGuard guard;
+    ERQ_TRY(guard.set(p->idx->device));
+    p->tunings[std::max<uint64_t>(batch, 1)] = *t;
+    p->drop_graphs();
+    return ERQ_OK;
+}
+
+erq_status erq_plan_get_tuning(const erq_plan* p, uint64_t batch, erq_plan_tuning* t) {
+    if (!p || !t) return fail(ERQ_ERR_INVALID_ARGUMENT, "NULL argument");
+    *t = plan_tuning(p, batch);
+    return ERQ_OK;
+}
+
+erq_status erq_plan_autotune(erq_plan* p, const float* queries, uint64_t n, int reps,
+                             erq_plan_tuning* chosen, float* best_ms) {
+    if (!p || !queries) return fail(ERQ_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (n == 0 || n > p->max_batch)
+        return fail(ERQ_ERR_INVALID_ARGUMENT, "sample of %llu queries outside 1..max_batch",
+                    (unsigned long long)n);
+    std::lock_guard<std::mutex> g(p->mu);
+    DeviceGuard guard;
+    ERQ_TRY(guard.set(p->idx->device));
+    cudaStream_t st = p->cap;
+    ERQ_TRY(plan_stage_queries(p, queries, n, st));
+    cudaEvent_t e0, e1;
+    ERQ_CUDA(cudaEventCreate(&e0));
+    ERQ_CUDA(cudaEventCreate(&e1));
+    float best = 1e30f;
+    erq_plan_tuning bt = default_tuning(n);
+    erq_status s = ERQ_OK;
+    for (const ScanShape& sh : kScanShapes) {
+        for (int cb : kChunkChoices) {
+            erq_plan_tuning t;
+            t.queries_per_item = (uint32_t)sh.qb;
+            t.blocks_per_item = (uint32_t)cb;
+            t.warps = (uint32_t)sh.warps;
+            if ((s = plan_pipeline(p, n, t, st)) != ERQ_OK) break;  // warm-up
+            float ms = 1e30f;
+            for (int r = 0; r < std::max(1, reps); ++r) {
+                cudaEventRecord(e0, st);
+                if ((s = plan_pipeline(p, n, t, st)) != ERQ_OK) break;
+                cudaEventRecord(e1, st);
+                cudaEventSynchronize(e1);
+                float x = 0.f;
+                cudaEventElapsedTime(&x, e0, e1);
+                ms = std::min(ms, x);
+            }
+            if (s != ERQ_OK) break;
+            if (ms < best) {
+                best = ms;
+                bt = t;
+            }
+        }
+        if (s != ERQ_OK) break;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    ERQ_TRY(s);
+    ERQ_CUDA(cudaStreamSynchronize(st));
+    p->tunings[n] = bt;
+    p->drop_graphs();
+    if (chosen) *chosen = bt;
+    if (best_ms) *best_ms = best;
+    return ERQ_OK;
+}
+
+erq_status erq_plan_search(erq_plan* p, const float* queries, uint64_t nq, uint32_t* ids,
+                           float* dists, uint32_t* nprobe_used, void* stream) {
+    if (!p) return fail(ERQ_ERR_INVALID_ARGUMENT, "plan is NULL");
+    if (nq == 0) return ERQ_OK;
+    if (!queries || !ids) return fail(ERQ_ERR_INVALID_ARGUMENT, "queries and ids are required");
+    if (nq > p->max_batch)
+        return fail(ERQ_ERR_INVALID_ARGUMENT, "batch of %llu exceeds the plan's max_batch %llu",
+                    (unsigned long long)nq, (unsigned long long)p->max_batch);
+    std::lock_guard<std::mutex> g(p->mu);
+    DeviceGuard guard;
+    ERQ_TRY(guard.set(p->idx->device));
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaGraphExec_t ge = nullptr;
+    ERQ_TRY(plan_graph(p, nq, &ge));
+    ERQ_TRY(plan_stage_queries(p, queries, nq, st));
+    ERQ_CUDA(cudaGraphLaunch(ge, st));
+    const bool host = !is_device_ptr(ids) || (dists && !is_device_ptr(dists)) ||
+                      (nprobe_used && !is_device_ptr(nprobe_used)) || !is_device_ptr(queries);
+    ERQ_CUDA(cudaMemcpyAsync(ids, p->ids, nq * p->k * sizeof(uint32_t), cudaMemcpyDefault, st));
+    if (dists)
+        ERQ_CUDA(cudaMemcpyAsync(dists, p->dists, nq * p->k * sizeof(float), cudaMemcpyDefault, st));
+    if (nprobe_used)  // a plan without a model keeps nprobe in every entry
+        ERQ_CUDA(cudaMemcpyAsync(nprobe_used, p->used, nq * sizeof(uint32_t), cudaMemcpyDefault, st));
+    if (host) ERQ_CUDA(cudaStreamSynchronize(st));
+    return ERQ_OK;
+}
+
+uint64_t erq_plan_device_bytes(const erq_plan* p) { return p ? p->arena.bytes : 0; }
 
 }  // extern "C"

@@ -8,8 +8,11 @@ include/erq.h); this package is its Python host side:
 * ``datasets``  - seeded synthetic datasets, k-means, exact ground truth
 * ``indexfile`` - reader/writer of the reference's index file format
 * ``metrics``   - recall@k and the reference's average distance ratio
+* ``plan``      - batched, graph-captured, autotuned search plans
+* ``learned``   - learned probing (probe MLP)
 """
 from ._lib import EXPORTED_SYMBOLS, ErqError, load_library  # noqa: F401
 from .ivf import IVF  # noqa: F401
+from .plan import Plan  # noqa: F401
 
-__all__ = ["IVF", "ErqError", "load_library", "EXPORTED_SYMBOLS"]
+__all__ = ["IVF", "Plan", "ErqError", "load_library", "EXPORTED_SYMBOLS"]

@@ -35,6 +35,8 @@ EXPORTED_SYMBOLS = (
     "erq_probe_model_free", "erq_probe_model_predict", "erq_search_learned",
     "erq_search_learned_raw",
     "erq_debug_probe_model_grads", "erq_debug_probe_model_params",
+    "erq_plan_create", "erq_plan_free", "erq_plan_set_learned", "erq_plan_autotune",
+    "erq_plan_set_tuning", "erq_plan_get_tuning", "erq_plan_search", "erq_plan_device_bytes",
 )
 
 
@@ -43,6 +45,18 @@ class ErqError(RuntimeError):
         self.status = status
         self.status_name = STATUS_NAMES.get(status, str(status))
         super().__init__(f"{self.status_name}: {message}")
+
+
+class PlanTuning(C.Structure):
+    _fields_ = [
+        ("queries_per_item", C.c_uint32),
+        ("blocks_per_item", C.c_uint32),
+        ("warps", C.c_uint32),
+    ]
+
+    def as_dict(self):
+        return {"queries_per_item": self.queries_per_item, "blocks_per_item": self.blocks_per_item,
+                "warps": self.warps}
 
 
 class IndexInfo(C.Structure):
@@ -97,6 +111,23 @@ def load_library(path: str | None = None) -> C.CDLL:
     lib.erq_debug_probe.restype = C.c_int
     lib.erq_debug_scan.argtypes = [vp, f32p, u64, u64, u32p, f32p, f32p, f32p, vp, vp, u64]
     lib.erq_debug_scan.restype = C.c_int
+    lib.erq_plan_create.argtypes = [vp, vp, u64, u64, u64, C.c_int, C.POINTER(C.c_void_p)]
+    lib.erq_plan_create.restype = C.c_int
+    lib.erq_plan_free.argtypes = [vp]
+    lib.erq_plan_free.restype = None
+    lib.erq_plan_set_learned.argtypes = [vp, C.c_float, C.c_float]
+    lib.erq_plan_set_learned.restype = C.c_int
+    lib.erq_plan_autotune.argtypes = [vp, vp, u64, C.c_int, C.POINTER(PlanTuning),
+                                      C.POINTER(C.c_float)]
+    lib.erq_plan_autotune.restype = C.c_int
+    lib.erq_plan_set_tuning.argtypes = [vp, u64, C.POINTER(PlanTuning)]
+    lib.erq_plan_set_tuning.restype = C.c_int
+    lib.erq_plan_get_tuning.argtypes = [vp, u64, C.POINTER(PlanTuning)]
+    lib.erq_plan_get_tuning.restype = C.c_int
+    lib.erq_plan_search.argtypes = [vp, vp, u64, vp, vp, vp, vp]
+    lib.erq_plan_search.restype = C.c_int
+    lib.erq_plan_device_bytes.argtypes = [vp]
+    lib.erq_plan_device_bytes.restype = u64
     lib.erq_profile_enable.argtypes = [C.c_int]
     lib.erq_profile_enable.restype = None
     lib.erq_profile_reset.restype = None

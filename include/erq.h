@@ -140,6 +140,54 @@ ERQ_API erq_status erq_search_learned_raw(const erq_index* index, const erq_prob
                                           float min_prob, uint32_t* ids, float* dists,
                                           uint32_t* nprobe_used, void* stream);
 
+/* ---------------------------------------------------------------------------
+ * Batched search plans.  No counterpart in the reference, which searches one
+ * query at a time (IVF::search, inc/index/IVF.hpp:295-324); a plan returns the
+ * same ids and distances as erq_search (plain) or erq_search_learned (with a
+ * model) for every query of a batch.
+ *
+ * A plan owns every device buffer a batch of up to max_batch queries needs, so
+ * erq_plan_search allocates nothing.  The first search of each batch size
+ * captures the pipeline (rotation when raw_queries, coarse probe, learned
+ * cut-off when a model is given, work list, scan, refinement) into a CUDA
+ * graph that later searches of that size replay.  The scan runs over a work
+ * list of (cluster, up to Q queries probing it, chunk of up to C 32-vector
+ * blocks) items in one persistent kernel; erq_plan_autotune times the tile
+ * choices on a sample batch and keeps the fastest for that batch size.
+ * Calls on one plan are serialised by the plan; use one plan per stream for
+ * concurrent batches. */
+typedef struct erq_plan erq_plan;
+
+typedef struct {
+    uint32_t queries_per_item;  /* Q: 1, 2, 4 or 8 */
+    uint32_t blocks_per_item;   /* C: cluster chunk, in 32-vector blocks */
+    uint32_t warps;             /* warps per scan block: 4 or 8 (Q = 1 needs 4, Q = 8 needs 8) */
+} erq_plan_tuning;
+
+/* model may be NULL (plain fixed-nprobe search); with a model, nprobe is the
+ * fallback probe count.  raw_queries: queries are DIM floats and are rotated
+ * inside, else they are rotated D floats. */
+ERQ_API erq_status erq_plan_create(const erq_index* index, const erq_probe_model* model,
+                                   uint64_t max_batch, uint64_t k, uint64_t nprobe,
+                                   int raw_queries, erq_plan** out);
+ERQ_API void erq_plan_free(erq_plan* plan);
+/* Confidence and minimum probability of the learned cut-off (defaults 0.9, 0). */
+ERQ_API erq_status erq_plan_set_learned(erq_plan* plan, float confidence, float min_prob);
+/* Times every tile choice on queries[n] (host or device; best of `reps` runs
+ * each) and keeps the fastest for batches of about n queries. */
+ERQ_API erq_status erq_plan_autotune(erq_plan* plan, const float* queries, uint64_t n, int reps,
+                                     erq_plan_tuning* chosen, float* best_ms);
+ERQ_API erq_status erq_plan_set_tuning(erq_plan* plan, uint64_t batch, const erq_plan_tuning* tuning);
+/* The tuning a batch of `batch` queries uses (the nearest tuned size, else a default). */
+ERQ_API erq_status erq_plan_get_tuning(const erq_plan* plan, uint64_t batch, erq_plan_tuning* tuning);
+/* Searches queries[nq] (nq <= max_batch).  Buffers may be host or device
+ * memory; with any host buffer the call returns when the results are in,
+ * otherwise it is asynchronous on `stream`.  dists and nprobe_used may be NULL. */
+ERQ_API erq_status erq_plan_search(erq_plan* plan, const float* queries, uint64_t nq, uint32_t* ids,
+                                   float* dists, uint32_t* nprobe_used, void* stream);
+/* Device bytes the plan holds. */
+ERQ_API uint64_t erq_plan_device_bytes(const erq_plan* plan);
+
 /* erq_search without any memory allocation.  Has no counterpart in the
  * reference: it is for callers that cannot allocate device memory while a
  * query runs - engines that hand all GPU memory to their own allocator up
