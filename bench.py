@@ -39,6 +39,8 @@ for _p in (PKG, ORACLE_DIR):
 
 import numpy as np  # noqa: E402
 
+MODE_NAMES = {"plain": "plain per-query", "batched": "batched plain (plan)",
+              "learned": "batched learned-probe (plan)"}
 METRIC = "QPS @ recall@100≥0.95, 1M×1536 8-bit: learned-probe vs plain GPU vs ref CPU"
 
 CONFIGS = {
@@ -388,17 +390,53 @@ def run_ours(args, cfg, name):
         plain["e2e"] = round(world * nq * args.steps / (ms_pe / 1e3), 1)
     scan_bytes_plain = int(nblocks[cids[:, :nprobe].astype(np.int64)].sum()) * block_bytes
 
-    # --- learned per-query depth
-    mode = "plain"
-    chosen = {"ms": ms_p, "prof": prof_p, "clocks": clocks_p, "recall": recall, "ids": ids0,
-              "scan_bytes": scan_bytes_plain, "e2e_ms": None}
+    # --- batched plans (CUDA graphs, work-list scan, autotuned tiles)
+    from erq_b200 import Plan
+
+    def plan_mode(plan, expect):
+        def dev():
+            plan.search_buffers(qd, ids_d, dist_d, stream=stream)
+
+        def host():
+            plan.search_buffers(qh, ids_h, dist_h, stream=stream)
+
+        ms, _, clocks = timed(dev, args.steps, args.warmup, world, stream, local)
+        assert (ids_d.cpu().numpy().view(np.uint32) == expect).all()
+        e2e = None
+        if not args.no_e2e:
+            e2e, _, _ = timed(host, args.steps, args.warmup, world, stream)
+            assert (ids_h.numpy().view(np.uint32) == expect).all()
+        # per-kernel times: the same steps with the kernels launched one by one
+        plan.set_graphs(False)
+        _, prof, _ = timed(dev, args.steps, 1, world, stream)
+        plan.set_graphs(True)
+        return ms, e2e, clocks, prof
+
+    modes = {"plain": {"ms": ms_p, "prof": prof_p, "clocks": clocks_p, "recall": recall,
+                       "ids": ids0, "scan_bytes": scan_bytes_plain, "e2e_ms": ms_pe}}
+    batched = None
+    if not args.no_batched:
+        plan_b = Plan(idx, max_batch=nq, k=k, nprobe=nprobe, raw=True)
+        tune_b, _ = plan_b.autotune(query, reps=2)
+        ms_b, e2e_b, clocks_b, prof_b = plan_mode(plan_b, ids0)
+        batched = {"value": round(world * nq * args.steps / (ms_b / 1e3), 1), "nprobe": nprobe,
+                   "recall@100": round(recall, 5), "ms_per_step": round(ms_b / args.steps, 4),
+                   "tuning": tune_b}
+        if e2e_b is not None:
+            batched["e2e"] = round(world * nq * args.steps / (e2e_b / 1e3), 1)
+        modes["batched"] = {"ms": ms_b, "prof": prof_b, "clocks": clocks_b, "recall": recall,
+                            "ids": ids0, "scan_bytes": scan_bytes_plain, "e2e_ms": e2e_b}
+        plan_b.free()
+
+    # --- learned per-query depth, batched
     learned_info = None
     if not args.no_learned and cfg.get("train_queries"):
         model, meta = learned_model(idx, d, cfg, nprobe)
-        used_h = np.empty(nq, np.uint32)
+        plan_l = Plan(idx, max_batch=nq, k=k, nprobe=nprobe, model=model, raw=True)
         best = None
         for conf in (0.5, 0.6, 0.7, 0.8, 0.9, 0.95, 0.99):
-            ids_l, _, used = learned.search_learned(idx, model, qrot_h, k, nprobe, conf)
+            plan_l.set_learned(conf)
+            ids_l, _, used = plan_l.search(query, with_dists=False, with_nprobe=True)
             r = metrics.recall_at_k(ids_l, gt, k)
             log(f"learned confidence={conf}: recall@{k}={r:.4f}, mean nprobe "
                 f"{used.mean():.3f}")
@@ -407,36 +445,24 @@ def run_ours(args, cfg, name):
                 break
         if best is not None:
             conf, r_l, ids_l, used = best
-            used_d = torch.empty(nq, dtype=torch.int32, device="cuda")
-
-            def learned_dev():
-                learned.search_learned_buffers(idx, model, qd, k, nprobe, conf, ids_d, dist_d,
-                                               used_d, raw=True, stream=stream)
-
-            def learned_host():
-                learned.search_learned_buffers(idx, model, qh, k, nprobe, conf, ids_h, dist_h,
-                                               None, raw=True, stream=stream)
-
-            ms_l, prof_l, clocks_l = timed(learned_dev, args.steps, args.warmup, world, stream,
-                                           local)
-            assert (ids_d.cpu().numpy().view(np.uint32) == ids_l).all()
-            e2e_l = None
-            if not args.no_e2e:
-                e2e_l, _, _ = timed(learned_host, args.steps, args.warmup, world, stream)
-                assert (ids_h.numpy().view(np.uint32) == ids_l).all()
+            plan_l.set_learned(conf)
+            tune_l, _ = plan_l.autotune(query, reps=2)
+            ms_l, e2e_l, clocks_l, prof_l = plan_mode(plan_l, ids_l)
             take = np.arange(cids.shape[1])[None, :] < used.astype(np.int64)[:, None]
             scan_bytes_l = int(nblocks[cids.astype(np.int64)][take].sum()) * block_bytes
             learned_info = {"value": round(world * nq * args.steps / (ms_l / 1e3), 1),
                             "confidence": conf, "mean_nprobe": round(float(used.mean()), 4),
                             "recall@100": round(r_l, 5),
-                            "ms_per_step": round(ms_l / args.steps, 4), "model": meta}
+                            "ms_per_step": round(ms_l / args.steps, 4), "tuning": tune_l,
+                            "model": meta}
             if e2e_l is not None:
                 learned_info["e2e"] = round(world * nq * args.steps / (e2e_l / 1e3), 1)
-            if ms_l < ms_p:
-                mode = "learned"
-                chosen = {"ms": ms_l, "prof": prof_l, "clocks": clocks_l, "recall": r_l,
-                          "ids": ids_l, "scan_bytes": scan_bytes_l, "e2e_ms": e2e_l}
+            modes["learned"] = {"ms": ms_l, "prof": prof_l, "clocks": clocks_l, "recall": r_l,
+                                "ids": ids_l, "scan_bytes": scan_bytes_l, "e2e_ms": e2e_l}
+        plan_l.free()
         model.free()
+    mode = min(modes, key=lambda m: modes[m]["ms"])
+    chosen = modes[mode]
 
     ratio = metrics.average_distance_ratio(query[:sub], base, chosen["ids"][:sub].astype(np.int64),
                                            gt[:sub].astype(np.int64), k)
@@ -455,7 +481,7 @@ def run_ours(args, cfg, name):
     if scan_n:
         per_launch_bytes = chosen["scan_bytes"] * args.steps / scan_n
         achieved = per_launch_bytes / (scan_ms / scan_n / 1e3) / 1e9
-    e2e_ms = chosen["e2e_ms"] if mode == "learned" else ms_pe
+    e2e_ms = chosen["e2e_ms"]
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         searcher, kind, note = cpu_searcher(index_path)
@@ -476,7 +502,7 @@ def run_ours(args, cfg, name):
             "ms_per_step": round(ms / args.steps, 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int32",
             "data": cfg["data"],
-            "config": {"workload": f"{name}: {'learned-probe' if mode == 'learned' else 'plain'} "
+            "config": {"workload": f"{name}: {MODE_NAMES[mode]} "
                                    f"GPU search, {cfg['n']}x{cfg['dim']}, K={cfg['K']}, "
                                    f"{cfg['bits']}-bit, {nq} queries per step, top-{k}",
                        "mode": mode, "nprobe": nprobe, "recall@100": round(chosen["recall"], 5),
@@ -486,6 +512,7 @@ def run_ours(args, cfg, name):
                              f"{chosen['scan_bytes'] / 1e9:.1f} GB of packed codes from a "
                              f"{os.path.getsize(index_path) / 1e9:.2f} GB index"},
             "plain_gpu": plain,
+            "batched_gpu": batched,
             "learned_gpu": learned_info,
             "e2e": None if e2e_ms is None else {
                 "value": round(world * nq * args.steps / (e2e_ms / 1e3), 1), "unit": "queries/s",
@@ -495,7 +522,8 @@ def run_ours(args, cfg, name):
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1) if achieved else None,
                          "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4) if achieved else None,
-                         "traffic": None, "kernel": "scan_kernel",
+                         "traffic": None,
+                         "kernel": "scan_kernel" if mode == "plain" else "scan_batched_kernel",
                          "peak_source": f"{peak_src} hbm_gbs (copy)"},
             "kernels_ms_per_step": {kk: round(v[1] / args.steps, 4) for kk, v in prof.items()
                                     if v[0]},
@@ -590,6 +618,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer e2e timing")
     ap.add_argument("--no-learned", action="store_true", help="plain fixed-nprobe search only")
+    ap.add_argument("--no-batched", action="store_true", help="skip the plain batched plan")
     ap.add_argument("--queries", type=int, default=0,
                     help="use only the first N queries of the batch (profiling cases)")
     ap.add_argument("--nprobe", type=int, default=0,

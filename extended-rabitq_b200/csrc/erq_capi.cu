@@ -1841,6 +1841,7 @@ struct erq_plan {
     uint32_t* item_off = nullptr;  // [K + 1]
     uint32_t* counter = nullptr;
     cudaStream_t cap = nullptr;
+    bool use_graphs = true;
     std::mutex mu;
     std::map<uint64_t, cudaGraphExec_t> graphs;
 
@@ -2176,10 +2177,15 @@ erq_status erq_plan_search(erq_plan* p, const float* queries, uint64_t nq, uint3
     DeviceGuard guard;
     ERQ_TRY(guard.set(p->idx->device));
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    cudaGraphExec_t ge = nullptr;
-    ERQ_TRY(plan_graph(p, nq, &ge));
-    ERQ_TRY(plan_stage_queries(p, queries, nq, st));
-    ERQ_CUDA(cudaGraphLaunch(ge, st));
+    if (p->use_graphs) {
+        cudaGraphExec_t ge = nullptr;
+        ERQ_TRY(plan_graph(p, nq, &ge));
+        ERQ_TRY(plan_stage_queries(p, queries, nq, st));
+        ERQ_CUDA(cudaGraphLaunch(ge, st));
+    } else {
+        ERQ_TRY(plan_stage_queries(p, queries, nq, st));
+        ERQ_TRY(plan_pipeline(p, nq, plan_tuning(p, nq), st));
+    }
     const bool host = !is_device_ptr(ids) || (dists && !is_device_ptr(dists)) ||
                       (nprobe_used && !is_device_ptr(nprobe_used)) || !is_device_ptr(queries);
     ERQ_CUDA(cudaMemcpyAsync(ids, p->ids, nq * p->k * sizeof(uint32_t), cudaMemcpyDefault, st));
@@ -2192,5 +2198,12 @@ erq_status erq_plan_search(erq_plan* p, const float* queries, uint64_t nq, uint3
 }
 
 uint64_t erq_plan_device_bytes(const erq_plan* p) { return p ? p->arena.bytes : 0; }
+
+erq_status erq_plan_set_graphs(erq_plan* p, int on) {
+    if (!p) return fail(ERQ_ERR_INVALID_ARGUMENT, "plan is NULL");
+    std::lock_guard<std::mutex> g(p->mu);
+    p->use_graphs = on != 0;
+    return ERQ_OK;
+}
 
 }  // extern "C"

@@ -66,6 +66,9 @@ class Plan:
         check(self._lib.erq_plan_get_tuning(self._h, batch, C.byref(t)))
         return t.as_dict()
 
+    def set_graphs(self, on: bool) -> None:
+        check(self._lib.erq_plan_set_graphs(self._h, 1 if on else 0))
+
     def device_bytes(self) -> int:
         return int(self._lib.erq_plan_device_bytes(self._h))
 

@@ -187,6 +187,9 @@ ERQ_API erq_status erq_plan_search(erq_plan* plan, const float* queries, uint64_
                                    float* dists, uint32_t* nprobe_used, void* stream);
 /* Device bytes the plan holds. */
 ERQ_API uint64_t erq_plan_device_bytes(const erq_plan* plan);
+/* on = 0 launches the kernels one by one instead of replaying a graph (same
+ * results; lets the kernel profiler of erq_debug.h time each launch). */
+ERQ_API erq_status erq_plan_set_graphs(erq_plan* plan, int on);
 
 /* erq_search without any memory allocation.  Has no counterpart in the
  * reference: it is for callers that cannot allocate device memory while a
