@@ -856,12 +856,15 @@ struct erq_probe_model {
     float* stdv = nullptr;          // [kMlpIn]
     int* bins_dev = nullptr;        // [kMlpBins] probe count of each class
     int bins[kMlpBins] = {};
+    __nv_bfloat16* w1d = nullptr;   // [256][640] = [W1 | W1], tensor-core inference
+    __nv_bfloat16* w2d = nullptr;   // [256][512] = [W2 | W2]
 
     ~erq_probe_model() {
         int prev = -1;
         cudaGetDevice(&prev);
         cudaSetDevice(device);
-        for (void* p : {(void*)w, (void*)wb, (void*)mean, (void*)stdv, (void*)bins_dev})
+        for (void* p : {(void*)w, (void*)wb, (void*)mean, (void*)stdv, (void*)bins_dev,
+                        (void*)w1d, (void*)w2d})
             if (p) cudaFree(p);
         if (prev >= 0) cudaSetDevice(prev);
     }
@@ -892,6 +895,8 @@ struct MlpWork {
     float* dh2 = nullptr;
     float* dh1 = nullptr;
     float* loss = nullptr;  // [B]
+    __nv_bfloat16* xs = nullptr;  // [B][640] split inputs (inference)
+    __nv_bfloat16* hs = nullptr;  // [B][512] split first hidden layer (inference)
 };
 
 template <class Alloc>
@@ -901,6 +906,10 @@ erq_status mlp_alloc(Alloc& s, int B, bool train, MlpWork& w) {
     ERQ_TRY(s.alloc(&w.h2, (size_t)B * kMlpHidden));
     ERQ_TRY(s.alloc(&w.z, (size_t)B * kMlpBins));
     ERQ_TRY(s.alloc(&w.probs, (size_t)B * kMlpBins));
+    if (!train) {
+        ERQ_TRY(s.alloc(&w.xs, (size_t)B * 2 * kMlpIn));
+        ERQ_TRY(s.alloc(&w.hs, (size_t)B * 2 * kMlpHidden));
+    }
     if (train) {
         ERQ_TRY(s.alloc(&w.dz, (size_t)B * kMlpBins));
         ERQ_TRY(s.alloc(&w.dh2, (size_t)B * kMlpHidden));
@@ -960,6 +969,8 @@ __global__ void mlp_gather_rows_kernel(const float* __restrict__ X, const uint8_
 }
 
 erq_status model_alloc(erq_probe_model* m) {
+    ERQ_CUDA(cudaMalloc(&m->w1d, sizeof(__nv_bfloat16) * kMlpHidden * 2 * kMlpIn));
+    ERQ_CUDA(cudaMalloc(&m->w2d, sizeof(__nv_bfloat16) * kMlpHidden * 2 * kMlpHidden));
     ERQ_CUDA(cudaMalloc(&m->w, sizeof(float) * kMlpParams));
     ERQ_CUDA(cudaMalloc(&m->wb, sizeof(__nv_bfloat16) * kMlpParams));
     ERQ_CUDA(cudaMalloc(&m->mean, sizeof(float) * kMlpIn));
@@ -968,6 +979,12 @@ erq_status model_alloc(erq_probe_model* m) {
     return ERQ_OK;
 }
 
+erq_status model_dup_weights(erq_probe_model* m, cudaStream_t st) {
+    mlp_dup_weights_kernel<<<(unsigned)div_up(kMlpHidden * 2 * kMlpIn, 256), 256, 0, st>>>(
+        m->wb, m->w1d, m->w2d);
+    ERQ_CUDA(cudaGetLastError());
+    return ERQ_OK;
+}
 erq_status model_upload(erq_probe_model* m, const std::vector<float>& w,
                         const std::vector<float>& mean, const std::vector<float>& stdv) {
     ERQ_CUDA(cudaMemcpy(m->w, w.data(), sizeof(float) * kMlpParams, cudaMemcpyHostToDevice));
@@ -976,7 +993,57 @@ erq_status model_upload(erq_probe_model* m, const std::vector<float>& w,
     ERQ_CUDA(cudaMemcpy(m->bins_dev, m->bins, sizeof(int) * kMlpBins, cudaMemcpyHostToDevice));
     mlp_to_bf16_kernel<<<(unsigned)div_up(kMlpParams, 256), 256>>>(m->w, m->wb, kMlpParams);
     ERQ_CUDA(cudaGetLastError());
+    ERQ_TRY(model_dup_weights(m, nullptr));
     ERQ_CUDA(cudaDeviceSynchronize());
+    return ERQ_OK;
+}
+
+// Forward pass for inference on tensor cores (mlp.cuh): probs[B][8] of raw
+// features feats[B][320].  Training and the gradient check use mlp_forward.
+erq_status mlp_infer(const erq_probe_model* m, const float* feats, const MlpWork& w, int B,
+                     float* probs, cudaStream_t st) {
+    if (B <= 0) return ERQ_OK;
+    {
+        LaunchTimer t(kMlp, st);
+        mlp_standardise_split_kernel<<<(unsigned)div_up((uint64_t)B * kMlpIn, 256), 256, 0, st>>>(
+            feats, m->mean, m->stdv, w.xs, B * kMlpIn);
+        t.finish();
+    }
+    {
+        GemmEpilogue e;
+        e.bias = m->w + kB1;
+        e.relu = true;
+        dim3 grid((unsigned)div_up(kMlpHidden, kGemmBN), (unsigned)div_up(B, kGemmBM));
+        LaunchTimer t(kMlp, st);
+        gemm_bf16_tn_kernel<<<grid, kGemmThreads, 0, st>>>(w.xs, m->w1d, w.h1, B, kMlpHidden,
+                                                          2 * kMlpIn, e);
+        t.finish();
+    }
+    {
+        LaunchTimer t(kMlp, st);
+        mlp_split_hidden_kernel<<<(unsigned)div_up((uint64_t)B * kMlpHidden, 256), 256, 0, st>>>(
+            w.h1, w.hs, B * kMlpHidden);
+        t.finish();
+    }
+    {
+        GemmEpilogue e;
+        e.bias = m->w + kB2;
+        e.relu = true;
+        dim3 grid((unsigned)div_up(kMlpHidden, kGemmBN), (unsigned)div_up(B, kGemmBM));
+        LaunchTimer t(kMlp, st);
+        gemm_bf16_tn_kernel<<<grid, kGemmThreads, 0, st>>>(w.hs, m->w2d, w.h2, B, kMlpHidden,
+                                                          2 * kMlpHidden, e);
+        t.finish();
+    }
+    ERQ_TRY(mlp_mm(w.h2, kMlpHidden, 1, m->wb + kW3, 1, kMlpHidden, w.z, B, kMlpBins, kMlpHidden,
+                   m->w + kB3, false, st));
+    {
+        LaunchTimer t(kMlp, st);
+        mlp_softmax_xent_kernel<<<(unsigned)div_up(B, 128), 128, 0, st>>>(w.z, nullptr, B, probs,
+                                                                         nullptr, nullptr);
+        t.finish();
+    }
+    ERQ_CUDA(cudaGetLastError());
     return ERQ_OK;
 }
 
@@ -1432,6 +1499,7 @@ erq_status erq_probe_model_train(const float* features, const uint8_t* labels, u
         }
         if (e == epochs - 1) last = seen ? sum / seen : 0.0;
     }
+    ERQ_TRY(model_dup_weights(m.get(), st));
     ERQ_CUDA(cudaStreamSynchronize(st));
     if (final_loss) *final_loss = (float)last;
     *out = m.release();
@@ -1520,17 +1588,16 @@ erq_status erq_probe_model_predict(const erq_probe_model* m, const float* featur
         pout = probs;
     }
     MlpWork wk;
-    for (float** p : {&wk.x, &wk.h1, &wk.h2, &wk.z}) {
-        const size_t cols = p == &wk.x ? kMlpIn : (p == &wk.z ? kMlpBins : kMlpHidden);
+    for (float** p : {&wk.h1, &wk.h2, &wk.z}) {
+        const size_t cols = p == &wk.z ? kMlpBins : kMlpHidden;
         ERQ_CUDA(cudaMalloc(p, n * cols * 4));
         owned.push_back(*p);
     }
-    mlp_standardise_kernel<<<(unsigned)div_up(n * kMlpIn, 256), 256, 0, st>>>(fin, m->mean, m->stdv,
-                                                                            wk.x, (int)(n * kMlpIn));
-    ERQ_TRY(mlp_forward(m, wk, (int)n, st));
-    mlp_softmax_xent_kernel<<<(unsigned)div_up(n, 128), 128, 0, st>>>(wk.z, nullptr, (int)n, pout,
-                                                                     nullptr, nullptr);
-    ERQ_CUDA(cudaGetLastError());
+    ERQ_CUDA(cudaMalloc(&wk.xs, n * 2 * kMlpIn * sizeof(__nv_bfloat16)));
+    owned.push_back(wk.xs);
+    ERQ_CUDA(cudaMalloc(&wk.hs, n * 2 * kMlpHidden * sizeof(__nv_bfloat16)));
+    owned.push_back(wk.hs);
+    ERQ_TRY(mlp_infer(m, fin, wk, (int)n, pout, st));
     if (!p_dev) ERQ_CUDA(cudaMemcpyAsync(probs, pout, n * kMlpBins * 4, cudaMemcpyDeviceToHost, st));
     ERQ_CUDA(cudaStreamSynchronize(st));
     return ERQ_OK;
@@ -1592,19 +1659,7 @@ static erq_status search_learned_entry(const erq_index* idx, const erq_probe_mod
         b.qrot = q + q0 * idx->D;
         const int B = (int)b.nq;
         ERQ_TRY(features_device(idx, b, nprobe_max, near_d, feats, st));
-        {
-            LaunchTimer t(kMlp, st);
-            mlp_standardise_kernel<<<(unsigned)div_up((uint64_t)B * kMlpIn, 256), 256, 0, st>>>(
-                feats, m->mean, m->stdv, wk.x, B * kMlpIn);
-            t.finish();
-        }
-        ERQ_TRY(mlp_forward(m, wk, B, st));
-        {
-            LaunchTimer t(kMlp, st);
-            mlp_softmax_xent_kernel<<<(unsigned)div_up(B, 128), 128, 0, st>>>(wk.z, nullptr, B,
-                                                                             wk.probs, nullptr, nullptr);
-            t.finish();
-        }
+        ERQ_TRY(mlp_infer(m, feats, wk, B, wk.probs, st));
         {
             LaunchTimer t(kMlp, st);
             mlp_choose_nprobe_kernel<<<(unsigned)div_up(B, 128), 128, 0, st>>>(
@@ -1956,19 +2011,7 @@ erq_status plan_pipeline(erq_plan* p, uint64_t nq, const erq_plan_tuning& t, cud
         const erq_probe_model* m = p->model;
         const int B = (int)nq;
         ERQ_TRY(features_device(idx, b, p->nprobe_run, p->near_d, p->feats, st));
-        {
-            LaunchTimer lt(kMlp, st);
-            mlp_standardise_kernel<<<(unsigned)div_up((uint64_t)B * kMlpIn, 256), 256, 0, st>>>(
-                p->feats, m->mean, m->stdv, p->wk.x, B * kMlpIn);
-            lt.finish();
-        }
-        ERQ_TRY(mlp_forward(m, p->wk, B, st));
-        {
-            LaunchTimer lt(kMlp, st);
-            mlp_softmax_xent_kernel<<<(unsigned)div_up(B, 128), 128, 0, st>>>(p->wk.z, nullptr, B,
-                                                                             p->wk.probs, nullptr, nullptr);
-            lt.finish();
-        }
+        ERQ_TRY(mlp_infer(m, p->feats, p->wk, B, p->wk.probs, st));
         {
             LaunchTimer lt(kMlp, st);
             mlp_choose_nprobe_kernel<<<(unsigned)div_up(B, 128), 128, 0, st>>>(

@@ -60,10 +60,13 @@ __global__ void split_rows_kernel(const float* __restrict__ in, int R, int C, in
 constexpr int kGemmBM = 128, kGemmBN = 128, kGemmBK = 32;
 constexpr int kGemmThreads = 256;
 
-// Epilogue: C = acc, or (ranking) C = rn[row] + cn[col] - 2 * acc.
+// Epilogue: C = acc, or (ranking) C = rn[row] + cn[col] - 2 * acc, or
+// (MLP layers) C = acc + bias[col], then max(C, 0) when relu.
 struct GemmEpilogue {
     const float* row_norm = nullptr;
     const float* col_norm = nullptr;
+    const float* bias = nullptr;
+    bool relu = false;
 };
 
 __device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, bool valid) {
@@ -175,6 +178,8 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_bf16_tn_kernel(
                 if (row < M && col < N) {
                     float v = acc[i][j][e];
                     if (epi.row_norm) v = epi.row_norm[row] + epi.col_norm[col] - 2.f * v;
+                    if (epi.bias) v += epi.bias[col];
+                    if (epi.relu) v = fmaxf(v, 0.f);
                     Cout[(size_t)row * N + col] = v;
                 }
             }

@@ -143,6 +143,51 @@ __global__ void mlp_standardise_kernel(const float* __restrict__ f, const float*
     }
 }
 
+// Tensor-core inference.  Activations x (FP32) are split as x = hi + lo with
+// hi = bf16(x), lo = bf16(x - hi), written [hi | lo] per row; the weights are
+// duplicated as [W | W], so one BF16 GEMM with FP32 accumulation gives
+// hi.W + lo.W, x.W to within 2^-16 relative (the BF16 weights are exact).
+__device__ __forceinline__ void split2(float x, __nv_bfloat16* hi, __nv_bfloat16* lo) {
+    const __nv_bfloat16 h = __float2bfloat16_rn(x);
+    *hi = h;
+    *lo = __float2bfloat16_rn(x - __bfloat162float(h));
+}
+
+// xs[r] = [hi | lo] of (f[r] - mean) / std, 2 * kMlpIn columns.
+__global__ void mlp_standardise_split_kernel(const float* __restrict__ f, const float* __restrict__ mean,
+                                             const float* __restrict__ stdv,
+                                             __nv_bfloat16* __restrict__ xs, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int r = i / kMlpIn, c = i - r * kMlpIn;
+    const float x = (f[i] - mean[c]) / stdv[c];
+    split2(x, xs + (size_t)r * 2 * kMlpIn + c, xs + (size_t)r * 2 * kMlpIn + kMlpIn + c);
+}
+
+// hs[r] = [hi | lo] of h[r], 2 * kMlpHidden columns.
+__global__ void mlp_split_hidden_kernel(const float* __restrict__ h, __nv_bfloat16* __restrict__ hs,
+                                        int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int r = i / kMlpHidden, c = i - r * kMlpHidden;
+    split2(h[i], hs + (size_t)r * 2 * kMlpHidden + c, hs + (size_t)r * 2 * kMlpHidden + kMlpHidden + c);
+}
+
+// w1d = [W1 | W1] ([256][640]), w2d = [W2 | W2] ([256][512]) from the BF16 copy.
+__global__ void mlp_dup_weights_kernel(const __nv_bfloat16* __restrict__ wb,
+                                       __nv_bfloat16* __restrict__ w1d,
+                                       __nv_bfloat16* __restrict__ w2d) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < kMlpHidden * 2 * kMlpIn) {
+        const int r = i / (2 * kMlpIn), c = (i - r * 2 * kMlpIn) % kMlpIn;
+        w1d[i] = wb[kW1 + r * kMlpIn + c];
+    }
+    if (i < kMlpHidden * 2 * kMlpHidden) {
+        const int r = i / (2 * kMlpHidden), c = (i - r * 2 * kMlpHidden) % kMlpHidden;
+        w2d[i] = wb[kW2 + r * kMlpHidden + c];
+    }
+}
+
 // Raw features of one query: 256 sketch dims (the first rotated coordinates,
 // a random projection, scaled by 16/||q_r||) and 64 values of its nearest
 // centroid distances e_0 <= e_1 <= ...: log(e_0 / ||q_r||^2 + 1e-12) and

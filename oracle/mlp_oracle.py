@@ -35,6 +35,19 @@ def unpack(params):
     return w1, b1, w2, b2, w3, b3
 
 
+def probabilities(params, mean, std, features):
+    """Softmax output [n, 8] of the forward pass, float64."""
+    w1, b1, w2, b2, w3, b3 = unpack(params)
+    x = (np.asarray(features, np.float32) - mean) / std
+    x = x.astype(np.float32).astype(np.float64)
+    h1 = np.maximum(x @ w1.T + b1, 0.0)
+    h2 = np.maximum(h1 @ w2.T + b2, 0.0)
+    z = h2 @ w3.T + b3
+    z -= z.max(axis=1, keepdims=True)
+    p = np.exp(z)
+    return p / p.sum(axis=1, keepdims=True)
+
+
 def loss_and_grads(params, mean, std, features, labels):
     w1, b1, w2, b2, w3, b3 = unpack(params)
     x = (np.asarray(features, np.float32) - mean) / std

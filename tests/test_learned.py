@@ -41,6 +41,10 @@ def test_gradients_match_fp64_oracle():
     loss, g = model.grads(fb, yb)
     loss_o, g_o = mlp_oracle.loss_and_grads(params, mean, std, fb, yb)
     assert loss == pytest.approx(loss_o, rel=1e-5)
+    # inference runs on tensor cores (split-BF16 activations): probabilities
+    # within 1e-4 of the float64 forward pass
+    probs = model.predict(fb)
+    assert np.abs(probs - mlp_oracle.probabilities(params, mean, std, fb)).max() < 1e-4
     for lo, hi in [(mlp_oracle.W1, mlp_oracle.B1), (mlp_oracle.B1, mlp_oracle.W2),
                    (mlp_oracle.W2, mlp_oracle.B2), (mlp_oracle.B2, mlp_oracle.W3),
                    (mlp_oracle.W3, mlp_oracle.B3), (mlp_oracle.B3, mlp_oracle.N_PARAMS)]:
