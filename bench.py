@@ -52,6 +52,13 @@ CONFIGS = {
         data="synthetic: seeded 4096-component unit-sphere mixture, tangent sigma 0.05, "
              "1M base + 10k queries (+200k training queries for the probe model), d=1536 "
              "(openai1536 stand-in)"),
+    # batched search over very uneven clusters: Zipf(1.1) component weights
+    "zipf1536-2M-7bit": dict(
+        gen="sphere", n=2_000_000, dim=1536, comps=4096, sigma=0.05, zipf=1.1, K=4096,
+        bits=7, nq=8192, k=100, seed=20242, nprobe=None, recall_target=0.95,
+        train_queries=0, save_base=False, latency_batches=(1, 64, 1024, 8192),
+        data="synthetic: seeded 4096-component unit-sphere mixture with Zipf(1.1) component "
+             "weights, tangent sigma 0.05, 2M base + 8192 queries, d=1536"),
     # the small CPU-runnable case
     "gauss128-100k-4bit": dict(
         gen="gauss", n=100_000, dim=128, comps=256, sigma=0.3, zipf=None, K=1024,
@@ -113,8 +120,9 @@ def prepare(name, cfg, device="cuda"):
     np.save(os.path.join(d, "query.npy"), query.cpu().numpy())
     np.save(os.path.join(d, "gt.npy"), gt.cpu().numpy().astype(np.uint32))
     np.save(os.path.join(d, "gt_dist.npy"), gtd.cpu().numpy())
-    # a slice of the base for the distance-ratio metric on a query subset
-    np.save(os.path.join(d, "base.npy"), base.cpu().numpy())
+    # the base for the distance-ratio metric on a query subset
+    if cfg.get("save_base", True):
+        np.save(os.path.join(d, "base.npy"), base.cpu().numpy())
     log(f"ground truth done at {time.time() - t0:.1f}s")
     del base, query, cent, ids, gt, gtd
     torch.cuda.empty_cache()
@@ -535,6 +543,91 @@ def run_ours(args, cfg, name):
     dist_finish(world)
 
 
+# ---------------------------------------------------- batched latency mode
+def run_latency(args, cfg, name):
+    """Per batch size B of cfg["latency_batches"]: a plan autotuned for B,
+    then calls of B queries (already in device memory) timed one by one with
+    CUDA events; QPS = queries / summed call time, p50 / p99 of the calls."""
+    import torch
+
+    from erq_b200 import IVF, Plan, metrics
+
+    world, rank, local = dist_setup(args)
+    torch.cuda.set_device(local)
+    if rank == 0:
+        d = prepare(name, cfg)
+    barrier(world)
+    d = prepare(name, cfg) if rank != 0 else d
+    index_path = os.path.join(d, "ivf.index")
+    query = np.load(os.path.join(d, "query.npy"))
+    gt = np.load(os.path.join(d, "gt.npy"))
+    nq, k = query.shape[0], cfg["k"]
+    idx = IVF(index_path, device=local)
+    if args.nprobe:
+        cfg = dict(cfg, nprobe=args.nprobe)
+    nprobe, recall, ids0 = choose_nprobe(idx, query, gt, cfg)
+    sizes = indexfile_sizes(index_path)
+    stream = torch.cuda.current_stream()
+    qd = torch.from_numpy(query).cuda()
+    out = {}
+    sampler = ClockSampler(local) if rank == 0 else None
+    if sampler:
+        sampler.mark_start()
+    for B in cfg["latency_batches"]:
+        plan = Plan(idx, max_batch=B, k=k, nprobe=nprobe, raw=True)
+        tune, _ = plan.autotune(query[:B], reps=2)
+        ids_d = torch.empty((B, k), dtype=torch.int32, device="cuda")
+        calls = max(args.steps, min(2000, (4 * nq) // B))
+        starts = list(range(0, nq - B + 1, B)) or [0]
+        for w in range(args.warmup):
+            s0 = starts[w % len(starts)]
+            plan.search_buffers(qd[s0:s0 + B], ids_d, stream=stream)
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(calls)]
+        torch.cuda.synchronize()
+        barrier(world)
+        for c in range(calls):
+            s0 = starts[c % len(starts)]
+            ev[c][0].record(stream)
+            plan.search_buffers(qd[s0:s0 + B], ids_d, stream=stream)
+            ev[c][1].record(stream)
+        torch.cuda.synchronize()
+        lat = np.array([a.elapsed_time(b) for a, b in ev])
+        tot = max_over_ranks(float(lat.sum()), world)
+        # results equal the plain search's
+        s0 = starts[(calls - 1) % len(starts)]
+        assert (ids_d.cpu().numpy().view(np.uint32) == ids0[s0:s0 + B]).all()
+        out[str(B)] = {"qps": round(world * B * calls / (tot / 1e3), 1),
+                       "p50_ms": round(float(np.percentile(lat, 50)), 4),
+                       "p99_ms": round(float(np.percentile(lat, 99)), 4),
+                       "calls": calls, "tuning": tune}
+        log(f"batch {B}: {out[str(B)]}")
+        plan.free()
+    clocks = sampler.stop() if sampler else None
+    if rank == 0:
+        big = str(max(cfg["latency_batches"]))
+        print(json.dumps({
+            "metric": f"QPS and per-batch p50/p99 latency, {name}", "value": out[big]["qps"],
+            "unit": "queries/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+            "data": cfg["data"],
+            "config": {"workload": f"{name}: batched plain plans, {cfg['n']}x{cfg['dim']}, "
+                                   f"K={cfg['K']}, {cfg['bits']}-bit, top-{k}",
+                       "nprobe": nprobe, "recall@100": round(recall, 5),
+                       "cluster_sizes": {"min": int(sizes.min()), "median": int(np.median(sizes)),
+                                         "max": int(sizes.max())}},
+            "batches": out, "clocks": clocks}), flush=True)
+    idx.free()
+    dist_finish(world)
+
+
+def indexfile_sizes(path):
+    """Cluster sizes from the index header (N, DIM, K, EX, then K sizes)."""
+    with open(path, "rb") as f:
+        hdr = np.fromfile(f, np.uint64, 4)
+        return np.fromfile(f, np.uint64, int(hdr[2])).astype(np.int64)
+
+
 # ------------------------------------------------------------ reference arm
 def run_reference(args, cfg, name):
     rank = int(os.environ.get("RANK", "0"))
@@ -635,7 +728,10 @@ def main():
     if args.impl == "reference":
         run_reference(args, cfg, args.config)
     else:
-        run_ours(args, cfg, args.config)
+        if cfg.get("latency_batches"):
+            run_latency(args, cfg, args.config)
+        else:
+            run_ours(args, cfg, args.config)
 
 
 if __name__ == "__main__":
