@@ -10,6 +10,7 @@
 // Per-call scratch comes from the stream-ordered allocator on the caller's
 // stream, so concurrent calls on different streams never share workspace.
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <cstdarg>
@@ -28,6 +29,7 @@
 #include "../../include/erq_debug.h"
 #include "coarse.cuh"
 #include "gemm.cuh"
+#include "gemm_tc.cuh"
 #include "mlp.cuh"
 #include "probe.cuh"
 #include "layout.cuh"
@@ -467,6 +469,123 @@ erq_status configure_kernels(int D, int K, int k) {
     return ERQ_OK;
 }
 
+// ------------------------------------------------------------ tcgen05 GEMM
+constexpr int kMaxDevices = 64;
+// Wait status of gemm_tc_kernel (bit 0: a bounded wait ran out), one word per
+// device image of the library.
+__device__ uint32_t g_tc_status;
+
+erq_status tc_status_ptr(uint32_t** out) {
+    static std::mutex mu;
+    static uint32_t* ptrs[kMaxDevices] = {};
+    int dev = 0;
+    ERQ_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) return fail(ERQ_ERR_UNSUPPORTED, "device ordinal %d", dev);
+    std::lock_guard<std::mutex> g(mu);
+    if (!ptrs[dev]) {
+        void* p = nullptr;
+        ERQ_CUDA(cudaGetSymbolAddress(&p, g_tc_status));
+        ptrs[dev] = static_cast<uint32_t*>(p);
+    }
+    *out = ptrs[dev];
+    return ERQ_OK;
+}
+
+// Copies the status word into pinned host memory on `st` (before a call
+// synchronises); tc_status_check reads it afterwards.
+erq_status tc_status_fetch(cudaStream_t st, uint32_t** host_word) {
+    static std::mutex mu;
+    static uint32_t* pinned[kMaxDevices] = {};
+    uint32_t* dword = nullptr;
+    ERQ_TRY(tc_status_ptr(&dword));
+    int dev = 0;
+    ERQ_CUDA(cudaGetDevice(&dev));
+    {
+        std::lock_guard<std::mutex> g(mu);
+        if (!pinned[dev]) {
+            ERQ_CUDA(cudaMallocHost(&pinned[dev], sizeof(uint32_t)));
+            *pinned[dev] = 0;
+        }
+    }
+    ERQ_CUDA(cudaMemcpyAsync(pinned[dev], dword, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    *host_word = pinned[dev];
+    return ERQ_OK;
+}
+erq_status tc_status_check(uint32_t* host_word) {
+    if (host_word && *host_word) {
+        *host_word = 0;
+        uint32_t* dword = nullptr;
+        ERQ_TRY(tc_status_ptr(&dword));
+        ERQ_CUDA(cudaMemset(dword, 0, sizeof(uint32_t)));
+        return fail(ERQ_ERR_TIMEOUT, "a bounded wait in the tcgen05 GEMM ran out; results are incomplete");
+    }
+    return ERQ_OK;
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        cudaDriverEntryPointQueryResult q;
+        void* f = nullptr;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+    });
+    return fn;
+}
+
+// 2-D map of a row-major BF16 matrix [rows][cols]: boxes of 64 columns
+// (128 bytes, the swizzle span) by box_rows rows, 128-byte swizzle, zero fill
+// outside the matrix.
+erq_status tensor_map_bf16(CUtensorMap* m, const void* ptr, uint64_t rows, uint64_t cols,
+                           uint32_t box_rows) {
+    auto fn = tensor_map_encoder();
+    if (!fn) return fail(ERQ_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+    if ((reinterpret_cast<uintptr_t>(ptr) & 15) || (cols * 2) % 16)
+        return fail(ERQ_ERR_INVALID_ARGUMENT, "TMA operand not 16-byte aligned");
+    cuuint64_t dims[2] = {cols, rows};
+    cuuint64_t strides[1] = {cols * 2};
+    cuuint32_t box[2] = {64, box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(ptr), dims, strides, box,
+                    estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(ERQ_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return ERQ_OK;
+}
+
+// C[M][N] = A[M][Kd] * B[N][Kd]^T (BF16, FP32 accumulate) with an epilogue,
+// on tcgen05 (gemm_tc.cuh).  Kd must be a multiple of 64.
+erq_status gemm_tc(const __nv_bfloat16* A, const __nv_bfloat16* B, float* C, int M, int N, int Kd,
+                   const GemmEpilogue& epi, int kernel_id, cudaStream_t st) {
+    if (M <= 0 || N <= 0) return ERQ_OK;
+    if (Kd <= 0 || Kd % kTcBK) return fail(ERQ_ERR_INVALID_ARGUMENT, "GEMM depth %d not a multiple of 64", Kd);
+    CUtensorMap ta, tb;
+    ERQ_TRY(tensor_map_bf16(&ta, A, (uint64_t)M, (uint64_t)Kd, kTcBM));
+    ERQ_TRY(tensor_map_bf16(&tb, B, (uint64_t)N, (uint64_t)Kd, kTcBN));
+    uint32_t* status = nullptr;
+    ERQ_TRY(tc_status_ptr(&status));
+    {
+        static std::mutex mu;
+        static bool configured[kMaxDevices] = {};
+        int dev = 0;
+        ERQ_CUDA(cudaGetDevice(&dev));
+        std::lock_guard<std::mutex> g(mu);
+        if (!configured[dev]) {
+            ERQ_CUDA(cudaFuncSetAttribute(gemm_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)gemm_tc_smem_bytes()));
+            configured[dev] = true;
+        }
+    }
+    dim3 grid((unsigned)div_up(N, kTcBN), (unsigned)div_up(M, kTcBM));
+    LaunchTimer t(kernel_id, st);
+    gemm_tc_kernel<<<grid, kTcThreads, gemm_tc_smem_bytes(), st>>>(ta, tb, C, M, N, Kd, epi, status);
+    t.finish();
+    ERQ_CUDA(cudaGetLastError());
+    return ERQ_OK;
+}
+
 // Device buffers of one query batch.
 struct Batch {
     const float* qrot = nullptr;  // [nq][D] on device
@@ -602,12 +721,7 @@ erq_status launch_probe_tc(const erq_index* idx, const Batch& b, uint64_t nprobe
         GemmEpilogue epi;
         epi.row_norm = b.qn;
         epi.col_norm = idx->cn;
-        dim3 grid((unsigned)div_up(K, kGemmBN), (unsigned)div_up(b.nq, kGemmBM));
-        LaunchTimer t(kGemm, st);
-        gemm_bf16_tn_kernel<<<grid, kGemmThreads, 0, st>>>(b.qsplit, idx->c_split, b.dist,
-                                                          (int)b.nq, K, 3 * D, epi);
-        t.finish();
-        ERQ_CUDA(cudaGetLastError());
+        ERQ_TRY(gemm_tc(b.qsplit, idx->c_split, b.dist, (int)b.nq, K, 3 * D, epi, kGemm, st));
     }
     ProbeArgs a;
     a.approx = b.dist;
@@ -780,13 +894,7 @@ erq_status rotate_into(const erq_index* idx, const float* q_dev, uint64_t nq, fl
         t.finish();
         ERQ_CUDA(cudaGetLastError());
     }
-    dim3 grid((unsigned)div_up(D, kGemmBN), (unsigned)div_up(nq, kGemmBM));
-    LaunchTimer t(kRotate, st);
-    gemm_bf16_tn_kernel<<<grid, kGemmThreads, 0, st>>>(qs, idx->pt_split, out_dev, (int)nq, D,
-                                                      3 * D, GemmEpilogue());
-    t.finish();
-    ERQ_CUDA(cudaGetLastError());
-    return ERQ_OK;
+    return gemm_tc(qs, idx->pt_split, out_dev, (int)nq, D, 3 * D, GemmEpilogue(), kRotate, st);
 }
 
 erq_status rotate_device(const erq_index* idx, const float* q_dev, uint64_t nq, float* out_dev,
@@ -840,7 +948,12 @@ erq_status search_entry(const erq_index* idx, const float* queries, bool rotated
         ERQ_CUDA(cudaMemcpyAsync(ids, ids_out, nq * k * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
     if (!d_dev)
         ERQ_CUDA(cudaMemcpyAsync(dists, d_out, nq * k * sizeof(float), cudaMemcpyDeviceToHost, st));
-    if (host_io) ERQ_CUDA(cudaStreamSynchronize(st));
+    if (host_io) {
+        uint32_t* hw = nullptr;
+        ERQ_TRY(tc_status_fetch(st, &hw));
+        ERQ_CUDA(cudaStreamSynchronize(st));
+        ERQ_TRY(tc_status_check(hw));
+    }
     return ERQ_OK;
 }
 
@@ -1013,11 +1126,7 @@ erq_status mlp_infer(const erq_probe_model* m, const float* feats, const MlpWork
         GemmEpilogue e;
         e.bias = m->w + kB1;
         e.relu = true;
-        dim3 grid((unsigned)div_up(kMlpHidden, kGemmBN), (unsigned)div_up(B, kGemmBM));
-        LaunchTimer t(kMlp, st);
-        gemm_bf16_tn_kernel<<<grid, kGemmThreads, 0, st>>>(w.xs, m->w1d, w.h1, B, kMlpHidden,
-                                                          2 * kMlpIn, e);
-        t.finish();
+        ERQ_TRY(gemm_tc(w.xs, m->w1d, w.h1, B, kMlpHidden, 2 * kMlpIn, e, kMlp, st));
     }
     {
         LaunchTimer t(kMlp, st);
@@ -1029,11 +1138,7 @@ erq_status mlp_infer(const erq_probe_model* m, const float* feats, const MlpWork
         GemmEpilogue e;
         e.bias = m->w + kB2;
         e.relu = true;
-        dim3 grid((unsigned)div_up(kMlpHidden, kGemmBN), (unsigned)div_up(B, kGemmBM));
-        LaunchTimer t(kMlp, st);
-        gemm_bf16_tn_kernel<<<grid, kGemmThreads, 0, st>>>(w.hs, m->w2d, w.h2, B, kMlpHidden,
-                                                          2 * kMlpHidden, e);
-        t.finish();
+        ERQ_TRY(gemm_tc(w.hs, m->w2d, w.h2, B, kMlpHidden, 2 * kMlpHidden, e, kMlp, st));
     }
     ERQ_TRY(mlp_mm(w.h2, kMlpHidden, 1, m->wb + kW3, 1, kMlpHidden, w.z, B, kMlpBins, kMlpHidden,
                    m->w + kB3, false, st));
@@ -1070,7 +1175,6 @@ constexpr uint64_t kNoAllocScratchBytes = 64ull << 20;
 static __device__ __align__(256) uint8_t g_noalloc_scratch[kNoAllocScratchBytes];
 
 namespace {
-constexpr int kMaxDevices = 64;
 std::mutex g_noalloc_mu;
 uint8_t* g_noalloc_ptr[kMaxDevices] = {};
 
@@ -1682,7 +1786,12 @@ static erq_status search_learned_entry(const erq_index* idx, const erq_probe_mod
         ERQ_CUDA(cudaMemcpyAsync(ids, ids_out, nq * k * 4, cudaMemcpyDeviceToHost, st));
     if (!d_dev)
         ERQ_CUDA(cudaMemcpyAsync(dists, d_out, nq * k * 4, cudaMemcpyDeviceToHost, st));
-    if (!q_dev || !ids_dev || !d_dev || !u_dev) ERQ_CUDA(cudaStreamSynchronize(st));
+    if (!q_dev || !ids_dev || !d_dev || !u_dev) {
+        uint32_t* hw = nullptr;
+        ERQ_TRY(tc_status_fetch(st, &hw));
+        ERQ_CUDA(cudaStreamSynchronize(st));
+        ERQ_TRY(tc_status_check(hw));
+    }
     return ERQ_OK;
 }
 
@@ -1788,6 +1897,42 @@ void erq_profile_reset(void) {
         p.launches[i] = 0;
         p.ms[i] = 0.0;
     }
+}
+
+erq_status erq_debug_gemm_bf16(const uint16_t* A, const uint16_t* B, uint64_t M, uint64_t N,
+                               uint64_t Kd, float* C, int device) {
+    if (!A || !B || !C) return fail(ERQ_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (M == 0 || N == 0 || Kd == 0 || M > (1u << 30) || N > (1u << 30) || Kd > (1u << 20))
+        return fail(ERQ_ERR_INVALID_ARGUMENT, "bad GEMM shape");
+    DeviceGuard guard;
+    ERQ_TRY(guard.set(device));
+    std::vector<void*> owned;
+    struct Free {
+        std::vector<void*>& v;
+        ~Free() {
+            for (void* p : v) cudaFree(p);
+        }
+    } frees{owned};
+    __nv_bfloat16 *a = nullptr, *b = nullptr;
+    float* c = nullptr;
+    ERQ_CUDA(cudaMalloc(&a, M * Kd * 2));
+    owned.push_back(a);
+    ERQ_CUDA(cudaMalloc(&b, N * Kd * 2));
+    owned.push_back(b);
+    ERQ_CUDA(cudaMalloc(&c, M * N * 4));
+    owned.push_back(c);
+    ERQ_CUDA(cudaMemcpy(a, A, M * Kd * 2, cudaMemcpyHostToDevice));
+    ERQ_CUDA(cudaMemcpy(b, B, N * Kd * 2, cudaMemcpyHostToDevice));
+    uint32_t* status = nullptr;
+    ERQ_TRY(tc_status_ptr(&status));
+    ERQ_CUDA(cudaMemset(status, 0, 4));
+    ERQ_TRY(gemm_tc(a, b, c, (int)M, (int)N, (int)Kd, GemmEpilogue(), kGemm, nullptr));
+    ERQ_CUDA(cudaDeviceSynchronize());
+    uint32_t st = 0;
+    ERQ_CUDA(cudaMemcpy(&st, status, 4, cudaMemcpyDeviceToHost));
+    if (st) return fail(ERQ_ERR_TIMEOUT, "a wait in the tcgen05 GEMM reached its limit");
+    ERQ_CUDA(cudaMemcpy(C, c, M * N * 4, cudaMemcpyDeviceToHost));
+    return ERQ_OK;
 }
 
 erq_status erq_profile_read(const char* kernel, uint64_t* launches, double* total_ms) {
@@ -2236,7 +2381,12 @@ erq_status erq_plan_search(erq_plan* p, const float* queries, uint64_t nq, uint3
         ERQ_CUDA(cudaMemcpyAsync(dists, p->dists, nq * p->k * sizeof(float), cudaMemcpyDefault, st));
     if (nprobe_used)  // a plan without a model keeps nprobe in every entry
         ERQ_CUDA(cudaMemcpyAsync(nprobe_used, p->used, nq * sizeof(uint32_t), cudaMemcpyDefault, st));
-    if (host) ERQ_CUDA(cudaStreamSynchronize(st));
+    if (host) {
+        uint32_t* hw = nullptr;
+        ERQ_TRY(tc_status_fetch(st, &hw));
+        ERQ_CUDA(cudaStreamSynchronize(st));
+        ERQ_TRY(tc_status_check(hw));
+    }
     return ERQ_OK;
 }
 

@@ -36,7 +36,7 @@ EXPORTED_SYMBOLS = (
     "erq_search_learned_raw",
     "erq_debug_probe_model_grads", "erq_debug_probe_model_params",
     "erq_plan_create", "erq_plan_free", "erq_plan_set_learned", "erq_plan_autotune",
-    "erq_plan_set_tuning", "erq_plan_get_tuning", "erq_plan_search", "erq_plan_device_bytes", "erq_plan_set_graphs",
+    "erq_plan_set_tuning", "erq_plan_get_tuning", "erq_plan_search", "erq_plan_device_bytes", "erq_plan_set_graphs", "erq_debug_gemm_bf16",
 )
 
 
@@ -128,6 +128,8 @@ def load_library(path: str | None = None) -> C.CDLL:
     lib.erq_plan_search.restype = C.c_int
     lib.erq_plan_device_bytes.argtypes = [vp]
     lib.erq_plan_device_bytes.restype = u64
+    lib.erq_debug_gemm_bf16.argtypes = [vp, vp, u64, u64, u64, vp, C.c_int]
+    lib.erq_debug_gemm_bf16.restype = C.c_int
     lib.erq_plan_set_graphs.argtypes = [vp, C.c_int]
     lib.erq_plan_set_graphs.restype = C.c_int
     lib.erq_profile_enable.argtypes = [C.c_int]

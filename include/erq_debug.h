@@ -53,6 +53,12 @@ ERQ_API erq_status erq_debug_probe_model_grads(const erq_probe_model* model, con
 ERQ_API erq_status erq_debug_probe_model_params(const erq_probe_model* model, float* params,
                                                 float* mean, float* stdv, uint32_t* bin_nprobe);
 
+/* C[M][N] = A[M][Kd] * B[N][Kd]^T on the tcgen05 GEMM of the search (BF16
+ * operands given as raw 16-bit patterns, FP32 result), host buffers; Kd a
+ * multiple of 64.  ERQ_ERR_TIMEOUT if one of its bounded waits ran out. */
+ERQ_API erq_status erq_debug_gemm_bf16(const uint16_t* A, const uint16_t* B, uint64_t M, uint64_t N,
+                                       uint64_t Kd, float* C, int device);
+
 /* Kernel timing.  While enabled, every kernel launch of the search and
  * rotation entry points is bracketed by CUDA events recorded on the stream
  * the kernel runs on.  erq_profile_read waits for the recorded events and
