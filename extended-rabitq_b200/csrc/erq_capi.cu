@@ -742,9 +742,7 @@ erq_status launch_probe_tc(const erq_index* idx, const Batch& b, uint64_t nprobe
     a.Kpow2 = next_pow2(K);
     a.D = D;
     a.nprobe = (int)nprobe;
-    // with features requested the 64 nearest distances are proven exact too
-    a.check_rank = near_d ? (int)std::max<uint64_t>(nprobe, std::min<uint64_t>(kFeatDists, K))
-                          : (int)nprobe;
+    a.check_rank = (int)nprobe;
     a.M = probe_candidates(a.check_rank);
     LaunchTimer t(kProbe, st);
     probe_kernel<<<(unsigned)b.nq, kProbeThreads, probe_smem_bytes(D, K, a.Kpow2), st>>>(a);

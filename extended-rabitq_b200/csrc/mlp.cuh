@@ -190,8 +190,8 @@ __global__ void mlp_dup_weights_kernel(const __nv_bfloat16* __restrict__ wb,
 
 // Raw features of one query: 256 sketch dims (the first rotated coordinates,
 // a random projection, scaled by 16/||q_r||) and 64 values of its nearest
-// centroid distances e_0 <= e_1 <= ...: log(e_0 / ||q_r||^2 + 1e-12) and
-// e_j / e_0 - 1 for j >= 1.
+// centroid distances e_0 <= e_1 <= ... (the tensor-core estimates, FP32
+// accurate): log(e_0 / ||q_r||^2 + 1e-12) and e_j / e_0 - 1 for j >= 1.
 __global__ void probe_features_kernel(const float* __restrict__ qrot, int D,
                                       const float* __restrict__ near_d, int nq,
                                       float* __restrict__ feats) {

@@ -31,12 +31,13 @@ struct ProbeArgs {
     float* probe_sqy;         // [nq][nprobe]
     uint64_t* s_off;          // [nq][nprobe]
     uint32_t* fallbacks;      // optional counter of queries that took step 4
-    float* near_d;            // optional [nq][64]: the 64 nearest exact distances
+    float* near_d;            // optional [nq][64]: the 64 smallest distance estimates, ascending
     int nq, K, Kpow2, D, nprobe, M;
     int check_rank;           // rank whose exactness the bound check proves (>= nprobe)
 };
 
 constexpr int kProbeThreads = 256;
+constexpr int kProbeFeatRank = 64;  // estimates written to near_d
 
 __device__ __forceinline__ uint32_t order_key(float f) {
     const uint32_t b = __float_as_uint(f);
@@ -101,12 +102,14 @@ __global__ void __launch_bounds__(kProbeThreads) probe_kernel(ProbeArgs a) {
     __syncthreads();
 
     const int M = a.M;
-    const bool select_all = M + 1 > K;
+    // with features requested the 64 smallest estimates are selected as well
+    const int Msel = a.near_d ? max(M, kProbeFeatRank) : M;
+    const bool select_all = Msel + 1 > K;
     uint32_t kstar = 0xffffffffu;
     if (!select_all) {
         // radix select of the (M+1)-th smallest key, 8 bits at a time
         uint32_t prefix = 0, pmask = 0;
-        int rank = M + 1;
+        int rank = Msel + 1;
         for (int shift = 24; shift >= 0; shift -= 8) {
             for (int i = tid; i < 256; i += blockDim.x) hist[i] = 0;
             __syncthreads();
@@ -155,11 +158,37 @@ __global__ void __launch_bounds__(kProbeThreads) probe_kernel(ProbeArgs a) {
     for (int c = tid; c < K; c += blockDim.x) {
         if (select_all || keys[c] < kstar) {
             const int slot = atomicAdd(&misc[2], 1);
-            sk[slot] = (uint64_t)c;  // id for now; exact distance filled below
+            // id (exact distance filled below), with its estimate key when
+            // the features need the estimates in order
+            sk[slot] = a.near_d ? (((uint64_t)keys[c] << 32) | (uint64_t)c) : (uint64_t)c;
         }
     }
     __syncthreads();
-    const int ns = misc[2];
+    int ns = misc[2];
+    uint32_t akey = kstar;        // estimate bound for the centroids not recomputed
+    bool truncated = !select_all;
+    if (a.near_d) {
+        // the 64 smallest estimates, in order, are the distance features; the
+        // first M of them are recomputed exactly and the (M+1)-th bounds the rest
+        int nsort0 = 1;
+        while (nsort0 < ns) nsort0 <<= 1;
+        for (int i = ns + tid; i < nsort0; i += blockDim.x) sk[i] = ~0ull;
+        __syncthreads();
+        block_bitonic_sort(sk, nsort0);
+        for (int j = tid; j < kProbeFeatRank; j += blockDim.x)
+            a.near_d[(size_t)q * kProbeFeatRank + j] =
+                ns > 0 ? order_key_value((uint32_t)(sk[j < ns ? j : ns - 1] >> 32)) : 0.f;
+        if (ns > M) {
+            akey = (uint32_t)(sk[M] >> 32);
+            ns = M;
+            truncated = true;
+        } else {
+            truncated = false;
+        }
+        __syncthreads();
+        for (int i = tid; i < ns; i += blockDim.x) sk[i] &= 0xffffffffull;
+        __syncthreads();
+    }
     // exact distances of the candidates, 16 per pass (one per half-warp)
     const int hw = tid >> 4, l = tid & 15, nhw = blockDim.x >> 4;
     for (int base = 0; base < ns; base += nhw) {
@@ -177,10 +206,10 @@ __global__ void __launch_bounds__(kProbeThreads) probe_kernel(ProbeArgs a) {
     // bound check
     if (tid == 0) {
         bool ok = ns >= a.check_rank;
-        if (ok && !select_all) {
+        if (ok && truncated) {
             const float e_n = __uint_as_float((uint32_t)(sk[a.check_rank - 1] >> 32));
             const float eps = a.eps_rel * (a.qn[q] + a.cn_max);
-            const float A = order_key_value(kstar);
+            const float A = order_key_value(akey);
             ok = (A - eps > e_n) && (e_n == e_n);
         }
         misc[3] = ok ? 1 : 0;
@@ -198,12 +227,6 @@ __global__ void __launch_bounds__(kProbeThreads) probe_kernel(ProbeArgs a) {
         for (int i = K + tid; i < a.Kpow2; i += blockDim.x) sk[i] = ~0ull;
         __syncthreads();
         block_bitonic_sort(sk, a.Kpow2);
-    }
-    if (a.near_d) {
-        const int avail = misc[3] ? ns : K;
-        for (int j = tid; j < 64; j += blockDim.x)
-            a.near_d[(size_t)q * 64 + j] =
-                __uint_as_float((uint32_t)(sk[j < avail ? j : avail - 1] >> 32));
     }
     // outputs + exclusive prefix of 32*nblocks over the probe order (warp 0)
     if (warp == 0) {

@@ -273,12 +273,13 @@ __device__ __forceinline__ void pool_merge_block(float* pool_d, uint32_t* pool_i
 // One block of 4 warps per query.  Per window of up to 16 blocks of the
 // current cluster: every warp computes the lower bounds of 4 blocks and lists
 // the lanes below the threshold as it stands at the window's start (a superset
-// of the exact candidates, because the threshold only falls); all 128 threads
-// refine the listed candidates, one each; warp 0 then replays the window in
-// the reference's order - each block's mask against the threshold at that
-// block's start, candidates in ascending lane order - inserting into the pool.
+// of the exact candidates, because the threshold only falls); the 32 quads
+// compute the listed candidates' exact distances (warps without a candidate
+// skip the round); warp 0 then replays the window in the reference's order -
+// each block's mask against the threshold at that block's start, the block's
+// candidates merged into the pool as inserting them in lane order would.
 template <int EX>
-__global__ void __launch_bounds__(kRefineThreads) refine_kernel(RefineArgs a) {
+__global__ void __launch_bounds__(kRefineThreads, 8) refine_kernel(RefineArgs a) {
     extern __shared__ __align__(16) uint8_t smem_raw[];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int q = a.order ? (int)a.order[blockIdx.x] : (int)blockIdx.x;
@@ -394,23 +395,32 @@ __global__ void __launch_bounds__(kRefineThreads) refine_kernel(RefineArgs a) {
                 __syncthreads();
             }
             // refine the listed candidates: quad g (lanes 4g..4g+3) takes two
-            // per round while at least 33 remain, else one; quads past the
-            // end repeat the list's first so every warp stays converged
+            // per round while at least 33 remain, else one; within a warp
+            // that has work, quads past the end repeat the list's first so
+            // the warp stays converged
             {
                 const int g = tid >> 2, r = tid & 3;
                 const float4* uq4 = reinterpret_cast<const float4*>(uq);
                 for (int base = 0; base < cnt;) {
                     const int two = cnt - base > kRefineThreads / 4;
+                    const int step = two ? kRefineThreads / 2 : kRefineThreads / 4;
+                    // per warp: skip when none of its slots holds a candidate,
+                    // one candidate per quad when its second slots are empty
+                    if (base + 8 * warp >= cnt) {
+                        base += step;
+                        continue;
+                    }
+                    const int wtwo = two && base + kRefineThreads / 4 + 8 * warp < cnt;
                     const int i0 = base + g, i1 = base + kRefineThreads / 4 + g;
                     const int s0 = w_list[i0 < cnt ? i0 : 0];
-                    const int s1 = w_list[two && i1 < cnt ? i1 : 0];
+                    const int s1 = w_list[wtwo && i1 < cnt ? i1 : 0];
                     const size_t pos0 = (size_t)first_vec + 32 * wb + s0;
                     const size_t pos1 = (size_t)first_vec + 32 * wb + s1;
                     const uint4* row0 = reinterpret_cast<const uint4*>(a.excode + pos0 * a.ex_row);
                     const uint4* row1 = reinterpret_cast<const uint4*>(a.excode + pos1 * a.ex_row);
                     // lane 0 of the quad finishes the first, lane 1 the second
                     const int i = r == 0 ? i0 : i1;
-                    const bool fin = r < 2 && (r == 0 || two) && i < cnt;
+                    const bool fin = r < 2 && (r == 0 || wtwo) && i < cnt;
                     const int slot = r == 0 ? s0 : s1;
                     const size_t pos = r == 0 ? pos0 : pos1;
                     float xipn = 0.f;
@@ -420,7 +430,7 @@ __global__ void __launch_bounds__(kRefineThreads) refine_kernel(RefineArgs a) {
                         vid = __ldg(a.ids + pos);
                     }
                     float ip[2];
-                    if (two)
+                    if (wtwo)
                         ex_ip_quad<ex_storage_bits(EX), 2>(uq4, row0, row1, r, D / 16, ip);
                     else
                         ex_ip_quad<ex_storage_bits(EX), 1>(uq4, row0, row0, r, D / 16, ip);
@@ -435,7 +445,7 @@ __global__ void __launch_bounds__(kRefineThreads) refine_kernel(RefineArgs a) {
                         w_ed[slot] = __double2float_rn(__dsub_rn((double)f, __dmul_rn((double)xy, br)));
                         w_id[slot] = vid;
                     }
-                    base += two ? kRefineThreads / 2 : kRefineThreads / 4;
+                    base += step;
                 }
             }
             __syncthreads();

@@ -118,3 +118,23 @@ def test_learned_search_equals_plain_at_chosen_depth_and_saves_probes(learned_ca
           f"{used.mean():.2f}, recall {r_learned:.4f}")
     assert r_learned >= rec[fixed] - 0.01
     assert used.mean() < fixed
+
+
+@pytest.mark.gpu
+def test_distance_features_follow_exact_centroid_distances(learned_case):
+    """The 64 distance features come from the tensor-core estimates; they must
+    agree with the same features computed from the exact distances."""
+    from erq_b200.learned import probe_features
+
+    ivf, rot_train, _, _ = learned_case
+    q = rot_train[:200]
+    f = probe_features(ivf, q)
+    exact = np.sort(ivf.debug_centroid_dists(q).astype(np.float64), axis=1)[:, :64]
+    qn = (q.astype(np.float64) ** 2).sum(1)
+    ref = np.concatenate([np.log(exact[:, :1] / qn[:, None] + 1e-12),
+                          exact[:, 1:] / exact[:, :1] - 1.0], axis=1)
+    assert np.abs(f[:, 256:] - ref).max() < 1e-3
+    sketch = np.zeros((q.shape[0], 256))
+    d = min(256, q.shape[1])  # dims beyond D read as 0
+    sketch[:, :d] = q[:, :d] * (16.0 / np.sqrt(qn))[:, None]
+    assert np.abs(f[:, :256] - sketch).max() < 1e-4
