@@ -363,6 +363,12 @@ def run_ours(args, cfg, name):
     if args.nprobe:
         cfg = dict(cfg, nprobe=args.nprobe)
     nprobe, recall, ids0 = choose_nprobe(idx, query, gt, cfg)
+    from erq_b200 import _lib as L
+
+    L.probe_fallbacks(local, reset=True)
+    idx.search_raw(query, k, nprobe, with_dists=False)
+    fallback_rate = L.probe_fallbacks(local, reset=True) / nq
+    log(f"probe fallback rate {fallback_rate:.5f}")
     base = np.load(os.path.join(d, "base.npy"), mmap_mode="r")
     sub = min(1000, nq)
     arr = indexfile.read_index(index_path)
@@ -454,6 +460,10 @@ def run_ours(args, cfg, name):
         if best is not None:
             conf, r_l, ids_l, used = best
             plan_l.set_learned(conf)
+            L.probe_fallbacks(local, reset=True)
+            plan_l.search(query, with_dists=False)
+            learned_fallback_rate = L.probe_fallbacks(local, reset=True) / nq
+            log(f"learned probe fallback rate {learned_fallback_rate:.5f}")
             tune_l, _ = plan_l.autotune(query, reps=2)
             ms_l, e2e_l, clocks_l, prof_l = plan_mode(plan_l, ids_l)
             take = np.arange(cids.shape[1])[None, :] < used.astype(np.int64)[:, None]
@@ -462,6 +472,9 @@ def run_ours(args, cfg, name):
                             "confidence": conf, "mean_nprobe": round(float(used.mean()), 4),
                             "recall@100": round(r_l, 5),
                             "ms_per_step": round(ms_l / args.steps, 4), "tuning": tune_l,
+                            "probe_fallback_rate": round(learned_fallback_rate, 5),
+                            "kernels_ms_per_step": {kk: round(v[1] / args.steps, 4)
+                                                    for kk, v in prof_l.items() if v[0]},
                             "model": meta}
             if e2e_l is not None:
                 learned_info["e2e"] = round(world * nq * args.steps / (e2e_l / 1e3), 1)
@@ -515,6 +528,7 @@ def run_ours(args, cfg, name):
                                    f"{cfg['bits']}-bit, {nq} queries per step, top-{k}",
                        "mode": mode, "nprobe": nprobe, "recall@100": round(chosen["recall"], 5),
                        "distance_ratio": round(ratio, 5), "queries_per_step": nq,
+                       "probe_fallback_rate": round(fallback_rate, 5),
                        "parallelism": f"replicas x{world} (queries replicated per GPU)",
                        "l2": "inputs larger than L2: every step streams "
                              f"{chosen['scan_bytes'] / 1e9:.1f} GB of packed codes from a "

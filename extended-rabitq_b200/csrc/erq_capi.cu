@@ -700,9 +700,27 @@ bool launch_order(const erq_index* idx, const Batch& b, uint64_t nprobe, cudaStr
     return true;
 }
 
-// Candidate count for the probe: nprobe plus a margin (probe.cuh).
+// Candidate count for the probe: nprobe plus a margin (probe.cuh).  When the
+// margin does not prove the cut the kernel computes all K exact distances
+// (counted in g_probe_fallbacks).
 int probe_candidates(uint64_t nprobe) {
     return (int)(nprobe + std::max<uint64_t>(32, nprobe / 2));
+}
+
+// Queries whose probe fell back to all K exact distances, per device image.
+__device__ uint32_t g_probe_fallbacks;
+uint32_t* probe_fallback_counter() {
+    static uint32_t* ptrs[kMaxDevices] = {};
+    static std::mutex mu;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return nullptr;
+    std::lock_guard<std::mutex> g(mu);
+    if (!ptrs[dev]) {
+        void* p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_probe_fallbacks) != cudaSuccess) return nullptr;
+        ptrs[dev] = static_cast<uint32_t*>(p);
+    }
+    return ptrs[dev];
 }
 
 // Coarse probe on tensor cores: split the rotated queries, estimate all
@@ -735,7 +753,7 @@ erq_status launch_probe_tc(const erq_index* idx, const Batch& b, uint64_t nprobe
     a.probe_cid = b.probe_cid;
     a.probe_sqy = b.probe_sqy;
     a.s_off = b.s_off;
-    a.fallbacks = nullptr;
+    a.fallbacks = probe_fallback_counter();
     a.near_d = near_d;
     a.nq = (int)b.nq;
     a.K = K;
@@ -1930,6 +1948,19 @@ erq_status erq_debug_gemm_bf16(const uint16_t* A, const uint16_t* B, uint64_t M,
     ERQ_CUDA(cudaMemcpy(&st, status, 4, cudaMemcpyDeviceToHost));
     if (st) return fail(ERQ_ERR_TIMEOUT, "a wait in the tcgen05 GEMM reached its limit");
     ERQ_CUDA(cudaMemcpy(C, c, M * N * 4, cudaMemcpyDeviceToHost));
+    return ERQ_OK;
+}
+
+erq_status erq_debug_probe_fallbacks(int device, uint64_t* count, int reset) {
+    if (!count) return fail(ERQ_ERR_INVALID_ARGUMENT, "count is NULL");
+    DeviceGuard guard;
+    ERQ_TRY(guard.set(device));
+    uint32_t* c = probe_fallback_counter();
+    if (!c) return fail(ERQ_ERR_CUDA, "fallback counter unavailable");
+    uint32_t v = 0;
+    ERQ_CUDA(cudaMemcpy(&v, c, sizeof(v), cudaMemcpyDeviceToHost));
+    *count = v;
+    if (reset) ERQ_CUDA(cudaMemset(c, 0, sizeof(uint32_t)));
     return ERQ_OK;
 }
 

@@ -36,7 +36,7 @@ EXPORTED_SYMBOLS = (
     "erq_search_learned_raw",
     "erq_debug_probe_model_grads", "erq_debug_probe_model_params",
     "erq_plan_create", "erq_plan_free", "erq_plan_set_learned", "erq_plan_autotune",
-    "erq_plan_set_tuning", "erq_plan_get_tuning", "erq_plan_search", "erq_plan_device_bytes", "erq_plan_set_graphs", "erq_debug_gemm_bf16",
+    "erq_plan_set_tuning", "erq_plan_get_tuning", "erq_plan_search", "erq_plan_device_bytes", "erq_plan_set_graphs", "erq_debug_gemm_bf16", "erq_debug_probe_fallbacks",
 )
 
 
@@ -130,6 +130,8 @@ def load_library(path: str | None = None) -> C.CDLL:
     lib.erq_plan_device_bytes.restype = u64
     lib.erq_debug_gemm_bf16.argtypes = [vp, vp, u64, u64, u64, vp, C.c_int]
     lib.erq_debug_gemm_bf16.restype = C.c_int
+    lib.erq_debug_probe_fallbacks.argtypes = [C.c_int, C.POINTER(C.c_uint64), C.c_int]
+    lib.erq_debug_probe_fallbacks.restype = C.c_int
     lib.erq_plan_set_graphs.argtypes = [vp, C.c_int]
     lib.erq_plan_set_graphs.restype = C.c_int
     lib.erq_profile_enable.argtypes = [C.c_int]
@@ -179,6 +181,13 @@ def profile_enable(on: bool = True) -> None:
 
 def profile_reset() -> None:
     load_library().erq_profile_reset()
+
+
+def probe_fallbacks(device: int = 0, reset: bool = True) -> int:
+    """Queries whose probe fell back to all K exact distances since the last reset."""
+    n = C.c_uint64()
+    check(load_library().erq_debug_probe_fallbacks(device, C.byref(n), 1 if reset else 0))
+    return int(n.value)
 
 
 def profile_read() -> dict:

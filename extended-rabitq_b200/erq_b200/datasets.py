@@ -155,13 +155,18 @@ def gaussian_mixture_torch(n: int, d: int, n_comp: int, sigma: float, seed: int,
 def kmeans_torch(x, k: int, iters: int = 20, seed: int = 0):
     """Lloyd's k-means on the GPU (TF32 distance products, float32 updates).
     Returns (centroids [k, d] float32, ids [n] int64) with ids the nearest
-    final centroid."""
+    final centroid.  Deterministic algorithms are on while it runs (the
+    centroid sums otherwise depend on the order of float atomics), so the same
+    seed gives the same clusters on every run."""
     import torch
 
     g = torch.Generator(device=x.device).manual_seed(seed)
     c = x[torch.randperm(x.shape[0], generator=g, device=x.device)[:k]].clone()
     prev = torch.backends.cuda.matmul.allow_tf32
+    prev_det = torch.are_deterministic_algorithms_enabled()
+    prev_warn = torch.is_deterministic_algorithms_warn_only_enabled()
     torch.backends.cuda.matmul.allow_tf32 = True
+    torch.use_deterministic_algorithms(True, warn_only=True)
     try:
         def assign(cent):
             cc = (cent * cent).sum(1)
@@ -183,6 +188,7 @@ def kmeans_torch(x, k: int, iters: int = 20, seed: int = 0):
         a = assign(c)
     finally:
         torch.backends.cuda.matmul.allow_tf32 = prev
+        torch.use_deterministic_algorithms(prev_det, warn_only=prev_warn)
     return c, a
 
 

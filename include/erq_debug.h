@@ -59,6 +59,11 @@ ERQ_API erq_status erq_debug_probe_model_params(const erq_probe_model* model, fl
 ERQ_API erq_status erq_debug_gemm_bf16(const uint16_t* A, const uint16_t* B, uint64_t M, uint64_t N,
                                        uint64_t Kd, float* C, int device);
 
+/* Queries whose coarse probe could not prove its cut from the tensor-core
+ * estimates and computed all K exact distances instead, since the last reset
+ * (process-wide, per device). */
+ERQ_API erq_status erq_debug_probe_fallbacks(int device, uint64_t* count, int reset);
+
 /* Kernel timing.  While enabled, every kernel launch of the search and
  * rotation entry points is bracketed by CUDA events recorded on the stream
  * the kernel runs on.  erq_profile_read waits for the recorded events and

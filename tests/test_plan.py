@@ -165,3 +165,15 @@ def test_learned_plan_equals_learned_search(uneven):
         assert (bits(d) == bits(d_l)).all()
     plan.free()
     model.free()
+
+
+def test_probe_rarely_falls_back(uneven):
+    """The coarse probe proves its cut from the estimates with a small margin;
+    falling back to all K exact distances must stay rare (a speed property:
+    results are exact either way)."""
+    from erq_b200 import _lib as L
+
+    idx, q, qr, _ = uneven
+    L.probe_fallbacks(0, reset=True)
+    idx.search_batch(qr, 100, 6, with_dists=False)
+    assert L.probe_fallbacks(0, reset=True) <= 0.02 * len(qr)
