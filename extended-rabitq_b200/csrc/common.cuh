@@ -50,4 +50,32 @@ __host__ __device__ __forceinline__ uint64_t div_up(uint64_t a, uint64_t b) {
     return (a + b - 1) / b;
 }
 
+// Lower bound of one vector's distance (accumulate_one_block_high_acc,
+// inc/index/fastscan/FastScan.hpp:295-323): constants of the (query, cluster)
+// pair, then lb = ((ipq - c1) * c2 * onorm + c3) + onorm^2 in that order.
+struct LbConsts {
+    float c1, c2, c3;
+};
+__device__ __forceinline__ LbConsts lb_consts(float sumq, float y, float one_over_sqrtD) {
+    LbConsts k;
+    k.c1 = __double2float_rn(__dsub_rn(__dmul_rn(0.5, (double)sumq), (double)kConstBound));
+    k.c2 = __fmul_rn(__fmul_rn(-5.f, y), one_over_sqrtD);
+    k.c3 = __fmul_rn(y, y);
+    return k;
+}
+__device__ __forceinline__ float lower_bound(float ipq, float on, const LbConsts& k) {
+    float t = __fsub_rn(ipq, k.c1);
+    t = __fmul_rn(t, k.c2);
+    t = __fmul_rn(t, on);
+    t = __fadd_rn(t, k.c3);
+    return __fadd_rn(t, __fmul_rn(on, on));
+}
+// Smallest lower bound of a 32-vector block over a warp (lane = vector;
+// invalid lanes pass +inf); valid in every lane.
+__device__ __forceinline__ float warp_min(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
 }  // namespace erq

@@ -605,12 +605,14 @@ struct Batch {
     uint32_t* buckets_q = nullptr;    // [K + 1] query sort
     uint32_t* order_pairs = nullptr;  // [nq * nprobe]
     uint32_t* order_q = nullptr;      // [nq]
+    float* bmin = nullptr;            // smallest lower bound per scanned block (S / 32 entries)
 };
 
 // Largest query batch whose scan workspace fits the budget.
 uint64_t batch_queries(const erq_index* idx, uint64_t nprobe, uint64_t nq) {
     const uint64_t per_q = 32ull * idx->top_blocks[nprobe] * sizeof(int32_t) +
-                           idx->K * sizeof(float) + nprobe * 24 + 6 * idx->D + 4;
+                           idx->K * sizeof(float) + nprobe * 24 + 6 * idx->D + 4 +
+                           idx->top_blocks[nprobe] * sizeof(float);
     const uint64_t budget = 3ull << 30;
     uint64_t b = std::max<uint64_t>(1, budget / std::max<uint64_t>(per_q, 1));
     return std::min(b, nq);
@@ -633,6 +635,7 @@ erq_status alloc_batch(Alloc& s, const erq_index* idx, uint64_t nq, uint64_t npr
     ERQ_TRY(s.alloc(&b.buckets_q, idx->K + 1));
     ERQ_TRY(s.alloc(&b.order_pairs, nq * nprobe));
     ERQ_TRY(s.alloc(&b.order_q, nq));
+    ERQ_TRY(s.alloc(&b.bmin, nq * idx->top_blocks[nprobe]));
     return ERQ_OK;
 }
 
@@ -792,6 +795,9 @@ erq_status launch_scan(const erq_index* idx, const Batch& b, uint64_t nprobe, cu
                        const int* q_nprobe = nullptr, const uint32_t* order = nullptr) {
     ScanArgs a;
     a.order = order;
+    a.onorm = idx->onorm;
+    a.c_size = idx->c_size;
+    a.bmin = b.bmin;
     a.qrot = b.qrot;
     a.centroids = idx->centroids;
     a.probe_cid = b.probe_cid;
@@ -820,6 +826,7 @@ erq_status launch_refine(const erq_index* idx, const Batch& b, uint64_t nprobe, 
                          const int* q_nprobe = nullptr, const uint32_t* order = nullptr) {
     RefineArgs a;
     a.order = order;
+    a.bmin = b.bmin;
     a.qrot = b.qrot;
     a.centroids = idx->centroids;
     a.probe_cid = b.probe_cid;
@@ -2149,6 +2156,9 @@ erq_status launch_scan_batched(erq_plan* p, uint64_t nq, const erq_plan_tuning& 
     a.S = p->b.S;
     a.qp_delta = p->b.delta;
     a.qp_sumq = p->b.sumq;
+    a.onorm = idx->onorm;
+    a.c_size = idx->c_size;
+    a.bmin = p->b.bmin;
     a.order_pairs = p->b.order_pairs;
     a.bucket_end = p->b.buckets;
     a.item_off = p->item_off;

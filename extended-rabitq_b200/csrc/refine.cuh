@@ -44,6 +44,8 @@ struct RefineArgs {
     float* out_dists;             // [nq][k] or null
     const int* q_nprobe;          // optional [nq]: clusters probed by each query
     const uint32_t* order;        // optional: block i refines query order[i]
+    const float* bmin;            // optional: smallest lower bound per scanned block, at
+                                  // s_off/32 + block (blocks above the threshold are skipped)
     int nq, D, EX, nprobe, k;
 };
 
@@ -153,7 +155,8 @@ constexpr int kWindowLanes = kWindowBlocks * 32;
 // Shared memory of one block: unit_q[D] | per window lane: lb, ipq, onorm,
 // ex_dist, id, list | pool_d[kpad] | pool_id[kpad] | misc
 __host__ __device__ constexpr size_t refine_smem_bytes_per_query(int D, int kpad) {
-    return (size_t)D * 4 + (size_t)kWindowLanes * (5 * 4 + 2) + (size_t)kpad * 8 + 64 + 128;
+    return (size_t)D * 4 + (size_t)kWindowLanes * (5 * 4 + 2) + (size_t)kpad * 8 + 64 + 128 +
+           kWindowBlocks * 4;
 }
 
 // Order key: ascending distance (-0 equal to +0, as float compares see it);
@@ -297,6 +300,7 @@ __global__ void __launch_bounds__(kRefineThreads, 8) refine_kernel(RefineArgs a)
     int* misc = reinterpret_cast<int*>(pool_id + kpad);  // [0] list count [1] pool size
     float* s_distk = reinterpret_cast<float*>(misc + 2);
     float* cs = reinterpret_cast<float*>(misc + 16);  // 32 floats of merge scratch
+    uint32_t* w_blk = reinterpret_cast<uint32_t*>(cs + 32);  // the window's blocks
     const int fac_rescale = 1 << EX;
     const float one_over_sqrtD = recip_via_double(__fsqrt_rn((float)D));
     const float* qv = a.qrot + (size_t)q * D;
@@ -322,14 +326,13 @@ __global__ void __launch_bounds__(kRefineThreads, 8) refine_kernel(RefineArgs a)
         const float delta = a.qp_delta[qp];
         const float sumq = a.qp_sumq[qp];
         // lower-bound constants (inc/index/fastscan/FastScan.hpp:297-303)
-        const float c1 = __double2float_rn(__dsub_rn(__dmul_rn(0.5, (double)sumq), (double)kConstBound));
-        const float c2 = __fmul_rn(__fmul_rn(-5.f, y), one_over_sqrtD);
-        const float c3 = __fmul_rn(y, y);
+        const LbConsts lbk = lb_consts(sumq, y, one_over_sqrtD);
         const double ex_sub = __dmul_rn((double)fac_rescale - 0.5, (double)sumq);
         const uint32_t n = a.c_size[cid];
         const uint32_t fb = a.c_first_block[cid];
         const uint32_t first_vec = a.c_first_vec[cid];
         const int32_t* S = a.S + a.s_off[qp];
+        const float* bmin = a.bmin ? a.bmin + a.s_off[qp] / 32 : nullptr;
         const uint32_t nblocks = (n + 31) >> 5;
         bool uq_ready = false;
         for (uint32_t wb = 0; wb < nblocks;) {
@@ -339,23 +342,48 @@ __global__ void __launch_bounds__(kRefineThreads, 8) refine_kernel(RefineArgs a)
             // enough blocks to fill it, so few lanes are refined in vain.
             const int want = filled < k ? min(kWindowBlocks, max(1, (k - filled + 31) / 32))
                                         : kWindowBlocks;
-            const int nbw = (int)min((uint32_t)want, nblocks - wb);
             __syncthreads();
-            if (tid == 0) misc[0] = 0;
+            // warp 0 picks the window: the next `want` blocks from wb whose
+            // smallest lower bound is below the threshold (a block above it
+            // has no candidate now or later: the threshold only falls)
+            if (warp == 0) {
+                int got = 0;
+                uint32_t pos = wb, next = nblocks;
+                while (got < want && pos < nblocks) {
+                    const uint32_t bb = pos + lane;
+                    const bool take = bb < nblocks && (!bmin || bmin[bb] < d0);
+                    const uint32_t m = __ballot_sync(0xffffffffu, take);
+                    const int rank = __popc(m & ((1u << lane) - 1u));
+                    if (take && got + rank < want) w_blk[got + rank] = bb;
+                    const int nm = __popc(m);
+                    if (got + nm >= want) {
+                        // the want-th taken block ends the window
+                        const uint32_t endm = __ballot_sync(0xffffffffu, take && rank == want - got - 1);
+                        next = pos + (uint32_t)(__ffs(endm) - 1) + 1;
+                        got = want;
+                        break;
+                    }
+                    got += nm;
+                    pos += 32;
+                }
+                if (lane == 0) {
+                    misc[0] = 0;
+                    misc[5] = got;
+                    misc[6] = (int)next;
+                }
+            }
             __syncthreads();
+            const int nbw = misc[5];
+            const uint32_t wnext = (uint32_t)misc[6];
             // lower bounds and the candidate superset, 4 blocks per warp
 #pragma unroll
             for (int i = 0; i < kWindowBlocks / (kRefineThreads / 32); ++i) {
                 const int b = warp * (kWindowBlocks / (kRefineThreads / 32)) + i;
                 if (b < nbw) {  // uniform per warp
-                    const uint32_t blk = wb + b;
+                    const uint32_t blk = w_blk[b];
                     const float ipq = __fmul_rn(__int2float_rn(S[32 * blk + lane]), delta);
                     const float on = a.onorm[(size_t)(fb + blk) * 32 + lane];
-                    float t = __fsub_rn(ipq, c1);
-                    t = __fmul_rn(t, c2);
-                    t = __fmul_rn(t, on);
-                    t = __fadd_rn(t, c3);
-                    t = __fadd_rn(t, __fmul_rn(on, on));
+                    const float t = lower_bound(ipq, on, lbk);
                     const bool valid = 32 * blk + lane < n;
                     // padding lanes never pass (NaN compares false)
                     w_lb[32 * b + lane] = valid ? t : __int_as_float(0x7fc00000);
@@ -379,7 +407,7 @@ __global__ void __launch_bounds__(kRefineThreads, 8) refine_kernel(RefineArgs a)
             __syncthreads();
             const int cnt = misc[0];
             if (cnt == 0) {  // uniform: nothing in this window can pass
-                wb += nbw;
+                wb = wnext;
                 continue;
             }
             if (!uq_ready) {
@@ -414,8 +442,8 @@ __global__ void __launch_bounds__(kRefineThreads, 8) refine_kernel(RefineArgs a)
                     const int i0 = base + g, i1 = base + kRefineThreads / 4 + g;
                     const int s0 = w_list[i0 < cnt ? i0 : 0];
                     const int s1 = w_list[wtwo && i1 < cnt ? i1 : 0];
-                    const size_t pos0 = (size_t)first_vec + 32 * wb + s0;
-                    const size_t pos1 = (size_t)first_vec + 32 * wb + s1;
+                    const size_t pos0 = (size_t)first_vec + 32 * w_blk[s0 >> 5] + (s0 & 31);
+                    const size_t pos1 = (size_t)first_vec + 32 * w_blk[s1 >> 5] + (s1 & 31);
                     const uint4* row0 = reinterpret_cast<const uint4*>(a.excode + pos0 * a.ex_row);
                     const uint4* row1 = reinterpret_cast<const uint4*>(a.excode + pos1 * a.ex_row);
                     // lane 0 of the quad finishes the first, lane 1 the second
@@ -465,7 +493,7 @@ __global__ void __launch_bounds__(kRefineThreads, 8) refine_kernel(RefineArgs a)
                 }
             }
             __syncthreads();
-            wb += nbw;
+            wb = wnext;
         }
     }
     if (warp == 0) {

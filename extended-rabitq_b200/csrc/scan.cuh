@@ -42,6 +42,10 @@ struct ScanArgs {
     float* qp_sumq;           // [nq][nprobe]
     const int* q_nprobe;      // optional [nq]: probe only the first q_nprobe[q] clusters
     const uint32_t* order;    // optional: block i scans pair order[i]
+    const float* onorm;       // [blocks*32] (for the block minima)
+    const uint32_t* c_size;   // [K]
+    float* bmin;              // optional: smallest lower bound of each scanned block,
+                              // at s_off/32 + block
     int D;
     int nprobe;
 };
@@ -137,8 +141,10 @@ __global__ void __launch_bounds__(kScanWarps * 32) scan_kernel(ScanArgs a) {
             for (int i = lane; i < D; i += 16) acc = __fadd_rn(acc, unit_q[i]);
         const float s = tree16_sum(acc);
         if (lane == 0) {
-            a.qp_sumq[pair] = normal ? s : __fmul_rn((float)D, fill);
+            const float sq = normal ? s : __fmul_rn((float)D, fill);
+            a.qp_sumq[pair] = sq;
             a.qp_delta[pair] = delta;
+            red[kScanWarps + 1] = sq;  // for the block minima, read after the barrier below
         }
     }
 
@@ -176,6 +182,9 @@ __global__ void __launch_bounds__(kScanWarps * 32) scan_kernel(ScanArgs a) {
     const uint32_t kconst = 0xC0804000u | (h ? 0x20202020u : 0u);
     // vector of this lane's output: perm0[j] for h = 0, perm0[j] + 16 for h = 1
     const uint32_t vout = ((j & 1) ? (j >> 1) + 8 : (j >> 1)) + 16 * h;
+    const LbConsts lbk = lb_consts(red[kScanWarps + 1], y, recip_via_double(__fsqrt_rn((float)D)));
+    const uint32_t csize = a.c_size[cid];
+    const uint32_t fblock = a.c_first_block[cid];
     for (uint32_t b = warp; b < nb; b += kScanWarps) {
         const uint2* src = reinterpret_cast<const uint2*>(cl_codes + (size_t)b * (4 * D)) + lane;
         int acc_lo = 0, acc_hi = 0;
@@ -193,7 +202,14 @@ __global__ void __launch_bounds__(kScanWarps * 32) scan_kernel(ScanArgs a) {
         // combine the two half-warps (even / odd group halves)
         acc_lo += __shfl_xor_sync(0xffffffffu, acc_lo, 16);
         acc_hi += __shfl_xor_sync(0xffffffffu, acc_hi, 16);
-        out[32 * b + vout] = h ? acc_hi : acc_lo;
+        const int sv = h ? acc_hi : acc_lo;
+        out[32 * b + vout] = sv;
+        if (a.bmin) {
+            const float on = a.onorm[(size_t)(fblock + b) * 32 + vout];
+            const float lb = lower_bound(__fmul_rn(__int2float_rn(sv), delta), on, lbk);
+            const float m = warp_min(32 * b + vout < csize ? lb : INFINITY);
+            if (lane == 0) a.bmin[a.s_off[pair] / 32 + b] = m;
+        }
     }
 }
 

@@ -36,6 +36,9 @@ struct ScanBatchArgs {
     int32_t* S;
     float* qp_delta;
     float* qp_sumq;
+    const float* onorm;            // [blocks*32] (for the block minima)
+    const uint32_t* c_size;        // [K]
+    float* bmin;                   // optional: smallest lower bound per scanned block
     const uint32_t* order_pairs;   // pairs sorted by cluster
     const uint32_t* bucket_end;    // [K + 1]: end of cluster c's run in order_pairs
     const uint32_t* item_off;      // [K + 1]: first item of cluster c; [K] = item count
@@ -89,9 +92,10 @@ __device__ __forceinline__ void lookup4_q(uint32_t lo2, uint32_t hi2, uint32_t b
     }
 }
 
-// Shared memory: [pad to 256][QB tables of kQStride][unit_q D floats][red]
+// Shared memory: [pad to 256][QB tables of kQStride][unit_q D floats]
+// [red 32 floats][item fields 4][per-query delta and lower-bound constants]
 __host__ __device__ constexpr size_t scan_batch_smem_bytes(int QB, int D) {
-    return 256 + (size_t)QB * kQStride + (size_t)D * 4 + 64 * 4;
+    return 256 + (size_t)QB * kQStride + (size_t)D * 4 + 128 * 4;
 }
 
 template <int QB, int WARPS>
@@ -108,6 +112,8 @@ __global__ void __launch_bounds__(WARPS * 32) scan_batched_kernel(ScanBatchArgs 
     float* unit_q = reinterpret_cast<float*>(tables + QB * kQStride);
     float* red = unit_q + D;                                    // [WARPS] maxima
     uint32_t* info = reinterpret_cast<uint32_t*>(red + 32);     // item fields
+    float* jk = reinterpret_cast<float*>(info + 4);             // [QB][4]: delta, c1, c2, c3
+    const float one_over_sqrtD = recip_via_double(__fsqrt_rn((float)D));
     const float fill = recip_via_double(__fsqrt_rn((float)D));
     const uint32_t h = lane >> 4, j16 = lane & 15;
     const uint32_t kconst = 0xC0804000u | (h ? 0x20202020u : 0u);
@@ -182,14 +188,22 @@ __global__ void __launch_bounds__(WARPS * 32) scan_batched_kernel(ScanBatchArgs 
 #pragma unroll
             for (int w = 1; w < WARPS; ++w) vmax = fmaxf(vmax, red[w]);
             const float delta = __fdiv_rn(vmax, 8191.f);
-            if (warp == 0 && chunk == 0) {
+            if (warp == 0) {
                 float acc = 0.f;
                 if (lane < 16)
                     for (int i = lane; i < D; i += 16) acc = __fadd_rn(acc, unit_q[i]);
                 const float s = tree16_sum(acc);
                 if (lane == 0) {
-                    a.qp_sumq[pair] = normal ? s : __fmul_rn((float)D, fill);
-                    a.qp_delta[pair] = delta;
+                    const float sq = normal ? s : __fmul_rn((float)D, fill);
+                    if (chunk == 0) {
+                        a.qp_sumq[pair] = sq;
+                        a.qp_delta[pair] = delta;
+                    }
+                    const LbConsts k = lb_consts(sq, y, one_over_sqrtD);
+                    jk[4 * j + 0] = delta;
+                    jk[4 * j + 1] = k.c1;
+                    jk[4 * j + 2] = k.c2;
+                    jk[4 * j + 3] = k.c3;
                 }
             }
             uint8_t* tj = tables + j * kQStride;
@@ -236,12 +250,24 @@ __global__ void __launch_bounds__(WARPS * 32) scan_batched_kernel(ScanBatchArgs 
                 const uint32_t hi1 = ((w.y >> 3) & 0x1E1E1E1Eu) | kconst;
                 lookup4_q<QB, true>(lo1, hi1, base, qn, acc_lo, acc_hi);
             }
+            const float on = a.bmin ? a.onorm[(size_t)(a.c_first_block[c] + b) * 32 + vout] : 0.f;
+            const bool valid = 32 * b + vout < a.c_size[c];
 #pragma unroll
             for (int j = 0; j < QB; ++j) {
                 if (j < qn) {
                     int lo = acc_lo[j] + __shfl_xor_sync(0xffffffffu, acc_lo[j], 16);
                     int hi = acc_hi[j] + __shfl_xor_sync(0xffffffffu, acc_hi[j], 16);
-                    a.S[a.s_off[pairs[j]] + 32 * b + vout] = h ? hi : lo;
+                    const int sv = h ? hi : lo;
+                    a.S[a.s_off[pairs[j]] + 32 * b + vout] = sv;
+                    if (a.bmin) {
+                        LbConsts k;
+                        k.c1 = jk[4 * j + 1];
+                        k.c2 = jk[4 * j + 2];
+                        k.c3 = jk[4 * j + 3];
+                        const float lb = lower_bound(__fmul_rn(__int2float_rn(sv), jk[4 * j]), on, k);
+                        const float m = warp_min(valid ? lb : INFINITY);
+                        if (lane == 0) a.bmin[a.s_off[pairs[j]] / 32 + b] = m;
+                    }
                 }
             }
         }
