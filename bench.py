@@ -448,7 +448,10 @@ def run_ours(args, cfg, name):
         model, meta = learned_model(idx, d, cfg, nprobe)
         plan_l = Plan(idx, max_batch=nq, k=k, nprobe=nprobe, model=model, raw=True)
         best = None
-        for conf in (0.5, 0.6, 0.7, 0.8, 0.9, 0.95, 0.99):
+        # lowest confidence first: the first that meets the recall target
+        # probes the fewest clusters
+        for conf in (0.005, 0.01, 0.02, 0.05, 0.1, 0.2, 0.3, 0.4, 0.5, 0.6, 0.7, 0.8, 0.9,
+                     0.95, 0.99):
             plan_l.set_learned(conf)
             ids_l, _, used = plan_l.search(query, with_dists=False, with_nprobe=True)
             r = metrics.recall_at_k(ids_l, gt, k)
