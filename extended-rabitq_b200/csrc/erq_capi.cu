@@ -458,7 +458,9 @@ erq_status configure_kernels(int D, int K, int k) {
     ERQ_CUDA(cudaFuncSetAttribute(scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)scan_smem_bytes(D)));
     ERQ_CUDA(cudaFuncSetAttribute(probe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)probe_smem_bytes(D, K, kp2)));
+                                  (int)probe_smem_bytes(D, kp2)));
+    ERQ_CUDA(cudaFuncSetAttribute(probe_fallback_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)probe_fallback_smem_bytes(D, kp2)));
     const int rs = (int)refine_smem_bytes(D, k);
     ERQ_CUDA(cudaFuncSetAttribute(refine_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, rs));
     ERQ_CUDA(cudaFuncSetAttribute(refine_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, rs));
@@ -606,6 +608,7 @@ struct Batch {
     uint32_t* order_pairs = nullptr;  // [nq * nprobe]
     uint32_t* order_q = nullptr;      // [nq]
     float* bmin = nullptr;            // smallest lower bound per scanned block (S / 32 entries)
+    uint32_t* fb_flag = nullptr;      // [nq] queries whose probe needs all K exact distances
 };
 
 // Largest query batch whose scan workspace fits the budget.
@@ -636,6 +639,7 @@ erq_status alloc_batch(Alloc& s, const erq_index* idx, uint64_t nq, uint64_t npr
     ERQ_TRY(s.alloc(&b.order_pairs, nq * nprobe));
     ERQ_TRY(s.alloc(&b.order_q, nq));
     ERQ_TRY(s.alloc(&b.bmin, nq * idx->top_blocks[nprobe]));
+    ERQ_TRY(s.alloc(&b.fb_flag, nq));
     return ERQ_OK;
 }
 
@@ -765,10 +769,24 @@ erq_status launch_probe_tc(const erq_index* idx, const Batch& b, uint64_t nprobe
     a.nprobe = (int)nprobe;
     a.check_rank = (int)nprobe;
     a.M = probe_candidates(a.check_rank);
-    LaunchTimer t(kProbe, st);
-    probe_kernel<<<(unsigned)b.nq, kProbeThreads, probe_smem_bytes(D, K, a.Kpow2), st>>>(a);
-    t.finish();
-    ERQ_CUDA(cudaGetLastError());
+    {
+        const int msel = near_d ? std::max(a.M, kProbeFeatRank) : a.M;
+        a.Spow2 = next_pow2(msel + 1 > K ? K : msel);
+    }
+    if (!b.fb_flag) return fail(ERQ_ERR_INVALID_ARGUMENT, "probe batch without fallback flags");
+    a.fallback_flag = b.fb_flag;
+    {
+        LaunchTimer t(kProbe, st);
+        probe_kernel<<<(unsigned)b.nq, kProbeThreads, probe_smem_bytes(D, a.Spow2), st>>>(a);
+        t.finish();
+        ERQ_CUDA(cudaGetLastError());
+    }
+    {
+        LaunchTimer t(kProbe, st);
+        probe_fallback_kernel<<<(unsigned)b.nq, kProbeThreads, probe_fallback_smem_bytes(D, a.Kpow2), st>>>(a);
+        t.finish();
+        ERQ_CUDA(cudaGetLastError());
+    }
     return ERQ_OK;
 }
 

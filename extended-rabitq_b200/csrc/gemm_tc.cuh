@@ -23,6 +23,7 @@
 namespace erq {
 
 constexpr int kTcBM = 128, kTcBN = 256, kTcBK = 64, kTcStages = 4;
+constexpr int kTcMinBlocks = 1;  // CTAs per SM the ring leaves room for
 constexpr int kTcThreads = 192;
 constexpr uint32_t kTcABytes = kTcBM * kTcBK * 2;   // 16 KB
 constexpr uint32_t kTcBBytes = kTcBN * kTcBK * 2;   // 32 KB
@@ -84,7 +85,7 @@ __device__ __forceinline__ void tc_fence_after() {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 }
 
-__global__ void __launch_bounds__(kTcThreads, 1) gemm_tc_kernel(
+__global__ void __launch_bounds__(kTcThreads, kTcMinBlocks) gemm_tc_kernel(
     const __grid_constant__ CUtensorMap tma_a, const __grid_constant__ CUtensorMap tma_b,
     float* __restrict__ Cout, int M, int N, int Kd, GemmEpilogue epi, uint32_t* status) {
     extern __shared__ uint8_t smem_raw[];
@@ -110,7 +111,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) gemm_tc_kernel(
     if (warp == 1) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                          (uint32_t)__cvta_generic_to_shared(tmem_slot)),
-                     "r"(256u)
+                     "r"((uint32_t)kTcBN)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -224,7 +225,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) gemm_tc_kernel(
     __syncthreads();
     if (warp == 1) {
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256u)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)kTcBN)
                      : "memory");
     }
     if (tid == 0 && *flag && status) atomicOr(status, 1u);

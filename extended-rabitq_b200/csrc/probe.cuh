@@ -33,6 +33,8 @@ struct ProbeArgs {
     uint32_t* fallbacks;      // optional counter of queries that took step 4
     float* near_d;            // optional [nq][64]: the 64 smallest distance estimates, ascending
     int nq, K, Kpow2, D, nprobe, M;
+    int Spow2;                // sort-key capacity of probe_kernel (probe_smem_bytes)
+    uint32_t* fallback_flag;  // [nq]: 1 when the query needs probe_fallback_kernel
     int check_rank;           // rank whose exactness the bound check proves (>= nprobe)
 };
 
@@ -79,9 +81,42 @@ __device__ __forceinline__ void block_bitonic_sort(uint64_t* keys, int n) {
     }
 }
 
-// Shared memory: q[D] | keys u32 [K] | sort keys u64 [Kpow2] | hist[256] | misc
-__host__ __device__ constexpr size_t probe_smem_bytes(int D, int K, int Kpow2) {
-    return (size_t)D * 4 + (size_t)K * 4 + 8 + (size_t)Kpow2 * 8 + 256 * 4 + 64;
+// Shared memory of probe_kernel: q[D] | sort keys u64 [Spow2] | hist[256] | misc.
+// Spow2 is a power of two >= max(M, 64) + 1 (or >= K when every centroid is
+// selected); the estimates are re-read from global memory (L1-resident) by each
+// radix pass instead of being copied, so many blocks fit on an SM.
+__host__ __device__ constexpr size_t probe_smem_bytes(int D, int Spow2) {
+    return (size_t)D * 4 + (size_t)Spow2 * 8 + 256 * 4 + 64;
+}
+// probe_fallback_kernel: q[D] | sort keys u64 [Kpow2]
+__host__ __device__ constexpr size_t probe_fallback_smem_bytes(int D, int Kpow2) {
+    return (size_t)D * 4 + (size_t)Kpow2 * 8 + 64;
+}
+
+// Outputs of one query from its sorted (distance, id) keys, and the exclusive
+// prefix of 32 * nblocks over the probe order; warp 0.
+__device__ __forceinline__ void probe_outputs(const ProbeArgs& a, int q, const uint64_t* sorted,
+                                              int lane) {
+    uint64_t run = (uint64_t)q * a.stride;
+    for (int p0 = 0; p0 < a.nprobe; p0 += 32) {
+        const int p = p0 + lane;
+        uint32_t nbv = 0;
+        if (p < a.nprobe) {
+            const uint64_t key = sorted[p];
+            const uint32_t cid = (uint32_t)(key & 0xffffffffu);
+            a.probe_cid[(size_t)q * a.nprobe + p] = cid;
+            a.probe_sqy[(size_t)q * a.nprobe + p] = __uint_as_float((uint32_t)(key >> 32));
+            nbv = 32u * a.c_nblocks[cid];
+        }
+        uint32_t incl = nbv;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t n = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += n;
+        }
+        if (p < a.nprobe) a.s_off[(size_t)q * a.nprobe + p] = run + (incl - nbv);
+        run += __shfl_sync(0xffffffffu, incl, 31);
+    }
 }
 
 __global__ void __launch_bounds__(kProbeThreads) probe_kernel(ProbeArgs a) {
@@ -90,16 +125,12 @@ __global__ void __launch_bounds__(kProbeThreads) probe_kernel(ProbeArgs a) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int K = a.K, D = a.D;
     float* qs = reinterpret_cast<float*>(smem_raw);
-    uint32_t* keys = reinterpret_cast<uint32_t*>(qs + D);
-    uint64_t* sk = reinterpret_cast<uint64_t*>(
-        reinterpret_cast<uint8_t*>(keys) + (((size_t)K * 4 + 15) & ~size_t(15)));
-    uint32_t* hist = reinterpret_cast<uint32_t*>(sk + a.Kpow2);
+    uint64_t* sk = reinterpret_cast<uint64_t*>(qs + D);
+    uint32_t* hist = reinterpret_cast<uint32_t*>(sk + a.Spow2);
     int* misc = reinterpret_cast<int*>(hist + 256);  // [0] digit [1] before [2] count [3] ok
 
     for (int i = tid; i < D; i += blockDim.x) qs[i] = a.qrot[(size_t)q * D + i];
     const float* aq = a.approx + (size_t)q * K;
-    for (int c = tid; c < K; c += blockDim.x) keys[c] = order_key(aq[c]);
-    __syncthreads();
 
     const int M = a.M;
     // with features requested the 64 smallest estimates are selected as well
@@ -107,14 +138,14 @@ __global__ void __launch_bounds__(kProbeThreads) probe_kernel(ProbeArgs a) {
     const bool select_all = Msel + 1 > K;
     uint32_t kstar = 0xffffffffu;
     if (!select_all) {
-        // radix select of the (M+1)-th smallest key, 8 bits at a time
+        // radix select of the (Msel+1)-th smallest key, 8 bits at a time
         uint32_t prefix = 0, pmask = 0;
         int rank = Msel + 1;
         for (int shift = 24; shift >= 0; shift -= 8) {
             for (int i = tid; i < 256; i += blockDim.x) hist[i] = 0;
             __syncthreads();
             for (int c = tid; c < K; c += blockDim.x) {
-                const uint32_t kk = keys[c];
+                const uint32_t kk = order_key(__ldg(aq + c));
                 if ((kk & pmask) == prefix) atomicAdd(&hist[(kk >> shift) & 255u], 1u);
             }
             __syncthreads();
@@ -152,15 +183,16 @@ __global__ void __launch_bounds__(kProbeThreads) probe_kernel(ProbeArgs a) {
         }
         kstar = prefix;
     }
-    // candidates: every centroid whose estimate is below the (M+1)-th
+    // candidates: every centroid whose estimate is below the (Msel+1)-th
     if (tid == 0) misc[2] = 0;
     __syncthreads();
     for (int c = tid; c < K; c += blockDim.x) {
-        if (select_all || keys[c] < kstar) {
+        const uint32_t kk = order_key(__ldg(aq + c));
+        if (select_all || kk < kstar) {
             const int slot = atomicAdd(&misc[2], 1);
             // id (exact distance filled below), with its estimate key when
             // the features need the estimates in order
-            sk[slot] = a.near_d ? (((uint64_t)keys[c] << 32) | (uint64_t)c) : (uint64_t)c;
+            sk[slot] = a.near_d ? (((uint64_t)kk << 32) | (uint64_t)c) : (uint64_t)c;
         }
     }
     __syncthreads();
@@ -203,7 +235,7 @@ __global__ void __launch_bounds__(kProbeThreads) probe_kernel(ProbeArgs a) {
     for (int i = ns + tid; i < nsort; i += blockDim.x) sk[i] = ~0ull;
     __syncthreads();
     block_bitonic_sort(sk, nsort);
-    // bound check
+    // bound check; a query that fails it goes to probe_fallback_kernel
     if (tid == 0) {
         bool ok = ns >= a.check_rank;
         if (ok && truncated) {
@@ -212,45 +244,37 @@ __global__ void __launch_bounds__(kProbeThreads) probe_kernel(ProbeArgs a) {
             const float A = order_key_value(akey);
             ok = (A - eps > e_n) && (e_n == e_n);
         }
+        a.fallback_flag[q] = ok ? 0u : 1u;
         misc[3] = ok ? 1 : 0;
         if (!ok && a.fallbacks) atomicAdd(a.fallbacks, 1u);
     }
     __syncthreads();
-    if (!misc[3]) {
-        // exact distances of all K centroids
-        for (int base = 0; base < K; base += nhw) {
-            const int c = base + hw;
-            const float e = l2sqr16_halfwarp(qs, a.centroids + (size_t)min(c, K - 1) * D, D, l);
-            if (l == 0 && c < K) sk[c] = dist_key(e, (uint32_t)c);
-        }
-        __syncthreads();
-        for (int i = K + tid; i < a.Kpow2; i += blockDim.x) sk[i] = ~0ull;
-        __syncthreads();
-        block_bitonic_sort(sk, a.Kpow2);
+    if (misc[3] && warp == 0) probe_outputs(a, q, sk, lane);
+}
+
+// The queries whose cut could not be proven: exact distances of all K
+// centroids, sorted by (distance, id).  Other blocks return at once.
+__global__ void __launch_bounds__(kProbeThreads) probe_fallback_kernel(ProbeArgs a) {
+    const int q = blockIdx.x;
+    if (!a.fallback_flag[q]) return;
+    extern __shared__ __align__(16) uint8_t smem_raw[];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int K = a.K, D = a.D;
+    float* qs = reinterpret_cast<float*>(smem_raw);
+    uint64_t* sk = reinterpret_cast<uint64_t*>(qs + D);
+    for (int i = tid; i < D; i += blockDim.x) qs[i] = a.qrot[(size_t)q * D + i];
+    __syncthreads();
+    const int hw = tid >> 4, l = tid & 15, nhw = blockDim.x >> 4;
+    for (int base = 0; base < K; base += nhw) {
+        const int c = base + hw;
+        const float e = l2sqr16_halfwarp(qs, a.centroids + (size_t)min(c, K - 1) * D, D, l);
+        if (l == 0 && c < K) sk[c] = dist_key(e, (uint32_t)c);
     }
-    // outputs + exclusive prefix of 32*nblocks over the probe order (warp 0)
-    if (warp == 0) {
-        uint64_t run = (uint64_t)q * a.stride;
-        for (int p0 = 0; p0 < a.nprobe; p0 += 32) {
-            const int p = p0 + lane;
-            uint32_t nbv = 0;
-            if (p < a.nprobe) {
-                const uint64_t key = sk[p];
-                const uint32_t cid = (uint32_t)(key & 0xffffffffu);
-                a.probe_cid[(size_t)q * a.nprobe + p] = cid;
-                a.probe_sqy[(size_t)q * a.nprobe + p] = __uint_as_float((uint32_t)(key >> 32));
-                nbv = 32u * a.c_nblocks[cid];
-            }
-            uint32_t incl = nbv;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const uint32_t n = __shfl_up_sync(0xffffffffu, incl, o);
-                if (lane >= o) incl += n;
-            }
-            if (p < a.nprobe) a.s_off[(size_t)q * a.nprobe + p] = run + (incl - nbv);
-            run += __shfl_sync(0xffffffffu, incl, 31);
-        }
-    }
+    __syncthreads();
+    for (int i = K + tid; i < a.Kpow2; i += blockDim.x) sk[i] = ~0ull;
+    __syncthreads();
+    block_bitonic_sort(sk, a.Kpow2);
+    if (warp == 0) probe_outputs(a, q, sk, lane);
 }
 
 }  // namespace erq
