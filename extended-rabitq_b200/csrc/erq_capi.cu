@@ -216,6 +216,7 @@ struct erq_index {
     uint32_t* c_first_vec = nullptr;
     uint32_t* c_size = nullptr;
     uint32_t* c_nblocks = nullptr;
+    uint32_t* c_size_rank = nullptr;  // [K] rank of each cluster by decreasing size (ties by id)
     // split-BF16 operands of the tensor-core GEMMs (gemm.cuh)
     __nv_bfloat16* c_split = nullptr;   // [K][3D] centroids (hi | lo | hi)
     __nv_bfloat16* pt_split = nullptr;  // [D][3D] rows of P^T (hi | lo | hi)
@@ -235,7 +236,7 @@ struct erq_index {
         }
         for (void* p : {(void*)P, (void*)centroids, (void*)codes, (void*)onorm, (void*)excode,
                         (void*)xipnorm, (void*)ids, (void*)c_first_block, (void*)c_first_vec,
-                        (void*)c_size, (void*)c_nblocks, (void*)c_split, (void*)pt_split,
+                        (void*)c_size, (void*)c_nblocks, (void*)c_size_rank, (void*)c_split, (void*)pt_split,
                         (void*)cn})
             if (p) cudaFree(p);
         if (prev >= 0) cudaSetDevice(prev);
@@ -395,6 +396,15 @@ erq_status load_impl(const char* path, erq_index* idx) {
     ERQ_CUDA(cudaMemcpy(idx->c_first_vec, first_vec.data(), K * 4, cudaMemcpyHostToDevice));
     ERQ_CUDA(cudaMemcpy(idx->c_size, csize.data(), K * 4, cudaMemcpyHostToDevice));
     ERQ_CUDA(cudaMemcpy(idx->c_nblocks, idx->h_nblocks.data(), K * 4, cudaMemcpyHostToDevice));
+    {
+        std::vector<uint32_t> byz(K), rank(K);
+        std::iota(byz.begin(), byz.end(), 0u);
+        std::stable_sort(byz.begin(), byz.end(),
+                         [&](uint32_t x, uint32_t y) { return csize[x] > csize[y]; });
+        for (uint64_t r = 0; r < K; ++r) rank[byz[r]] = (uint32_t)r;
+        ERQ_TRY(dev_alloc(idx, &idx->c_size_rank, K));
+        ERQ_CUDA(cudaMemcpy(idx->c_size_rank, rank.data(), K * 4, cudaMemcpyHostToDevice));
+    }
     // split-BF16 GEMM operands: centroids and the rows of P^T
     ERQ_TRY(dev_alloc(idx, &idx->c_split, K * 3 * D));
     ERQ_TRY(dev_alloc(idx, &idx->pt_split, D * 3 * D));
@@ -672,13 +682,14 @@ erq_status bucket_sort(const erq_index* idx, const uint32_t* keys, uint32_t n, u
 // (query, probe) pairs by cluster into b.order_pairs (pairs a per-query probe
 // count leaves out go last), runs delimited by b.buckets.
 erq_status order_pairs(const erq_index* idx, const Batch& b, uint64_t nprobe, cudaStream_t st,
-                       const int* q_nprobe) {
+                       const int* q_nprobe, bool by_size = false) {
     const uint64_t pairs = b.nq * nprobe;
     if (pairs == 0) return ERQ_OK;
     {
         LaunchTimer t(kOrder, st);
         pair_keys_kernel<<<(unsigned)div_up(pairs, 256), 256, 0, st>>>(
-            b.probe_cid, (uint32_t)pairs, (int)nprobe, q_nprobe, (uint32_t)idx->K, b.keys);
+            b.probe_cid, (uint32_t)pairs, (int)nprobe, q_nprobe, (uint32_t)idx->K,
+            by_size ? idx->c_size_rank : nullptr, b.keys);
         t.finish();
     }
     return bucket_sort(idx, b.keys, (uint32_t)pairs, b.buckets, b.order_pairs, st);
@@ -690,7 +701,8 @@ erq_status order_queries(const erq_index* idx, const Batch& b, uint64_t nprobe, 
     {
         LaunchTimer t(kOrder, st);
         query_keys_kernel<<<(unsigned)div_up(b.nq, 256), 256, 0, st>>>(b.probe_cid, (uint32_t)b.nq,
-                                                                      (int)nprobe, b.keys);
+                                                                      (int)nprobe, idx->c_size_rank,
+                                                                      b.keys);
         t.finish();
     }
     return bucket_sort(idx, b.keys, (uint32_t)b.nq, b.buckets_q, b.order_q, st);
@@ -702,7 +714,7 @@ bool launch_order(const erq_index* idx, const Batch& b, uint64_t nprobe, cudaStr
                   const int* q_nprobe, erq_status* err) {
     *err = ERQ_OK;
     if (b.nq * nprobe < 1024 || !b.order_pairs) return false;
-    if ((*err = order_pairs(idx, b, nprobe, st, q_nprobe)) != ERQ_OK) return false;
+    if ((*err = order_pairs(idx, b, nprobe, st, q_nprobe, true)) != ERQ_OK) return false;
     if ((*err = order_queries(idx, b, nprobe, st)) != ERQ_OK) return false;
     return true;
 }

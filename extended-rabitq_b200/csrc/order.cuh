@@ -13,20 +13,27 @@ namespace erq {
 
 // key of (query, probe) pair i: its cluster, or K for pairs a per-query probe
 // count leaves out (those blocks exit at once; they go last).
+// With size_rank the key is the cluster's rank by decreasing size instead
+// (one scan block per pair: the longest scans start first).
 __global__ void pair_keys_kernel(const uint32_t* __restrict__ probe_cid, uint32_t pairs, int nprobe,
                                  const int* __restrict__ q_nprobe, uint32_t K,
+                                 const uint32_t* __restrict__ size_rank,
                                  uint32_t* __restrict__ keys) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= pairs) return;
     const uint32_t q = i / (uint32_t)nprobe, p = i - q * (uint32_t)nprobe;
-    keys[i] = (q_nprobe && (int)p >= q_nprobe[q]) ? K : probe_cid[i];
+    const uint32_t c = probe_cid[i];
+    keys[i] = (q_nprobe && (int)p >= q_nprobe[q]) ? K : (size_rank ? size_rank[c] : c);
 }
 
-// key of query q: the cluster it probes first.
+// key of query q: the rank, by decreasing size, of the cluster it probes
+// first.  Queries of one cluster stay together (L2 reuse) and the queries
+// with the most refinement work start first, so none of them is left for the
+// last wave of thread blocks.
 __global__ void query_keys_kernel(const uint32_t* __restrict__ probe_cid, uint32_t nq, int nprobe,
-                                  uint32_t* __restrict__ keys) {
+                                  const uint32_t* __restrict__ size_rank, uint32_t* __restrict__ keys) {
     const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q < nq) keys[q] = probe_cid[(size_t)q * nprobe];
+    if (q < nq) keys[q] = size_rank[probe_cid[(size_t)q * nprobe]];
 }
 
 // Lanes of a warp with equal keys add once (popular clusters and the
