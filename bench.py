@@ -366,14 +366,19 @@ def run_ours(args, cfg, name):
     from erq_b200 import _lib as L
 
     L.probe_fallbacks(local, reset=True)
+    L.refine_stats(local, enable=True)
     idx.search_raw(query, k, nprobe, with_dists=False)
+    rst_plain = L.refine_stats(local, enable=False)
+    cand_plain = rst_plain["candidates"]
     fallback_rate = L.probe_fallbacks(local, reset=True) / nq
-    log(f"probe fallback rate {fallback_rate:.5f}")
+    log(f"probe fallback rate {fallback_rate:.5f}; refinement per query: "
+        + ", ".join(f"{kk} {v / nq:.1f}" for kk, v in rst_plain.items()))
     base = np.load(os.path.join(d, "base.npy"), mmap_mode="r")
     sub = min(1000, nq)
     arr = indexfile.read_index(index_path)
     nblocks = (arr.sizes.astype(np.int64) + 31) // 32
     block_bytes = 4 * arr.D + 128
+    cand_bytes = arr.D * arr.EX // 8 + 8  # EX-code row + xipnorm + id per exact candidate
     qrot_h = idx.rotate(query)
     cids, _ = idx.debug_probe(qrot_h, max(nprobe, learned.DEFAULT_BINS[-1]))
     del arr
@@ -396,7 +401,8 @@ def run_ours(args, cfg, name):
     ms_p, prof_p, clocks_p = timed(plain_dev, args.steps, args.warmup, world, stream, local)
     assert (ids_d.cpu().numpy().view(np.uint32) == ids0).all()
     plain = {"value": round(world * nq * args.steps / (ms_p / 1e3), 1), "nprobe": nprobe,
-             "recall@100": round(recall, 5), "ms_per_step": round(ms_p / args.steps, 4)}
+             "recall@100": round(recall, 5), "ms_per_step": round(ms_p / args.steps, 4),
+             "refine_per_query": {kk: round(v / nq, 2) for kk, v in rst_plain.items()}}
     ms_pe = None
     if not args.no_e2e:
         ms_pe, _, _ = timed(plain_host, args.steps, args.warmup, world, stream)
@@ -427,7 +433,8 @@ def run_ours(args, cfg, name):
         return ms, e2e, clocks, prof
 
     modes = {"plain": {"ms": ms_p, "prof": prof_p, "clocks": clocks_p, "recall": recall,
-                       "ids": ids0, "scan_bytes": scan_bytes_plain, "e2e_ms": ms_pe}}
+                       "ids": ids0, "scan_bytes": scan_bytes_plain, "e2e_ms": ms_pe,
+                       "refine_bytes": cand_plain * cand_bytes}}
     batched = None
     if not args.no_batched:
         plan_b = Plan(idx, max_batch=nq, k=k, nprobe=nprobe, raw=True)
@@ -439,7 +446,8 @@ def run_ours(args, cfg, name):
         if e2e_b is not None:
             batched["e2e"] = round(world * nq * args.steps / (e2e_b / 1e3), 1)
         modes["batched"] = {"ms": ms_b, "prof": prof_b, "clocks": clocks_b, "recall": recall,
-                            "ids": ids0, "scan_bytes": scan_bytes_plain, "e2e_ms": e2e_b}
+                            "ids": ids0, "scan_bytes": scan_bytes_plain, "e2e_ms": e2e_b,
+                            "refine_bytes": cand_plain * cand_bytes}
         plan_b.free()
 
     # --- learned per-query depth, batched
@@ -464,9 +472,15 @@ def run_ours(args, cfg, name):
             conf, r_l, ids_l, used = best
             plan_l.set_learned(conf)
             L.probe_fallbacks(local, reset=True)
+            plan_l.set_graphs(False)  # counting is fixed into a graph when it is captured
+            L.refine_stats(local, enable=True)
             plan_l.search(query, with_dists=False)
+            rst_l = L.refine_stats(local, enable=False)
+            cand_l = rst_l["candidates"]
+            plan_l.set_graphs(True)
             learned_fallback_rate = L.probe_fallbacks(local, reset=True) / nq
-            log(f"learned probe fallback rate {learned_fallback_rate:.5f}")
+            log(f"learned probe fallback rate {learned_fallback_rate:.5f}; refinement per "
+                "query: " + ", ".join(f"{kk} {v / nq:.1f}" for kk, v in rst_l.items()))
             tune_l, _ = plan_l.autotune(query, reps=2)
             ms_l, e2e_l, clocks_l, prof_l = plan_mode(plan_l, ids_l)
             take = np.arange(cids.shape[1])[None, :] < used.astype(np.int64)[:, None]
@@ -476,13 +490,15 @@ def run_ours(args, cfg, name):
                             "recall@100": round(r_l, 5),
                             "ms_per_step": round(ms_l / args.steps, 4), "tuning": tune_l,
                             "probe_fallback_rate": round(learned_fallback_rate, 5),
+                            "refine_per_query": {kk: round(v / nq, 2) for kk, v in rst_l.items()},
                             "kernels_ms_per_step": {kk: round(v[1] / args.steps, 4)
                                                     for kk, v in prof_l.items() if v[0]},
                             "model": meta}
             if e2e_l is not None:
                 learned_info["e2e"] = round(world * nq * args.steps / (e2e_l / 1e3), 1)
             modes["learned"] = {"ms": ms_l, "prof": prof_l, "clocks": clocks_l, "recall": r_l,
-                                "ids": ids_l, "scan_bytes": scan_bytes_l, "e2e_ms": e2e_l}
+                                "ids": ids_l, "scan_bytes": scan_bytes_l, "e2e_ms": e2e_l,
+                                "refine_bytes": cand_l * cand_bytes}
         plan_l.free()
         model.free()
     mode = min(modes, key=lambda m: modes[m]["ms"])
@@ -491,7 +507,6 @@ def run_ours(args, cfg, name):
     ratio = metrics.average_distance_ratio(query[:sub], base, chosen["ids"][:sub].astype(np.int64),
                                            gt[:sub].astype(np.int64), k)
     prof = chosen["prof"]
-    scan_n, scan_ms = prof["scan"]
     launches = sum(v[0] for v in prof.values())
     peaks = {}
     try:
@@ -501,10 +516,23 @@ def run_ours(args, cfg, name):
     peak = peaks.get("hbm_gbs")
     peak_src = "measured" if peak else "fallback"
     peak = peak or 6650.0
-    achieved = None
-    if scan_n:
-        per_launch_bytes = chosen["scan_bytes"] * args.steps / scan_n
-        achieved = per_launch_bytes / (scan_ms / scan_n / 1e3) / 1e9
+    # algorithmic bytes per step of the two HBM-side kernels: scan = the
+    # probed clusters' code blocks (4D + 128 B per block), refine = the exact
+    # candidates' EX-code rows + xipnorm + id (D*EX/8 + 8 B each)
+    kernel_names = {"scan": "scan_kernel" if mode == "plain" else "scan_batched_kernel",
+                    "refine": "refine_kernel"}
+    rooflines = {}
+    for kn, step_bytes in (("scan", chosen["scan_bytes"]), ("refine", chosen["refine_bytes"])):
+        n_launch, tot_ms = prof.get(kn, (0, 0.0))
+        if not n_launch:
+            continue
+        achieved = step_bytes * args.steps / n_launch / (tot_ms / n_launch / 1e3) / 1e9
+        rooflines[kn] = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+                         "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
+                         "kernel": kernel_names[kn], "ms_per_step": round(tot_ms / args.steps, 4),
+                         "bytes_per_step": int(step_bytes),
+                         "peak_source": f"{peak_src} hbm_gbs (copy)"}
+    dominant = max(rooflines, key=lambda kn: rooflines[kn]["ms_per_step"]) if rooflines else None
     e2e_ms = chosen["e2e_ms"]
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -544,12 +572,8 @@ def run_ours(args, cfg, name):
                 "h2d_bytes_per_step": int(nq * query.shape[1] * 4),
                 "d2h_bytes_per_step": int(nq * k * 8)},
             "gpu_launches": int(launches),
-            "roofline": {"bound": "hbm", "achieved": round(achieved, 1) if achieved else None,
-                         "peak": peak, "unit": "GB/s",
-                         "frac": round(achieved / peak, 4) if achieved else None,
-                         "traffic": None,
-                         "kernel": "scan_kernel" if mode == "plain" else "scan_batched_kernel",
-                         "peak_source": f"{peak_src} hbm_gbs (copy)"},
+            "roofline": rooflines.get(dominant),
+            "roofline_other": {kn: r for kn, r in rooflines.items() if kn != dominant},
             "kernels_ms_per_step": {kk: round(v[1] / args.steps, 4) for kk, v in prof.items()
                                     if v[0]},
             "cpu_baseline": cpu,

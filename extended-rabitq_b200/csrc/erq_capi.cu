@@ -13,6 +13,7 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdarg>
 #include <cstdio>
 #include <cmath>
@@ -742,6 +743,24 @@ uint32_t* probe_fallback_counter() {
     return ptrs[dev];
 }
 
+// Refinement statistics (RefineArgs::stats), per device image, counted while
+// g_refine_stats_on is set (erq_debug_refine_stats).
+__device__ unsigned long long g_refine_stats[4];
+std::atomic<bool> g_refine_stats_on{false};
+unsigned long long* refine_stats_counter() {
+    static unsigned long long* ptrs[kMaxDevices] = {};
+    static std::mutex mu;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return nullptr;
+    std::lock_guard<std::mutex> g(mu);
+    if (!ptrs[dev]) {
+        void* p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_refine_stats) != cudaSuccess) return nullptr;
+        ptrs[dev] = static_cast<unsigned long long*>(p);
+    }
+    return ptrs[dev];
+}
+
 // Coarse probe on tensor cores: split the rotated queries, estimate all
 // distances with the split-BF16 GEMM, then the exact probe kernel.
 erq_status launch_probe_tc(const erq_index* idx, const Batch& b, uint64_t nprobe, cudaStream_t st,
@@ -857,6 +876,7 @@ erq_status launch_refine(const erq_index* idx, const Batch& b, uint64_t nprobe, 
     RefineArgs a;
     a.order = order;
     a.bmin = b.bmin;
+    a.stats = g_refine_stats_on.load() ? refine_stats_counter() : nullptr;
     a.qrot = b.qrot;
     a.centroids = idx->centroids;
     a.probe_cid = b.probe_cid;
@@ -1998,6 +2018,21 @@ erq_status erq_debug_probe_fallbacks(int device, uint64_t* count, int reset) {
     ERQ_CUDA(cudaMemcpy(&v, c, sizeof(v), cudaMemcpyDeviceToHost));
     *count = v;
     if (reset) ERQ_CUDA(cudaMemset(c, 0, sizeof(uint32_t)));
+    return ERQ_OK;
+}
+
+erq_status erq_debug_refine_stats(int device, int enable, uint64_t stats[4]) {
+    if (!stats) return fail(ERQ_ERR_INVALID_ARGUMENT, "stats is NULL");
+    DeviceGuard guard;
+    ERQ_TRY(guard.set(device));
+    unsigned long long* c = refine_stats_counter();
+    if (!c) return fail(ERQ_ERR_CUDA, "refinement counters unavailable");
+    ERQ_CUDA(cudaDeviceSynchronize());
+    unsigned long long v[4] = {};
+    ERQ_CUDA(cudaMemcpy(v, c, sizeof(v), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < 4; ++i) stats[i] = v[i];
+    ERQ_CUDA(cudaMemset(c, 0, sizeof(v)));
+    g_refine_stats_on.store(enable != 0);
     return ERQ_OK;
 }
 

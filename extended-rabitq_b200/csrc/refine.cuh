@@ -46,6 +46,10 @@ struct RefineArgs {
     const uint32_t* order;        // optional: block i refines query order[i]
     const float* bmin;            // optional: smallest lower bound per scanned block, at
                                   // s_off/32 + block (blocks above the threshold are skipped)
+    unsigned long long* stats;    // optional [4], added to once per query: the reference's
+                                  // exact candidates (lower bound below the threshold at
+                                  // their block's start), lanes refined (the windows'
+                                  // supersets), windows, window blocks
     int nq, D, EX, nprobe, k;
 };
 
@@ -315,6 +319,7 @@ __global__ void __launch_bounds__(kRefineThreads, 8) refine_kernel(RefineArgs a)
     }
     int size = 0;         // pool state, maintained by warp 0
     float distk = FLT_MAX;
+    uint32_t st_cand = 0, st_refined = 0, st_windows = 0, st_blocks = 0;  // with a.stats
     __syncthreads();
 
     const int np_q = a.q_nprobe ? a.q_nprobe[q] : a.nprobe;
@@ -406,6 +411,11 @@ __global__ void __launch_bounds__(kRefineThreads, 8) refine_kernel(RefineArgs a)
             }
             __syncthreads();
             const int cnt = misc[0];
+            if (a.stats) {
+                st_refined += cnt;
+                st_windows += 1;
+                st_blocks += nbw;
+            }
             if (cnt == 0) {  // uniform: nothing in this window can pass
                 wb = wnext;
                 continue;
@@ -482,7 +492,9 @@ __global__ void __launch_bounds__(kRefineThreads, 8) refine_kernel(RefineArgs a)
                     // candidates of the block against the threshold at its
                     // start; those above a full pool's k-th cannot enter
                     const float ed = w_ed[32 * b + lane];
-                    const bool enter = w_lb[32 * b + lane] < distk && (size < k || !(ed > distk));
+                    const bool below = w_lb[32 * b + lane] < distk;
+                    if (a.stats) st_cand += __popc(__ballot_sync(0xffffffffu, below));
+                    const bool enter = below && (size < k || !(ed > distk));
                     if (__ballot_sync(0xffffffffu, enter))
                         pool_merge_block(pool_d, pool_id, size, k, distk, enter, ed,
                                          w_id[32 * b + lane], cs, lane);
@@ -497,6 +509,12 @@ __global__ void __launch_bounds__(kRefineThreads, 8) refine_kernel(RefineArgs a)
         }
     }
     if (warp == 0) {
+        if (a.stats && lane == 0) {
+            atomicAdd(a.stats + 0, (unsigned long long)st_cand);
+            atomicAdd(a.stats + 1, (unsigned long long)st_refined);
+            atomicAdd(a.stats + 2, (unsigned long long)st_windows);
+            atomicAdd(a.stats + 3, (unsigned long long)st_blocks);
+        }
         uint32_t* oid = a.out_ids + (size_t)q * k;
         for (int i = lane; i < k; i += 32) {
             oid[i] = i < size ? pool_id[i] : 0u;

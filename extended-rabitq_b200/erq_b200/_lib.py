@@ -36,7 +36,7 @@ EXPORTED_SYMBOLS = (
     "erq_search_learned_raw",
     "erq_debug_probe_model_grads", "erq_debug_probe_model_params",
     "erq_plan_create", "erq_plan_free", "erq_plan_set_learned", "erq_plan_autotune",
-    "erq_plan_set_tuning", "erq_plan_get_tuning", "erq_plan_search", "erq_plan_device_bytes", "erq_plan_set_graphs", "erq_debug_gemm_bf16", "erq_debug_probe_fallbacks",
+    "erq_plan_set_tuning", "erq_plan_get_tuning", "erq_plan_search", "erq_plan_device_bytes", "erq_plan_set_graphs", "erq_debug_gemm_bf16", "erq_debug_probe_fallbacks", "erq_debug_refine_stats",
 )
 
 
@@ -132,6 +132,8 @@ def load_library(path: str | None = None) -> C.CDLL:
     lib.erq_debug_gemm_bf16.restype = C.c_int
     lib.erq_debug_probe_fallbacks.argtypes = [C.c_int, C.POINTER(C.c_uint64), C.c_int]
     lib.erq_debug_probe_fallbacks.restype = C.c_int
+    lib.erq_debug_refine_stats.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_uint64)]
+    lib.erq_debug_refine_stats.restype = C.c_int
     lib.erq_plan_set_graphs.argtypes = [vp, C.c_int]
     lib.erq_plan_set_graphs.restype = C.c_int
     lib.erq_profile_enable.argtypes = [C.c_int]
@@ -188,6 +190,16 @@ def probe_fallbacks(device: int = 0, reset: bool = True) -> int:
     n = C.c_uint64()
     check(load_library().erq_debug_probe_fallbacks(device, C.byref(n), 1 if reset else 0))
     return int(n.value)
+
+
+def refine_stats(device: int = 0, enable: bool = False) -> dict:
+    """Refinement counters since the last call (exact candidates, distances
+    computed, windows, window blocks); counting is then on for later
+    refinement launches when `enable` (graphs captured earlier keep their
+    setting)."""
+    v = (C.c_uint64 * 4)()
+    check(load_library().erq_debug_refine_stats(device, 1 if enable else 0, v))
+    return dict(zip(("candidates", "refined", "windows", "blocks"), (int(x) for x in v)))
 
 
 def profile_read() -> dict:

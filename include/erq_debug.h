@@ -64,6 +64,16 @@ ERQ_API erq_status erq_debug_gemm_bf16(const uint16_t* A, const uint16_t* B, uin
  * (process-wide, per device). */
 ERQ_API erq_status erq_debug_probe_fallbacks(int device, uint64_t* count, int reset);
 
+/* Refinement counters since the last call, process-wide per device:
+ * stats[0] = exact candidates (vectors whose lower bound was below the top-k
+ * threshold at the start of their block: the vectors whose EX-bit distance
+ * the reference computes), stats[1] = distances computed (the candidate
+ * supersets of the refinement windows), stats[2] = windows, stats[3] =
+ * blocks of 32 vectors in those windows.  Waits for the device, returns and
+ * resets the counters, and turns counting on or off for refinement launches
+ * issued afterwards (a CUDA graph keeps the setting it was captured with). */
+ERQ_API erq_status erq_debug_refine_stats(int device, int enable, uint64_t stats[4]);
+
 /* Kernel timing.  While enabled, every kernel launch of the search and
  * rotation entry points is bracketed by CUDA events recorded on the stream
  * the kernel runs on.  erq_profile_read waits for the recorded events and

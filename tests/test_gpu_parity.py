@@ -118,6 +118,26 @@ def test_every_nprobe_and_k_match_oracle(case, oracle_mod):
     o.close()
 
 
+def test_refine_candidate_count(case, oracle_mod):
+    """The refinement's candidate counter equals the number of EX-bit
+    distances the reference computes (the oracle's trace length)."""
+    from erq_b200 import _lib as L
+
+    g, idx = case
+    o = oracle_mod.Oracle(g["path"])
+    q = g["qrot"]
+    k, nprobe = int(g["k"]), int(g["nprobe"])
+    L.refine_stats(0, enable=True)
+    idx.search_batch(q, k, nprobe)
+    st = L.refine_stats(0, enable=False)
+    want = sum(len(o.trace(q[i], k, nprobe)[0]) for i in range(q.shape[0]))
+    assert st["candidates"] == want
+    assert want <= st["refined"] <= 32 * st["blocks"] and st["windows"] > 0
+    idx.search_batch(q, k, nprobe)  # counting off: nothing added
+    assert L.refine_stats(0, enable=False) == dict.fromkeys(st, 0)
+    o.close()
+
+
 def test_rotation_accuracy(case):
     g, idx = case
     from erq_b200 import indexfile
