@@ -26,6 +26,24 @@ __device__ __forceinline__ float tree16_sum(float v) {
     return v;
 }
 
+// Packed FP32 pairs (sm_100a f32x2): two independent IEEE round-to-nearest
+// operations per instruction, each equal to its scalar counterpart.
+__device__ __forceinline__ float2 ffma2(float2 a, float2 b, float2 c) {
+    uint64_t d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;"
+        : "=l"(d)
+        : "l"(*reinterpret_cast<const uint64_t*>(&a)), "l"(*reinterpret_cast<const uint64_t*>(&b)),
+          "l"(*reinterpret_cast<const uint64_t*>(&c)));
+    return *reinterpret_cast<float2*>(&d);
+}
+__device__ __forceinline__ float2 fsub2(float2 a, float2 b) {
+    uint64_t d;
+    asm("sub.rn.f32x2 %0, %1, %2;"
+        : "=l"(d)
+        : "l"(*reinterpret_cast<const uint64_t*>(&a)), "l"(*reinterpret_cast<const uint64_t*>(&b)));
+    return *reinterpret_cast<float2*>(&d);
+}
+
 // (float)(1.0 / (double)x): the reference computes these reciprocals in
 // double and rounds once to float (inc/utils/space.hpp:760,774;
 // inc/index/HASearcher.hpp:56).

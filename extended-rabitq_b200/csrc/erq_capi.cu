@@ -469,7 +469,7 @@ erq_status configure_kernels(int D, int K, int k) {
     ERQ_CUDA(cudaFuncSetAttribute(scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)scan_smem_bytes(D)));
     ERQ_CUDA(cudaFuncSetAttribute(probe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)probe_smem_bytes(D, kp2)));
+                                  (int)probe_smem_bytes(D, kp2, K <= kProbeStageKeys ? K : 0)));
     ERQ_CUDA(cudaFuncSetAttribute(probe_fallback_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)probe_fallback_smem_bytes(D, kp2)));
     const int rs = (int)refine_smem_bytes(D, k);
@@ -806,9 +806,11 @@ erq_status launch_probe_tc(const erq_index* idx, const Batch& b, uint64_t nprobe
     }
     if (!b.fb_flag) return fail(ERQ_ERR_INVALID_ARGUMENT, "probe batch without fallback flags");
     a.fallback_flag = b.fb_flag;
+    a.stage_keys = K <= kProbeStageKeys ? 1 : 0;
     {
         LaunchTimer t(kProbe, st);
-        probe_kernel<<<(unsigned)b.nq, kProbeThreads, probe_smem_bytes(D, a.Spow2), st>>>(a);
+        probe_kernel<<<(unsigned)b.nq, kProbeThreads, probe_smem_bytes(D, a.Spow2, a.stage_keys ? K : 0),
+                       st>>>(a);
         t.finish();
         ERQ_CUDA(cudaGetLastError());
     }

@@ -36,10 +36,13 @@ struct ProbeArgs {
     int Spow2;                // sort-key capacity of probe_kernel (probe_smem_bytes)
     uint32_t* fallback_flag;  // [nq]: 1 when the query needs probe_fallback_kernel
     int check_rank;           // rank whose exactness the bound check proves (>= nprobe)
+    int stage_keys;           // nonzero: probe_kernel copies the K order keys to shared
+                              // memory once (K <= kProbeStageKeys)
 };
 
 constexpr int kProbeThreads = 256;
 constexpr int kProbeFeatRank = 64;  // estimates written to near_d
+constexpr int kProbeStageKeys = 4096;  // largest K whose keys are staged in shared memory
 
 __device__ __forceinline__ uint32_t order_key(float f) {
     const uint32_t b = __float_as_uint(f);
@@ -81,12 +84,13 @@ __device__ __forceinline__ void block_bitonic_sort(uint64_t* keys, int n) {
     }
 }
 
-// Shared memory of probe_kernel: q[D] | sort keys u64 [Spow2] | hist[256] | misc.
-// Spow2 is a power of two >= max(M, 64) + 1 (or >= K when every centroid is
-// selected); the estimates are re-read from global memory (L1-resident) by each
-// radix pass instead of being copied, so many blocks fit on an SM.
-__host__ __device__ constexpr size_t probe_smem_bytes(int D, int Spow2) {
-    return (size_t)D * 4 + (size_t)Spow2 * 8 + 256 * 4 + 64;
+// Shared memory of probe_kernel: q[D] | order keys u32 [Kst] | sort keys u64
+// [Spow2] | hist[256] | misc.  Kst = K rounded up to even when the keys are
+// staged (stage_keys), else 0 and each radix pass re-reads the estimates
+// from global memory.  Spow2 is a power of two >= the number of selected
+// candidates (max(M, 64) with features, else M; K when all are selected).
+__host__ __device__ constexpr size_t probe_smem_bytes(int D, int Spow2, int Kst) {
+    return (size_t)D * 4 + (size_t)((Kst + 1) & ~1) * 4 + (size_t)Spow2 * 8 + 256 * 4 + 64;
 }
 // probe_fallback_kernel: q[D] | sort keys u64 [Kpow2]
 __host__ __device__ constexpr size_t probe_fallback_smem_bytes(int D, int Kpow2) {
@@ -125,12 +129,19 @@ __global__ void __launch_bounds__(kProbeThreads) probe_kernel(ProbeArgs a) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int K = a.K, D = a.D;
     float* qs = reinterpret_cast<float*>(smem_raw);
-    uint64_t* sk = reinterpret_cast<uint64_t*>(qs + D);
+    uint32_t* ks = reinterpret_cast<uint32_t*>(qs + D);
+    const int Kst = a.stage_keys ? (K + 1) & ~1 : 0;
+    uint64_t* sk = reinterpret_cast<uint64_t*>(ks + Kst);
     uint32_t* hist = reinterpret_cast<uint32_t*>(sk + a.Spow2);
     int* misc = reinterpret_cast<int*>(hist + 256);  // [0] digit [1] before [2] count [3] ok
 
     for (int i = tid; i < D; i += blockDim.x) qs[i] = a.qrot[(size_t)q * D + i];
     const float* aq = a.approx + (size_t)q * K;
+    if (a.stage_keys)
+        for (int c = tid; c < K; c += blockDim.x) ks[c] = order_key(__ldg(aq + c));
+    // order key of centroid c's estimate (the staged copy is read only after
+    // the barrier that follows the histogram reset)
+    auto key_of = [&](int c) -> uint32_t { return a.stage_keys ? ks[c] : order_key(__ldg(aq + c)); };
 
     const int M = a.M;
     // with features requested the 64 smallest estimates are selected as well
@@ -145,7 +156,7 @@ __global__ void __launch_bounds__(kProbeThreads) probe_kernel(ProbeArgs a) {
             for (int i = tid; i < 256; i += blockDim.x) hist[i] = 0;
             __syncthreads();
             for (int c = tid; c < K; c += blockDim.x) {
-                const uint32_t kk = order_key(__ldg(aq + c));
+                const uint32_t kk = key_of(c);
                 if ((kk & pmask) == prefix) atomicAdd(&hist[(kk >> shift) & 255u], 1u);
             }
             __syncthreads();
@@ -187,7 +198,7 @@ __global__ void __launch_bounds__(kProbeThreads) probe_kernel(ProbeArgs a) {
     if (tid == 0) misc[2] = 0;
     __syncthreads();
     for (int c = tid; c < K; c += blockDim.x) {
-        const uint32_t kk = order_key(__ldg(aq + c));
+        const uint32_t kk = key_of(c);
         if (select_all || kk < kstar) {
             const int slot = atomicAdd(&misc[2], 1);
             // id (exact distance filled below), with its estimate key when

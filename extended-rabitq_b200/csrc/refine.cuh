@@ -54,24 +54,6 @@ struct RefineArgs {
 };
 
 
-// Packed FP32 pairs (sm_100a f32x2): two independent IEEE round-to-nearest
-// operations per instruction, each equal to its scalar counterpart.
-__device__ __forceinline__ float2 ffma2(float2 a, float2 b, float2 c) {
-    uint64_t d;
-    asm("fma.rn.f32x2 %0, %1, %2, %3;"
-        : "=l"(d)
-        : "l"(*reinterpret_cast<const uint64_t*>(&a)), "l"(*reinterpret_cast<const uint64_t*>(&b)),
-          "l"(*reinterpret_cast<const uint64_t*>(&c)));
-    return *reinterpret_cast<float2*>(&d);
-}
-__device__ __forceinline__ float2 fsub2(float2 a, float2 b) {
-    uint64_t d;
-    asm("sub.rn.f32x2 %0, %1, %2;"
-        : "=l"(d)
-        : "l"(*reinterpret_cast<const uint64_t*>(&a)), "l"(*reinterpret_cast<const uint64_t*>(&b)));
-    return *reinterpret_cast<float2*>(&d);
-}
-
 // Codes of bytes (lo, lo+1) of w as exact floats: 0x4B0000vv is 2^23 + v.
 __device__ __forceinline__ float2 code_pair(uint32_t w, int lo) {
     const float2 big = make_float2(__int_as_float((int)__byte_perm(w, 0x4B000000u, 0x7540u | (uint32_t)lo)),
@@ -116,13 +98,16 @@ __device__ __forceinline__ void ex_ip_quad(const float4* __restrict__ uq4, const
 #pragma unroll
     for (int c = 0; c < NC; ++c) {
         cur[c] = __ldg(rows[c]);
-        nxt[c] = U > 1 ? __ldg(rows[c] + 4) : make_uint4(0, 0, 0, 0);
+        nxt[c] = U > 1 ? __ldg(rows[c] + 4) : cur[c];
     }
-    const int Uf = steps / SPU;  // uint4s whose steps are all real
-    for (int u = 0; u < Uf; ++u) {
+    const int Uf = steps / SPU;      // uint4s whose steps are all real
+    const int Upf = min(Uf, U - 2);  // passes that fetch the uint4 two ahead
+    int u = 0;
+#pragma unroll 3
+    for (; u < Upf; ++u) {
         uint4 nn[NC];
 #pragma unroll
-        for (int c = 0; c < NC; ++c) nn[c] = u + 2 < U ? __ldg(rows[c] + 4 * (u + 2)) : make_uint4(0, 0, 0, 0);
+        for (int c = 0; c < NC; ++c) nn[c] = __ldg(rows[c] + 4 * (u + 2));
 #pragma unroll
         for (int t = 0; t < SPU; ++t) {
             const float4 q = uq4[4 * (u * SPU + t) + r];
@@ -134,6 +119,16 @@ __device__ __forceinline__ void ex_ip_quad(const float4* __restrict__ uq4, const
             cur[c] = nxt[c];
             nxt[c] = nn[c];
         }
+    }
+    for (; u < Uf; ++u) {  // the last passes: nothing left to fetch
+#pragma unroll
+        for (int t = 0; t < SPU; ++t) {
+            const float4 q = uq4[4 * (u * SPU + t) + r];
+#pragma unroll
+            for (int c = 0; c < NC; ++c) ip_step(acc[c], q, step_word<SB>(cur[c], t));
+        }
+#pragma unroll
+        for (int c = 0; c < NC; ++c) cur[c] = nxt[c];
     }
     for (int t = 0; t < steps - Uf * SPU; ++t) {  // a partly filled last uint4
         const float4 q = uq4[4 * (Uf * SPU + t) + r];
