@@ -1189,9 +1189,9 @@ erq_status model_upload(erq_probe_model* m, const std::vector<float>& w,
 // Forward pass for inference on tensor cores (mlp.cuh): probs[B][8] of raw
 // features feats[B][320].  Training and the gradient check use mlp_forward.
 erq_status mlp_infer(const erq_probe_model* m, const float* feats, const MlpWork& w, int B,
-                     float* probs, cudaStream_t st) {
+                     float* probs, cudaStream_t st, bool xs_ready = false) {
     if (B <= 0) return ERQ_OK;
-    {
+    if (!xs_ready) {
         LaunchTimer t(kMlp, st);
         mlp_standardise_split_kernel<<<(unsigned)div_up((uint64_t)B * kMlpIn, 256), 256, 0, st>>>(
             feats, m->mean, m->stdv, w.xs, B * kMlpIn);
@@ -1215,12 +1215,10 @@ erq_status mlp_infer(const erq_probe_model* m, const float* feats, const MlpWork
         e.relu = true;
         ERQ_TRY(gemm_tc(w.hs, m->w2d, w.h2, B, kMlpHidden, 2 * kMlpHidden, e, kMlp, st));
     }
-    ERQ_TRY(mlp_mm(w.h2, kMlpHidden, 1, m->wb + kW3, 1, kMlpHidden, w.z, B, kMlpBins, kMlpHidden,
-                   m->w + kB3, false, st));
     {
         LaunchTimer t(kMlp, st);
-        mlp_softmax_xent_kernel<<<(unsigned)div_up(B, 128), 128, 0, st>>>(w.z, nullptr, B, probs,
-                                                                         nullptr, nullptr);
+        mlp_head_kernel<<<(unsigned)div_up(B, 256 / kMlpBins), 256, 0, st>>>(w.h2, m->wb + kW3,
+                                                                           m->w + kB3, B, probs);
         t.finish();
     }
     ERQ_CUDA(cudaGetLastError());
@@ -1228,12 +1226,15 @@ erq_status mlp_infer(const erq_probe_model* m, const float* feats, const MlpWork
 }
 
 // Probe features of a batch of rotated queries on the device.
+// With a model and xs, also its standardised first-layer input.
 erq_status features_device(const erq_index* idx, const Batch& b, uint64_t nprobe, float* near_d,
-                           float* feats, cudaStream_t st) {
+                           float* feats, cudaStream_t st, const erq_probe_model* m = nullptr,
+                           __nv_bfloat16* xs = nullptr) {
     ERQ_TRY(launch_probe_tc(idx, b, nprobe, st, near_d));
     LaunchTimer t(kMlp, st);
-    probe_features_kernel<<<(unsigned)b.nq, 128, 0, st>>>(b.qrot, (int)idx->D, near_d,
-                                                         (int)b.nq, feats);
+    probe_features_kernel<<<(unsigned)b.nq, 128, 0, st>>>(
+        b.qrot, (int)idx->D, near_d, (int)b.nq, feats, m && xs ? m->mean : nullptr,
+        m && xs ? m->stdv : nullptr, m ? xs : nullptr);
     t.finish();
     ERQ_CUDA(cudaGetLastError());
     return ERQ_OK;
@@ -1837,8 +1838,8 @@ static erq_status search_learned_entry(const erq_index* idx, const erq_probe_mod
         b.nq = std::min(bq, nq - q0);
         b.qrot = q + q0 * idx->D;
         const int B = (int)b.nq;
-        ERQ_TRY(features_device(idx, b, nprobe_max, near_d, feats, st));
-        ERQ_TRY(mlp_infer(m, feats, wk, B, wk.probs, st));
+        ERQ_TRY(features_device(idx, b, nprobe_max, near_d, feats, st, m, wk.xs));
+        ERQ_TRY(mlp_infer(m, feats, wk, B, wk.probs, st, true));
         {
             LaunchTimer t(kMlp, st);
             mlp_choose_nprobe_kernel<<<(unsigned)div_up(B, 128), 128, 0, st>>>(
@@ -2261,8 +2262,8 @@ erq_status plan_pipeline(erq_plan* p, uint64_t nq, const erq_plan_tuning& t, cud
     if (p->model) {
         const erq_probe_model* m = p->model;
         const int B = (int)nq;
-        ERQ_TRY(features_device(idx, b, p->nprobe_run, p->near_d, p->feats, st));
-        ERQ_TRY(mlp_infer(m, p->feats, p->wk, B, p->wk.probs, st));
+        ERQ_TRY(features_device(idx, b, p->nprobe_run, p->near_d, p->feats, st, m, p->wk.xs));
+        ERQ_TRY(mlp_infer(m, p->feats, p->wk, B, p->wk.probs, st, true));
         {
             LaunchTimer lt(kMlp, st);
             mlp_choose_nprobe_kernel<<<(unsigned)div_up(B, 128), 128, 0, st>>>(

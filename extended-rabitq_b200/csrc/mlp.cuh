@@ -93,6 +93,51 @@ __global__ void mlp_softmax_xent_kernel(const float* __restrict__ logits,
     if (loss_rows && labels) loss_rows[r] = -(z[labels[r]] - mx - logf(s));
 }
 
+// Output layer and softmax of inference in one pass: z = h2 . W3^T + b3 and
+// probs = softmax(z).  Eight threads per row (one per bin), 32 rows per block
+// of 256; each dot product runs k = 0..255 in order and the softmax sums the
+// bins in order, so the results equal mlp_matmul_kernel followed by
+// mlp_softmax_xent_kernel.  W3 (BF16 [8][256]) is staged in shared memory as
+// floats, bin-minor, so the 8 threads of a row read consecutive banks.
+__global__ void __launch_bounds__(256) mlp_head_kernel(const float* __restrict__ h2,
+                                                       const __nv_bfloat16* __restrict__ w3,
+                                                       const float* __restrict__ b3, int B,
+                                                       float* __restrict__ probs) {
+    __shared__ float ws[kMlpHidden * kMlpBins];
+    for (int i = threadIdx.x; i < kMlpHidden * kMlpBins; i += blockDim.x) {
+        const int j = i / kMlpHidden, k = i - j * kMlpHidden;
+        ws[k * kMlpBins + j] = __bfloat162float(w3[i]);
+    }
+    __syncthreads();
+    const int r = blockIdx.x * (blockDim.x / kMlpBins) + threadIdx.x / kMlpBins;
+    const int j = threadIdx.x % kMlpBins;
+    float acc = 0.f;
+    if (r < B) {
+        const float4* h = reinterpret_cast<const float4*>(h2 + (size_t)r * kMlpHidden);
+#pragma unroll 4
+        for (int k4 = 0; k4 < kMlpHidden / 4; ++k4) {
+            const float4 v = h[k4];
+            acc = fmaf(v.x, ws[(4 * k4 + 0) * kMlpBins + j], acc);
+            acc = fmaf(v.y, ws[(4 * k4 + 1) * kMlpBins + j], acc);
+            acc = fmaf(v.z, ws[(4 * k4 + 2) * kMlpBins + j], acc);
+            acc = fmaf(v.w, ws[(4 * k4 + 3) * kMlpBins + j], acc);
+        }
+    }
+    const float zj = acc + b3[j];
+    float z[kMlpBins];
+#pragma unroll
+    for (int t = 0; t < kMlpBins; ++t) z[t] = __shfl_sync(0xffffffffu, zj, t, kMlpBins);
+    float mx = z[0];
+    for (int t = 1; t < kMlpBins; ++t) mx = fmaxf(mx, z[t]);
+    float s = 0.f, ej = 0.f;
+    for (int t = 0; t < kMlpBins; ++t) {
+        const float e = expf(z[t] - mx);
+        s += e;
+        if (t == j) ej = e;
+    }
+    if (r < B) probs[(size_t)r * kMlpBins + j] = ej * (1.f / s);
+}
+
 // dH *= (H > 0), elementwise.
 __global__ void mlp_relu_grad_kernel(float* __restrict__ dH, const float* __restrict__ H, int n) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -192,9 +237,14 @@ __global__ void mlp_dup_weights_kernel(const __nv_bfloat16* __restrict__ wb,
 // a random projection, scaled by 16/||q_r||) and 64 values of its nearest
 // centroid distances e_0 <= e_1 <= ... (the tensor-core estimates, FP32
 // accurate): log(e_0 / ||q_r||^2 + 1e-12) and e_j / e_0 - 1 for j >= 1.
+// With xs, the standardised features (f - mean) / std are also written as
+// [hi | lo] BF16, the input of the first layer (mlp_standardise_split_kernel's
+// arithmetic).
 __global__ void probe_features_kernel(const float* __restrict__ qrot, int D,
                                       const float* __restrict__ near_d, int nq,
-                                      float* __restrict__ feats) {
+                                      float* __restrict__ feats, const float* __restrict__ mean,
+                                      const float* __restrict__ stdv,
+                                      __nv_bfloat16* __restrict__ xs) {
     const int q = blockIdx.x;
     if (q >= nq) return;
     __shared__ float red[8];
@@ -208,7 +258,12 @@ __global__ void probe_features_kernel(const float* __restrict__ qrot, int D,
     for (int w = 0; w < (int)(blockDim.x >> 5); ++w) qn += red[w];
     const float inv = qn > 0.f ? 16.f / sqrtf(qn) : 0.f;
     float* f = feats + (size_t)q * kMlpIn;
-    for (int i = threadIdx.x; i < kSketchDims; i += blockDim.x) f[i] = i < D ? v[i] * inv : 0.f;
+    __nv_bfloat16* xr = xs ? xs + (size_t)q * 2 * kMlpIn : nullptr;
+    auto put = [&](int c, float x) {
+        f[c] = x;
+        if (xr) split2((x - mean[c]) / stdv[c], xr + c, xr + kMlpIn + c);
+    };
+    for (int i = threadIdx.x; i < kSketchDims; i += blockDim.x) put(i, i < D ? v[i] * inv : 0.f);
     const float* d = near_d + (size_t)q * kFeatDists;
     const float d0 = d[0];
     for (int j = threadIdx.x; j < kFeatDists; j += blockDim.x) {
@@ -217,7 +272,7 @@ __global__ void probe_features_kernel(const float* __restrict__ qrot, int D,
             x = logf(d0 / fmaxf(qn, 1e-30f) + 1e-12f);
         else
             x = d0 > 0.f ? d[j] / d0 - 1.f : 0.f;
-        f[kSketchDims + j] = x;
+        put(kSketchDims + j, x);
     }
 }
 
