@@ -222,6 +222,7 @@ struct erq_index {
     __nv_bfloat16* c_split = nullptr;   // [K][3D] centroids (hi | lo | hi)
     __nv_bfloat16* pt_split = nullptr;  // [D][3D] rows of P^T (hi | lo | hi)
     float* cn = nullptr;                // [K] squared centroid norms
+    float* c_chain = nullptr;           // [K][D] centroids in chain order (probe.cuh)
     float cn_max = 0.f;
     float eps_rel = 0.f;                // distance-estimate bound (probe.cuh)
     // per-call scratch pool; keeps freed blocks for reuse by later calls
@@ -238,7 +239,7 @@ struct erq_index {
         for (void* p : {(void*)P, (void*)centroids, (void*)codes, (void*)onorm, (void*)excode,
                         (void*)xipnorm, (void*)ids, (void*)c_first_block, (void*)c_first_vec,
                         (void*)c_size, (void*)c_nblocks, (void*)c_size_rank, (void*)c_split, (void*)pt_split,
-                        (void*)cn})
+                        (void*)cn, (void*)c_chain})
             if (p) cudaFree(p);
         if (prev >= 0) cudaSetDevice(prev);
     }
@@ -410,6 +411,7 @@ erq_status load_impl(const char* path, erq_index* idx) {
     ERQ_TRY(dev_alloc(idx, &idx->c_split, K * 3 * D));
     ERQ_TRY(dev_alloc(idx, &idx->pt_split, D * 3 * D));
     ERQ_TRY(dev_alloc(idx, &idx->cn, K));
+    ERQ_TRY(dev_alloc(idx, &idx->c_chain, K * D));
     {
         std::vector<float> hp(D * D), hpt(D * D);
         ERQ_CUDA(cudaMemcpy(hp.data(), idx->P, D * D * 4, cudaMemcpyDeviceToHost));
@@ -423,6 +425,7 @@ erq_status load_impl(const char* path, erq_index* idx) {
                                                     idx->pt_split, nullptr);
             split_rows_kernel<<<(unsigned)K, 256>>>(idx->centroids, (int)K, (int)D, (int)D, false,
                                                     idx->c_split, idx->cn);
+            chain_layout_kernel<<<1184, 256>>>(idx->centroids, (int)K, (int)D, idx->c_chain);
             e = cudaGetLastError();
             if (e == cudaSuccess) e = cudaDeviceSynchronize();
         }
@@ -782,7 +785,7 @@ erq_status launch_probe_tc(const erq_index* idx, const Batch& b, uint64_t nprobe
     ProbeArgs a;
     a.approx = b.dist;
     a.qrot = b.qrot;
-    a.centroids = idx->centroids;
+    a.centroids = idx->c_chain;
     a.qn = b.qn;
     a.c_nblocks = idx->c_nblocks;
     a.cn_max = idx->cn_max;

@@ -21,7 +21,7 @@ namespace erq {
 struct ProbeArgs {
     const float* approx;      // [nq][K] distance estimates
     const float* qrot;        // [nq][D]
-    const float* centroids;   // [K][D]
+    const float* centroids;   // [K][D] in chain order (chain_pos)
     const float* qn;          // [nq] squared query norms
     const uint32_t* c_nblocks; // [K]
     float cn_max;             // largest squared centroid norm
@@ -52,14 +52,43 @@ __device__ __forceinline__ float order_key_value(uint32_t k) {
     return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
 }
 
-// Exact L2Sqr16 of (q, centroid c) by the 16 lanes of a half-warp; valid in
-// the half-warp's lane 0.
-__device__ __forceinline__ float l2sqr16_halfwarp(const float* __restrict__ q,
-                                                  const float* __restrict__ c, int D, int l) {
+// Probe copy of the centroids in accumulator-chain order: L2Sqr16's
+// accumulator l (0..15) takes dims l, l+16, l+32, ... in turn; position
+// (s * 16 + l) * 4 + i holds dim l + 16 * (4s + i).  Lane l of a half-warp then
+// reads its accumulator's next four dims as one float4 at step s, the 16
+// lanes 256 contiguous bytes.  D is a multiple of 64.
+__host__ __device__ __forceinline__ int chain_pos(int d) {
+    const int l = d & 15, j = d >> 4;
+    return ((j >> 2) * 16 + l) * 4 + (j & 3);
+}
+
+__global__ void chain_layout_kernel(const float* __restrict__ in, int rows, int D,
+                                    float* __restrict__ out) {
+    const size_t n = (size_t)rows * D;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const size_t r = i / D;
+        const int d = (int)(i - r * D);
+        out[r * D + chain_pos(d)] = in[i];
+    }
+}
+
+// Exact L2Sqr16 of (q, centroid c) by the 16 lanes l of a half-warp, both in
+// chain order: accumulator l takes t = q - c and fma(t, t, acc) over its dims
+// in ascending order, then the reduce tree; valid in the half-warp's lane 0.
+__device__ __forceinline__ float l2sqr16_chain(const float4* __restrict__ q4,
+                                               const float4* __restrict__ c4, int D, int l) {
     float acc = 0.f;
 #pragma unroll 4
-    for (int i = l; i < D; i += 16) {
-        const float t = __fsub_rn(q[i], c[i]);
+    for (int s = 0; s < (D >> 6); ++s) {
+        const float4 c = __ldg(c4 + s * 16 + l);
+        const float4 x = q4[s * 16 + l];
+        float t = __fsub_rn(x.x, c.x);
+        acc = __fmaf_rn(t, t, acc);
+        t = __fsub_rn(x.y, c.y);
+        acc = __fmaf_rn(t, t, acc);
+        t = __fsub_rn(x.z, c.z);
+        acc = __fmaf_rn(t, t, acc);
+        t = __fsub_rn(x.w, c.w);
         acc = __fmaf_rn(t, t, acc);
     }
     return tree16_sum(acc);
@@ -135,7 +164,7 @@ __global__ void __launch_bounds__(kProbeThreads) probe_kernel(ProbeArgs a) {
     uint32_t* hist = reinterpret_cast<uint32_t*>(sk + a.Spow2);
     int* misc = reinterpret_cast<int*>(hist + 256);  // [0] digit [1] before [2] count [3] ok
 
-    for (int i = tid; i < D; i += blockDim.x) qs[i] = a.qrot[(size_t)q * D + i];
+    for (int i = tid; i < D; i += blockDim.x) qs[chain_pos(i)] = a.qrot[(size_t)q * D + i];
     const float* aq = a.approx + (size_t)q * K;
     if (a.stage_keys)
         for (int c = tid; c < K; c += blockDim.x) ks[c] = order_key(__ldg(aq + c));
@@ -237,7 +266,7 @@ __global__ void __launch_bounds__(kProbeThreads) probe_kernel(ProbeArgs a) {
     for (int base = 0; base < ns; base += nhw) {
         const int i = base + hw;
         const uint32_t c = (uint32_t)(sk[i < ns ? i : 0] & 0xffffffffu);
-        const float e = l2sqr16_halfwarp(qs, a.centroids + (size_t)c * D, D, l);
+        const float e = l2sqr16_chain(reinterpret_cast<const float4*>(qs), reinterpret_cast<const float4*>(a.centroids + (size_t)c * D), D, l);
         if (l == 0 && i < ns) sk[i] = dist_key(e, c);
     }
     int nsort = 1;
@@ -273,12 +302,12 @@ __global__ void __launch_bounds__(kProbeThreads) probe_fallback_kernel(ProbeArgs
     const int K = a.K, D = a.D;
     float* qs = reinterpret_cast<float*>(smem_raw);
     uint64_t* sk = reinterpret_cast<uint64_t*>(qs + D);
-    for (int i = tid; i < D; i += blockDim.x) qs[i] = a.qrot[(size_t)q * D + i];
+    for (int i = tid; i < D; i += blockDim.x) qs[chain_pos(i)] = a.qrot[(size_t)q * D + i];
     __syncthreads();
     const int hw = tid >> 4, l = tid & 15, nhw = blockDim.x >> 4;
     for (int base = 0; base < K; base += nhw) {
         const int c = base + hw;
-        const float e = l2sqr16_halfwarp(qs, a.centroids + (size_t)min(c, K - 1) * D, D, l);
+        const float e = l2sqr16_chain(reinterpret_cast<const float4*>(qs), reinterpret_cast<const float4*>(a.centroids + (size_t)min(c, K - 1) * D), D, l);
         if (l == 0 && c < K) sk[c] = dist_key(e, (uint32_t)c);
     }
     __syncthreads();
