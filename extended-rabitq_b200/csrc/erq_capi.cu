@@ -617,8 +617,9 @@ struct Batch {
     float* qn = nullptr;              // [nq]
     // work order (order.cuh)
     uint32_t* keys = nullptr;         // [nq * nprobe]
+    uint32_t* keys_q = nullptr;       // [nq]
     uint32_t* buckets = nullptr;      // [K + 1] pair sort; ends of each cluster's run after it
-    uint32_t* buckets_q = nullptr;    // [K + 1] query sort
+    uint32_t* buckets_q = nullptr;    // [K + 1] query sort, right after buckets
     uint32_t* order_pairs = nullptr;  // [nq * nprobe]
     uint32_t* order_q = nullptr;      // [nq]
     float* bmin = nullptr;            // smallest lower bound per scanned block (S / 32 entries)
@@ -648,8 +649,9 @@ erq_status alloc_batch(Alloc& s, const erq_index* idx, uint64_t nq, uint64_t npr
     ERQ_TRY(s.alloc(&b.qsplit, nq * 3 * idx->D));
     ERQ_TRY(s.alloc(&b.qn, nq));
     ERQ_TRY(s.alloc(&b.keys, nq * nprobe));
-    ERQ_TRY(s.alloc(&b.buckets, idx->K + 1));
-    ERQ_TRY(s.alloc(&b.buckets_q, idx->K + 1));
+    ERQ_TRY(s.alloc(&b.keys_q, nq));
+    ERQ_TRY(s.alloc(&b.buckets, 2 * (idx->K + 1)));
+    b.buckets_q = b.buckets + idx->K + 1;
     ERQ_TRY(s.alloc(&b.order_pairs, nq * nprobe));
     ERQ_TRY(s.alloc(&b.order_q, nq));
     ERQ_TRY(s.alloc(&b.bmin, nq * idx->top_blocks[nprobe]));
@@ -657,59 +659,37 @@ erq_status alloc_batch(Alloc& s, const erq_index* idx, uint64_t nq, uint64_t npr
     return ERQ_OK;
 }
 
-// Counting sort of keys[0, n) over K + 1 buckets into order; afterwards
-// buckets[c] is the end of bucket c's run (order.cuh).
-erq_status bucket_sort(const erq_index* idx, const uint32_t* keys, uint32_t n, uint32_t* buckets,
-                       uint32_t* order, cudaStream_t st) {
+// Both work orders at once: (query, probe) pairs by cluster id (or by the
+// cluster's size rank) into b.order_pairs, runs delimited by b.buckets (pairs
+// a per-query probe count leaves out go last), and queries by the size rank
+// of their nearest cluster into b.order_q.  One memset and three kernels.
+erq_status order_both(const erq_index* idx, const Batch& b, uint64_t nprobe, cudaStream_t st,
+                      const int* q_nprobe, bool pairs_by_size) {
+    const uint64_t pairs = b.nq * nprobe;
     const uint32_t nb = (uint32_t)idx->K + 1;
-    ERQ_CUDA(cudaMemsetAsync(buckets, 0, nb * sizeof(uint32_t), st));
-    if (n == 0) return ERQ_OK;
+    ERQ_CUDA(cudaMemsetAsync(b.buckets, 0, 2ull * nb * sizeof(uint32_t), st));
+    if (pairs == 0) return ERQ_OK;
+    const unsigned grid = (unsigned)div_up(pairs, 256);
     {
         LaunchTimer t(kOrder, st);
-        bucket_count_kernel<<<(unsigned)div_up(n, 256), 256, 0, st>>>(keys, n, buckets);
+        order_keys_count_kernel<<<grid, 256, 0, st>>>(
+            b.probe_cid, (uint32_t)pairs, (uint32_t)b.nq, (int)nprobe, q_nprobe, (uint32_t)idx->K,
+            pairs_by_size, idx->c_size_rank, b.keys, b.buckets, b.keys_q, b.buckets_q);
         t.finish();
     }
     {
         LaunchTimer t(kOrder, st);
-        bucket_scan_kernel<<<1, kBucketScanThreads, 0, st>>>(buckets, nb);
+        bucket_scan_kernel<<<2, kBucketScanThreads, 0, st>>>(b.buckets, b.buckets_q, nb);
         t.finish();
     }
     {
         LaunchTimer t(kOrder, st);
-        bucket_scatter_kernel<<<(unsigned)div_up(n, 256), 256, 0, st>>>(keys, n, buckets, order);
+        bucket_scatter2_kernel<<<grid, 256, 0, st>>>(b.keys, (uint32_t)pairs, b.buckets, b.order_pairs,
+                                                     b.keys_q, (uint32_t)b.nq, b.buckets_q, b.order_q);
         t.finish();
     }
     ERQ_CUDA(cudaGetLastError());
     return ERQ_OK;
-}
-
-// (query, probe) pairs by cluster into b.order_pairs (pairs a per-query probe
-// count leaves out go last), runs delimited by b.buckets.
-erq_status order_pairs(const erq_index* idx, const Batch& b, uint64_t nprobe, cudaStream_t st,
-                       const int* q_nprobe, bool by_size = false) {
-    const uint64_t pairs = b.nq * nprobe;
-    if (pairs == 0) return ERQ_OK;
-    {
-        LaunchTimer t(kOrder, st);
-        pair_keys_kernel<<<(unsigned)div_up(pairs, 256), 256, 0, st>>>(
-            b.probe_cid, (uint32_t)pairs, (int)nprobe, q_nprobe, (uint32_t)idx->K,
-            by_size ? idx->c_size_rank : nullptr, b.keys);
-        t.finish();
-    }
-    return bucket_sort(idx, b.keys, (uint32_t)pairs, b.buckets, b.order_pairs, st);
-}
-
-// queries by their nearest cluster into b.order_q.
-erq_status order_queries(const erq_index* idx, const Batch& b, uint64_t nprobe, cudaStream_t st) {
-    if (b.nq == 0) return ERQ_OK;
-    {
-        LaunchTimer t(kOrder, st);
-        query_keys_kernel<<<(unsigned)div_up(b.nq, 256), 256, 0, st>>>(b.probe_cid, (uint32_t)b.nq,
-                                                                      (int)nprobe, idx->c_size_rank,
-                                                                      b.keys);
-        t.finish();
-    }
-    return bucket_sort(idx, b.keys, (uint32_t)b.nq, b.buckets_q, b.order_q, st);
 }
 
 // Both orders for the per-pair scan and the refinement.  Small batches gain
@@ -718,8 +698,7 @@ bool launch_order(const erq_index* idx, const Batch& b, uint64_t nprobe, cudaStr
                   const int* q_nprobe, erq_status* err) {
     *err = ERQ_OK;
     if (b.nq * nprobe < 1024 || !b.order_pairs) return false;
-    if ((*err = order_pairs(idx, b, nprobe, st, q_nprobe, true)) != ERQ_OK) return false;
-    if ((*err = order_queries(idx, b, nprobe, st)) != ERQ_OK) return false;
+    if ((*err = order_both(idx, b, nprobe, st, q_nprobe, true)) != ERQ_OK) return false;
     return true;
 }
 
@@ -2211,7 +2190,7 @@ erq_status launch_scan_batched(erq_plan* p, uint64_t nq, const erq_plan_tuning& 
     }
     {
         LaunchTimer lt(kOrder, st);
-        bucket_scan_kernel<<<1, kBucketScanThreads, 0, st>>>(p->item_off, (uint32_t)K + 1);
+        bucket_scan_kernel<<<1, kBucketScanThreads, 0, st>>>(p->item_off, p->item_off, (uint32_t)K + 1);
         lt.finish();
     }
     ERQ_CUDA(cudaMemsetAsync(p->counter, 0, sizeof(uint32_t), st));
@@ -2279,8 +2258,7 @@ erq_status plan_pipeline(erq_plan* p, uint64_t nq, const erq_plan_tuning& t, cud
     } else {
         ERQ_TRY(launch_probe_tc(idx, b, p->nprobe_run, st));
     }
-    ERQ_TRY(order_pairs(idx, b, p->nprobe_run, st, qnp));
-    ERQ_TRY(order_queries(idx, b, p->nprobe_run, st));
+    ERQ_TRY(order_both(idx, b, p->nprobe_run, st, qnp, false));
     ERQ_TRY(launch_scan_batched(p, nq, t, st));
     ERQ_TRY(launch_refine(idx, b, p->nprobe_run, p->k, p->ids, p->dists, st, qnp, b.order_q));
     return ERQ_OK;

@@ -4,14 +4,21 @@
 // ranks all K centroids by L2Sqr16 (inc/utils/space.hpp:18-39) and keeps the
 // nprobe nearest.  Here the GEMM of gemm.cuh gives an estimate a_c of every
 // squared distance with |a_c - true_c| <= eps_a, and one thread block per query
-//   1. selects the M smallest estimates (radix select on order-preserving
-//      keys): candidate set S, and A = the (M+1)-th smallest estimate;
+//   1. selects the Msel smallest estimates (radix select on order-preserving
+//      keys) and sorts them by estimate; A = the (Msel+1)-th smallest estimate
+//      bounds every centroid outside the list;
 //   2. recomputes the exact reference value e_c (16 ordered FMA chains + the
-//      reduce tree) for every c in S and sorts S by (e_c, c);
-//   3. checks A - eps > e_(nprobe), eps = eps_a + the reference's own rounding
-//      bound.  Any centroid outside S then has e_c >= A - eps > e_(nprobe), so
-//      the first nprobe of S are exactly the reference's choice (ties by id);
-//   4. if the check fails, computes e_c for all K centroids and sorts them all.
+//      reduce tree) of the first n = nprobe of the list, e_max = their largest;
+//   3. finds the first list position P >= n whose estimate satisfies
+//      a_P - eps > e_max, eps = eps_a + the reference's own rounding bound.
+//      Every centroid at or after P (and outside the list) then has
+//      e_c >= a_c - eps > e_max >= the n-th smallest exact distance, so the
+//      exact top n lie in the first P: those are recomputed and sorted by
+//      (e_c, c);
+//   4. when no list position qualifies, all Msel are recomputed and the cut is
+//      checked as A - eps > e_(n); if that fails too, probe_fallback_kernel
+//      computes e_c for all K centroids and sorts them all.
+// Usually P is a few positions past n, so few centroid rows are read.
 #pragma once
 
 #include "common.cuh"
@@ -111,6 +118,53 @@ __device__ __forceinline__ void block_bitonic_sort(uint64_t* keys, int n) {
             __syncthreads();
         }
     }
+}
+
+// Ascending sort of keys[0..n), n <= 64, by warp 0's lanes (element i in
+// lane i % 32, register i / 32), bitonic network over 32 or 64 elements with
+// the missing ones as ~0; no block barrier.
+__device__ __forceinline__ void warp_sort64(uint64_t* keys, int n, int lane) {
+    const int N = n <= 32 ? 32 : 64;
+    uint64_t a = lane < n ? keys[lane] : ~0ull;
+    uint64_t b = lane + 32 < n ? keys[lane + 32] : ~0ull;
+    for (int size = 2; size <= N; size <<= 1) {
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            if (stride == 32) {  // size 64: the pair sits in one lane
+                const uint64_t lo = a < b ? a : b, hi = a < b ? b : a;
+                a = lo;
+                b = hi;
+            } else {
+                const bool low = (lane & stride) == 0;
+                const uint64_t pa = __shfl_xor_sync(0xffffffffu, a, stride);
+                const bool upa = (lane & size) == 0;
+                a = (low == upa) ? (a < pa ? a : pa) : (a < pa ? pa : a);
+                if (N == 64) {
+                    const uint64_t pb = __shfl_xor_sync(0xffffffffu, b, stride);
+                    const bool upb = ((lane + 32) & size) == 0;
+                    b = (low == upb) ? (b < pb ? b : pb) : (b < pb ? pb : b);
+                }
+            }
+        }
+    }
+    if (lane < n) keys[lane] = a;
+    if (lane + 32 < n) keys[lane + 32] = b;
+}
+
+// Ascending sort of keys[0..n) by the whole block (called by every thread,
+// after the keys are visible to all; returns synchronised).  Up to 64 keys
+// warp 0 sorts them in registers; more are padded with ~0 to a power of two
+// (keys must hold that many) and sorted by the block.
+__device__ __forceinline__ void sort_prefix(uint64_t* keys, int n) {
+    if (n <= 64) {
+        if (threadIdx.x < 32) warp_sort64(keys, n, threadIdx.x);
+        __syncthreads();
+        return;
+    }
+    int np = 1;
+    while (np < n) np <<= 1;
+    for (int i = n + threadIdx.x; i < np; i += blockDim.x) keys[i] = ~0ull;
+    __syncthreads();
+    block_bitonic_sort(keys, np);
 }
 
 // Shared memory of probe_kernel: q[D] | order keys u32 [Kst] | sort keys u64
@@ -223,65 +277,68 @@ __global__ void __launch_bounds__(kProbeThreads) probe_kernel(ProbeArgs a) {
         }
         kstar = prefix;
     }
-    // candidates: every centroid whose estimate is below the (Msel+1)-th
+    // candidates: every centroid whose estimate is below the (Msel+1)-th,
+    // keyed by (estimate, id)
     if (tid == 0) misc[2] = 0;
     __syncthreads();
     for (int c = tid; c < K; c += blockDim.x) {
         const uint32_t kk = key_of(c);
         if (select_all || kk < kstar) {
             const int slot = atomicAdd(&misc[2], 1);
-            // id (exact distance filled below), with its estimate key when
-            // the features need the estimates in order
-            sk[slot] = a.near_d ? (((uint64_t)kk << 32) | (uint64_t)c) : (uint64_t)c;
+            sk[slot] = ((uint64_t)kk << 32) | (uint64_t)c;
         }
     }
     __syncthreads();
-    int ns = misc[2];
-    uint32_t akey = kstar;        // estimate bound for the centroids not recomputed
-    bool truncated = !select_all;
+    const int ns = misc[2];
+    const bool truncated = !select_all;  // A = value of kstar bounds the rest
+    sort_prefix(sk, ns);
     if (a.near_d) {
-        // the 64 smallest estimates, in order, are the distance features; the
-        // first M of them are recomputed exactly and the (M+1)-th bounds the rest
-        int nsort0 = 1;
-        while (nsort0 < ns) nsort0 <<= 1;
-        for (int i = ns + tid; i < nsort0; i += blockDim.x) sk[i] = ~0ull;
-        __syncthreads();
-        block_bitonic_sort(sk, nsort0);
+        // the 64 smallest estimates, in order, are the distance features
         for (int j = tid; j < kProbeFeatRank; j += blockDim.x)
             a.near_d[(size_t)q * kProbeFeatRank + j] =
                 ns > 0 ? order_key_value((uint32_t)(sk[j < ns ? j : ns - 1] >> 32)) : 0.f;
-        if (ns > M) {
-            akey = (uint32_t)(sk[M] >> 32);
-            ns = M;
-            truncated = true;
-        } else {
-            truncated = false;
-        }
-        __syncthreads();
-        for (int i = tid; i < ns; i += blockDim.x) sk[i] &= 0xffffffffull;
-        __syncthreads();
     }
-    // exact distances of the candidates, 16 per pass (one per half-warp)
+    const int n = min(a.check_rank, ns);
+    const float eps = a.eps_rel * (a.qn[q] + a.cn_max);
+    if (tid == 0) {
+        misc[4] = 0;   // largest exact distance of the first n (float bits)
+        misc[5] = ns;  // P
+    }
+    __syncthreads();
+    // exact distances of list positions [lo, hi), one half-warp each; a warp
+    // with no position in a pass skips it, a half-warp past the end repeats
+    // its neighbour (both halves take part in the reduce's shuffles)
     const int hw = tid >> 4, l = tid & 15, nhw = blockDim.x >> 4;
-    for (int base = 0; base < ns; base += nhw) {
-        const int i = base + hw;
-        const uint32_t c = (uint32_t)(sk[i < ns ? i : 0] & 0xffffffffu);
-        const float e = l2sqr16_chain(reinterpret_cast<const float4*>(qs), reinterpret_cast<const float4*>(a.centroids + (size_t)c * D), D, l);
-        if (l == 0 && i < ns) sk[i] = dist_key(e, c);
-    }
-    int nsort = 1;
-    while (nsort < ns) nsort <<= 1;
+    auto exact_range = [&](int lo, int hi, bool track_max) {
+        for (int base = lo; base < hi; base += nhw) {
+            const int i0 = base + 2 * warp;
+            if (i0 >= hi) continue;  // uniform per warp
+            const int i = base + hw;
+            const uint32_t c = (uint32_t)(sk[i < hi ? i : i0] & 0xffffffffu);
+            const float e = l2sqr16_chain(reinterpret_cast<const float4*>(qs), reinterpret_cast<const float4*>(a.centroids + (size_t)c * D), D, l);
+            if (l == 0 && i < hi) {
+                sk[i] = dist_key(e, c);
+                if (track_max) atomicMax(reinterpret_cast<unsigned*>(&misc[4]), __float_as_uint(e));
+            }
+        }
+    };
+    exact_range(0, n, true);
     __syncthreads();
-    for (int i = ns + tid; i < nsort; i += blockDim.x) sk[i] = ~0ull;
+    const float e_max = __uint_as_float((uint32_t)misc[4]);
+    for (int i = n + tid; i < ns; i += blockDim.x)
+        if (order_key_value((uint32_t)(sk[i] >> 32)) - eps > e_max) atomicMin(&misc[5], i);
     __syncthreads();
-    block_bitonic_sort(sk, nsort);
-    // bound check; a query that fails it goes to probe_fallback_kernel
+    const int P = misc[5];
+    const bool proven = P < ns || !truncated || (order_key_value(kstar) - eps > e_max);
+    exact_range(n, P, false);
+    __syncthreads();
+    sort_prefix(sk, P);
+    // a query whose cut is not proven goes to probe_fallback_kernel
     if (tid == 0) {
         bool ok = ns >= a.check_rank;
-        if (ok && truncated) {
+        if (ok && !proven) {
             const float e_n = __uint_as_float((uint32_t)(sk[a.check_rank - 1] >> 32));
-            const float eps = a.eps_rel * (a.qn[q] + a.cn_max);
-            const float A = order_key_value(akey);
+            const float A = order_key_value(kstar);
             ok = (A - eps > e_n) && (e_n == e_n);
         }
         a.fallback_flag[q] = ok ? 0u : 1u;
