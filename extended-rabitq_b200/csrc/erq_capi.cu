@@ -455,9 +455,36 @@ erq_status load_impl(const char* path, erq_index* idx) {
 
 // ------------------------------------------------------------ pipeline
 size_t scan_smem_bytes(int D) { return 256 + (size_t)(D / 64) * 512 + (size_t)D * 4 + 64; }
-size_t refine_smem_bytes(int D, int k) {
+size_t refine_smem_bytes(int D, int k, bool wide = false) {
     const int kpad = (k + 31) & ~31;
-    return refine_smem_bytes_per_query(D, kpad);
+    return refine_smem_bytes_per_query(D, kpad, wide ? kWideWindowBlocks : kWindowBlocks);
+}
+
+// Streaming multiprocessors of the current device (cached per device).
+int device_sms() {
+    static int sms[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+    if (!sms[dev]) {
+        int n = 0;
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0)
+            n = 148;
+        sms[dev] = n;
+    }
+    return sms[dev];
+}
+
+// The limits cover the largest k, so a later call with a smaller k never
+// lowers them below what a captured graph's launches need.
+template <int EX>
+erq_status configure_refine(int D) {
+    ERQ_CUDA(cudaFuncSetAttribute(refine_kernel<EX, 4, kWindowBlocks>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)refine_smem_bytes(D, kMaxTopK)));
+    ERQ_CUDA(cudaFuncSetAttribute(refine_kernel<EX, kWideWarps, kWideWindowBlocks>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)refine_smem_bytes(D, kMaxTopK, true)));
+    return ERQ_OK;
 }
 int next_pow2(int x) {
     int p = 1;
@@ -475,13 +502,12 @@ erq_status configure_kernels(int D, int K, int k) {
                                   (int)probe_smem_bytes(D, kp2, K <= kProbeStageKeys ? K : 0)));
     ERQ_CUDA(cudaFuncSetAttribute(probe_fallback_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)probe_fallback_smem_bytes(D, kp2)));
-    const int rs = (int)refine_smem_bytes(D, k);
-    ERQ_CUDA(cudaFuncSetAttribute(refine_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, rs));
-    ERQ_CUDA(cudaFuncSetAttribute(refine_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, rs));
-    ERQ_CUDA(cudaFuncSetAttribute(refine_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, rs));
-    ERQ_CUDA(cudaFuncSetAttribute(refine_kernel<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, rs));
-    ERQ_CUDA(cudaFuncSetAttribute(refine_kernel<7>, cudaFuncAttributeMaxDynamicSharedMemorySize, rs));
-    ERQ_CUDA(cudaFuncSetAttribute(refine_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, rs));
+    ERQ_TRY(configure_refine<2>(D));
+    ERQ_TRY(configure_refine<3>(D));
+    ERQ_TRY(configure_refine<4>(D));
+    ERQ_TRY(configure_refine<6>(D));
+    ERQ_TRY(configure_refine<7>(D));
+    ERQ_TRY(configure_refine<8>(D));
     return ERQ_OK;
 }
 
@@ -886,17 +912,27 @@ erq_status launch_refine(const erq_index* idx, const Batch& b, uint64_t nprobe, 
     a.nprobe = (int)nprobe;
     a.k = (int)k;
     const unsigned grid = (unsigned)b.nq;
-    const size_t smem = refine_smem_bytes(a.D, a.k);
+    // a batch with no more queries than SMs runs one wide block per query
+    const bool wide = b.nq <= (uint64_t)device_sms();
+    const size_t smem = refine_smem_bytes(a.D, a.k, wide);
     LaunchTimer t(kRefine, st);
+#define ERQ_REFINE_CASE(X)                                                                          \
+    case X:                                                                                         \
+        if (wide)                                                                                   \
+            refine_kernel<X, kWideWarps, kWideWindowBlocks><<<grid, kWideWarps * 32, smem, st>>>(a); \
+        else                                                                                        \
+            refine_kernel<X, 4, kWindowBlocks><<<grid, kRefineThreads, smem, st>>>(a);              \
+        break;
     switch (idx->EX) {
-        case 2: refine_kernel<2><<<grid, kRefineThreads, smem, st>>>(a); break;
-        case 3: refine_kernel<3><<<grid, kRefineThreads, smem, st>>>(a); break;
-        case 4: refine_kernel<4><<<grid, kRefineThreads, smem, st>>>(a); break;
-        case 6: refine_kernel<6><<<grid, kRefineThreads, smem, st>>>(a); break;
-        case 7: refine_kernel<7><<<grid, kRefineThreads, smem, st>>>(a); break;
-        case 8: refine_kernel<8><<<grid, kRefineThreads, smem, st>>>(a); break;
+        ERQ_REFINE_CASE(2)
+        ERQ_REFINE_CASE(3)
+        ERQ_REFINE_CASE(4)
+        ERQ_REFINE_CASE(6)
+        ERQ_REFINE_CASE(7)
+        ERQ_REFINE_CASE(8)
         default: return fail(ERQ_ERR_FORMAT, "bad EX");
     }
+#undef ERQ_REFINE_CASE
     t.finish();
     ERQ_CUDA(cudaGetLastError());
     return ERQ_OK;

@@ -149,13 +149,14 @@ __device__ __forceinline__ void ex_ip_quad(const float4* __restrict__ uq4, const
 
 constexpr int kRefineThreads = 128;     // 4 warps per query
 constexpr int kWindowBlocks = 16;       // blocks whose candidates are refined together
-constexpr int kWindowLanes = kWindowBlocks * 32;
+// Wide form for small batches (a query per SM): more warps, longer windows.
+constexpr int kWideWarps = 32;
+constexpr int kWideWindowBlocks = 128;
 
 // Shared memory of one block: unit_q[D] | per window lane: lb, ipq, onorm,
-// ex_dist, id, list | pool_d[kpad] | pool_id[kpad] | misc
-__host__ __device__ constexpr size_t refine_smem_bytes_per_query(int D, int kpad) {
-    return (size_t)D * 4 + (size_t)kWindowLanes * (5 * 4 + 2) + (size_t)kpad * 8 + 64 + 128 +
-           kWindowBlocks * 4;
+// ex_dist, id, list | pool_d[kpad] | pool_id[kpad] | misc | window blocks
+__host__ __device__ constexpr size_t refine_smem_bytes_per_query(int D, int kpad, int wb) {
+    return (size_t)D * 4 + (size_t)wb * 32 * (5 * 4 + 2) + (size_t)kpad * 8 + 64 + 128 + (size_t)wb * 4;
 }
 
 // Order key: ascending distance (-0 equal to +0, as float compares see it);
@@ -272,16 +273,19 @@ __device__ __forceinline__ void pool_merge_block(float* pool_d, uint32_t* pool_i
     distk = size == k ? pool_d[k - 1] : FLT_MAX;
 }
 
-// One block of 4 warps per query.  Per window of up to 16 blocks of the
-// current cluster: every warp computes the lower bounds of 4 blocks and lists
+// One block of WARPS warps per query (4, or 32 in the wide form).  Per window
+// of up to WB blocks of the current cluster (16, or 128): every warp computes
+// the lower bounds of WB / WARPS = 4 blocks and lists
 // the lanes below the threshold as it stands at the window's start (a superset
 // of the exact candidates, because the threshold only falls); the 32 quads
-// compute the listed candidates' exact distances (warps without a candidate
+// compute the listed candidates' exact distances (8 quads per warp; warps without a candidate
 // skip the round); warp 0 then replays the window in the reference's order -
 // each block's mask against the threshold at that block's start, the block's
 // candidates merged into the pool as inserting them in lane order would.
-template <int EX>
-__global__ void __launch_bounds__(kRefineThreads, 8) refine_kernel(RefineArgs a) {
+template <int EX, int WARPS, int WB>
+__global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 8 : 1) refine_kernel(RefineArgs a) {
+    constexpr int kThreads = WARPS * 32, kLanes = WB * 32;
+    static_assert(WB % WARPS == 0 && kLanes <= 65536, "window lanes are listed as u16");
     extern __shared__ __align__(16) uint8_t smem_raw[];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int q = a.order ? (int)a.order[blockIdx.x] : (int)blockIdx.x;
@@ -289,12 +293,12 @@ __global__ void __launch_bounds__(kRefineThreads, 8) refine_kernel(RefineArgs a)
     const int kpad = (k + 31) & ~31;
     float* uq = reinterpret_cast<float*>(smem_raw);
     float* w_lb = uq + D;
-    float* w_ipq = w_lb + kWindowLanes;
-    float* w_on = w_ipq + kWindowLanes;
-    float* w_ed = w_on + kWindowLanes;
-    uint32_t* w_id = reinterpret_cast<uint32_t*>(w_ed + kWindowLanes);
-    uint16_t* w_list = reinterpret_cast<uint16_t*>(w_id + kWindowLanes);
-    float* pool_d = reinterpret_cast<float*>(w_list + kWindowLanes);
+    float* w_ipq = w_lb + kLanes;
+    float* w_on = w_ipq + kLanes;
+    float* w_ed = w_on + kLanes;
+    uint32_t* w_id = reinterpret_cast<uint32_t*>(w_ed + kLanes);
+    uint16_t* w_list = reinterpret_cast<uint16_t*>(w_id + kLanes);
+    float* pool_d = reinterpret_cast<float*>(w_list + kLanes);
     uint32_t* pool_id = reinterpret_cast<uint32_t*>(pool_d + kpad);
     int* misc = reinterpret_cast<int*>(pool_id + kpad);  // [0] list count [1] pool size
     float* s_distk = reinterpret_cast<float*>(misc + 2);
@@ -340,8 +344,8 @@ __global__ void __launch_bounds__(kRefineThreads, 8) refine_kernel(RefineArgs a)
             const int filled = misc[1];
             // While the pool is filling every lane is a candidate: take just
             // enough blocks to fill it, so few lanes are refined in vain.
-            const int want = filled < k ? min(kWindowBlocks, max(1, (k - filled + 31) / 32))
-                                        : kWindowBlocks;
+            const int want = filled < k ? min(WB, max(1, (k - filled + 31) / 32))
+                                        : WB;
             __syncthreads();
             // warp 0 picks the window: the next `want` blocks from wb whose
             // smallest lower bound is below the threshold (a block above it
@@ -377,8 +381,8 @@ __global__ void __launch_bounds__(kRefineThreads, 8) refine_kernel(RefineArgs a)
             const uint32_t wnext = (uint32_t)misc[6];
             // lower bounds and the candidate superset, 4 blocks per warp
 #pragma unroll
-            for (int i = 0; i < kWindowBlocks / (kRefineThreads / 32); ++i) {
-                const int b = warp * (kWindowBlocks / (kRefineThreads / 32)) + i;
+            for (int i = 0; i < WB / (kThreads / 32); ++i) {
+                const int b = warp * (WB / (kThreads / 32)) + i;
                 if (b < nbw) {  // uniform per warp
                     const uint32_t blk = w_blk[b];
                     const float ipq = __fmul_rn(__int2float_rn(S[32 * blk + lane]), delta);
@@ -428,23 +432,23 @@ __global__ void __launch_bounds__(kRefineThreads, 8) refine_kernel(RefineArgs a)
                 __syncthreads();
             }
             // refine the listed candidates: quad g (lanes 4g..4g+3) takes two
-            // per round while at least 33 remain, else one; within a warp
+            // per round while more than one per quad remain, else one; within a warp
             // that has work, quads past the end repeat the list's first so
             // the warp stays converged
             {
                 const int g = tid >> 2, r = tid & 3;
                 const float4* uq4 = reinterpret_cast<const float4*>(uq);
                 for (int base = 0; base < cnt;) {
-                    const int two = cnt - base > kRefineThreads / 4;
-                    const int step = two ? kRefineThreads / 2 : kRefineThreads / 4;
+                    const int two = cnt - base > kThreads / 4;
+                    const int step = two ? kThreads / 2 : kThreads / 4;
                     // per warp: skip when none of its slots holds a candidate,
                     // one candidate per quad when its second slots are empty
                     if (base + 8 * warp >= cnt) {
                         base += step;
                         continue;
                     }
-                    const int wtwo = two && base + kRefineThreads / 4 + 8 * warp < cnt;
-                    const int i0 = base + g, i1 = base + kRefineThreads / 4 + g;
+                    const int wtwo = two && base + kThreads / 4 + 8 * warp < cnt;
+                    const int i0 = base + g, i1 = base + kThreads / 4 + g;
                     const int s0 = w_list[i0 < cnt ? i0 : 0];
                     const int s1 = w_list[wtwo && i1 < cnt ? i1 : 0];
                     const size_t pos0 = (size_t)first_vec + 32 * w_blk[s0 >> 5] + (s0 & 31);
