@@ -880,9 +880,12 @@ erq_status launch_scan(const erq_index* idx, const Batch& b, uint64_t nprobe, cu
     return ERQ_OK;
 }
 
+// refine_warps: 4 or kWideWarps chooses the form; 0 takes the wide one when
+// the batch has no more queries than SMs.
 erq_status launch_refine(const erq_index* idx, const Batch& b, uint64_t nprobe, uint64_t k,
                          uint32_t* out_ids, float* out_dists, cudaStream_t st,
-                         const int* q_nprobe = nullptr, const uint32_t* order = nullptr) {
+                         const int* q_nprobe = nullptr, const uint32_t* order = nullptr,
+                         int refine_warps = 0) {
     RefineArgs a;
     a.order = order;
     a.bmin = b.bmin;
@@ -912,8 +915,7 @@ erq_status launch_refine(const erq_index* idx, const Batch& b, uint64_t nprobe, 
     a.nprobe = (int)nprobe;
     a.k = (int)k;
     const unsigned grid = (unsigned)b.nq;
-    // a batch with no more queries than SMs runs one wide block per query
-    const bool wide = b.nq <= (uint64_t)device_sms();
+    const bool wide = refine_warps ? refine_warps == kWideWarps : b.nq <= (uint64_t)device_sms();
     const size_t smem = refine_smem_bytes(a.D, a.k, wide);
     LaunchTimer t(kRefine, st);
 #define ERQ_REFINE_CASE(X)                                                                          \
@@ -2189,6 +2191,7 @@ erq_plan_tuning default_tuning(uint64_t nq) {
     t.queries_per_item = nq >= 1024 ? 4 : 1;
     t.blocks_per_item = 16;
     t.warps = nq >= 1024 ? 8 : 4;
+    t.refine_warps = 0;
     return t;
 }
 
@@ -2211,7 +2214,8 @@ erq_plan_tuning plan_tuning(const erq_plan* p, uint64_t nq) {
 bool tuning_valid(const erq_plan_tuning& t) {
     bool shape = false;
     for (auto& sh : kScanShapes) shape |= (int)t.queries_per_item == sh.qb && (int)t.warps == sh.warps;
-    return shape && t.blocks_per_item >= 1 && t.blocks_per_item <= 4096;
+    return shape && t.blocks_per_item >= 1 && t.blocks_per_item <= 4096 &&
+           (t.refine_warps == 0 || t.refine_warps == 4 || t.refine_warps == (uint32_t)kWideWarps);
 }
 
 erq_status launch_scan_batched(erq_plan* p, uint64_t nq, const erq_plan_tuning& t, cudaStream_t st) {
@@ -2296,7 +2300,8 @@ erq_status plan_pipeline(erq_plan* p, uint64_t nq, const erq_plan_tuning& t, cud
     }
     ERQ_TRY(order_both(idx, b, p->nprobe_run, st, qnp, false));
     ERQ_TRY(launch_scan_batched(p, nq, t, st));
-    ERQ_TRY(launch_refine(idx, b, p->nprobe_run, p->k, p->ids, p->dists, st, qnp, b.order_q));
+    ERQ_TRY(launch_refine(idx, b, p->nprobe_run, p->k, p->ids, p->dists, st, qnp, b.order_q,
+                          (int)t.refine_warps));
     return ERQ_OK;
 }
 
@@ -2466,6 +2471,28 @@ erq_status erq_plan_autotune(erq_plan* p, const float* queries, uint64_t n, int 
         }
         if (s != ERQ_OK) break;
     }
+    // both refinement forms with the chosen tile (the auto choice is one of them)
+    for (uint32_t rw : {4u, (uint32_t)kWideWarps}) {
+        if (s != ERQ_OK) break;
+        erq_plan_tuning t = bt;
+        t.refine_warps = rw;
+        if ((s = plan_pipeline(p, n, t, st)) != ERQ_OK) break;  // warm-up
+        float ms = 1e30f;
+        for (int r = 0; r < std::max(1, reps); ++r) {
+            cudaEventRecord(e0, st);
+            if ((s = plan_pipeline(p, n, t, st)) != ERQ_OK) break;
+            cudaEventRecord(e1, st);
+            cudaEventSynchronize(e1);
+            float x = 0.f;
+            cudaEventElapsedTime(&x, e0, e1);
+            ms = std::min(ms, x);
+        }
+        if (s == ERQ_OK && ms < best) {
+            best = ms;
+            bt = t;
+        }
+    }
+    if (bt.refine_warps == 0) bt.refine_warps = n <= (uint64_t)device_sms() ? kWideWarps : 4;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     ERQ_TRY(s);

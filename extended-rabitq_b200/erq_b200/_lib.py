@@ -52,11 +52,12 @@ class PlanTuning(C.Structure):
         ("queries_per_item", C.c_uint32),
         ("blocks_per_item", C.c_uint32),
         ("warps", C.c_uint32),
+        ("refine_warps", C.c_uint32),
     ]
 
     def as_dict(self):
         return {"queries_per_item": self.queries_per_item, "blocks_per_item": self.blocks_per_item,
-                "warps": self.warps}
+                "warps": self.warps, "refine_warps": self.refine_warps}
 
 
 class IndexInfo(C.Structure):

@@ -57,8 +57,10 @@ class Plan:
                                           C.byref(ms)))
         return t.as_dict(), float(ms.value)
 
-    def set_tuning(self, batch: int, queries_per_item: int, blocks_per_item: int, warps: int) -> None:
-        t = PlanTuning(queries_per_item, blocks_per_item, warps)
+    def set_tuning(self, batch: int, queries_per_item: int, blocks_per_item: int, warps: int,
+                   refine_warps: int = 0) -> None:
+        """refine_warps: 4, 32 (wide refinement form) or 0 (by batch size)."""
+        t = PlanTuning(queries_per_item, blocks_per_item, warps, refine_warps)
         check(self._lib.erq_plan_set_tuning(self._h, batch, C.byref(t)))
 
     def tuning(self, batch: int) -> dict:

@@ -162,6 +162,9 @@ typedef struct {
     uint32_t queries_per_item;  /* Q: 1, 2, 4 or 8 */
     uint32_t blocks_per_item;   /* C: cluster chunk, in 32-vector blocks */
     uint32_t warps;             /* warps per scan block: 4 or 8 (Q = 1 needs 4, Q = 8 needs 8) */
+    uint32_t refine_warps;      /* warps per refinement block: 4, 32 (the wide form, windows of
+                                   128 blocks), or 0 = 32 when the batch has no more queries
+                                   than SMs, else 4 */
 } erq_plan_tuning;
 
 /* model may be NULL (plain fixed-nprobe search); with a model, nprobe is the
@@ -174,7 +177,8 @@ ERQ_API void erq_plan_free(erq_plan* plan);
 /* Confidence and minimum probability of the learned cut-off (defaults 0.9, 0). */
 ERQ_API erq_status erq_plan_set_learned(erq_plan* plan, float confidence, float min_prob);
 /* Times every tile choice on queries[n] (host or device; best of `reps` runs
- * each) and keeps the fastest for batches of about n queries. */
+ * each), then both refinement forms with the fastest tile, and keeps the
+ * fastest for batches of about n queries. */
 ERQ_API erq_status erq_plan_autotune(erq_plan* plan, const float* queries, uint64_t n, int reps,
                                      erq_plan_tuning* chosen, float* best_ms);
 ERQ_API erq_status erq_plan_set_tuning(erq_plan* plan, uint64_t batch, const erq_plan_tuning* tuning);

@@ -107,6 +107,26 @@ def test_batch_sizes_and_graph_replays(uneven):
     plan.free()
 
 
+def test_both_refinement_forms(uneven):
+    """The 4-warp and the wide (32-warp, 128-block window) refinement give the
+    same results at batch sizes below and above the SM count, and with k up
+    to the largest the pool supports."""
+    from erq_b200 import Plan
+
+    idx, q, qr, _ = uneven
+    for k, nprobe, n in ((100, 6, 50), (100, 6, 300), (1024, 12, 40)):
+        sl = qr[:n]
+        ref_ids, ref_d = idx.search_batch(sl, k, nprobe)
+        plan = Plan(idx, max_batch=n, k=k, nprobe=nprobe)
+        for rw in (4, 32, 0):
+            plan.set_tuning(n, 2, 16, 4, rw)
+            assert plan.tuning(n)["refine_warps"] == rw
+            ids, d, _ = plan.search(sl)
+            assert (ids == ref_ids).all(), (k, n, rw)
+            assert (bits(d) == bits(ref_d)).all(), (k, n, rw)
+        plan.free()
+
+
 def test_raw_queries_and_device_buffers(uneven):
     from erq_b200 import Plan
 
@@ -135,6 +155,7 @@ def test_autotune_keeps_results(uneven):
     plan = Plan(idx, max_batch=2000, k=k, nprobe=nprobe)
     t, ms = plan.autotune(qr, reps=1)
     assert t["queries_per_item"] in (1, 2, 4, 8) and t["warps"] in (4, 8) and ms > 0
+    assert t["refine_warps"] in (4, 32)
     assert plan.tuning(2000) == t
     ref_ids, ref_d = idx.search_batch(qr, k, nprobe)
     ids, d, _ = plan.search(qr)
