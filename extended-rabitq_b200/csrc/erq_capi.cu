@@ -1253,7 +1253,7 @@ erq_status features_device(const erq_index* idx, const Batch& b, uint64_t nprobe
     ERQ_TRY(launch_probe_tc(idx, b, nprobe, st, near_d));
     LaunchTimer t(kMlp, st);
     probe_features_kernel<<<(unsigned)b.nq, 128, 0, st>>>(
-        b.qrot, (int)idx->D, near_d, (int)b.nq, feats, m && xs ? m->mean : nullptr,
+        b.qrot, (int)idx->D, b.qn, near_d, (int)b.nq, feats, m && xs ? m->mean : nullptr,
         m && xs ? m->stdv : nullptr, m ? xs : nullptr);
     t.finish();
     ERQ_CUDA(cudaGetLastError());

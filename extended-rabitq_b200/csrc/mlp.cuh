@@ -240,22 +240,30 @@ __global__ void mlp_dup_weights_kernel(const __nv_bfloat16* __restrict__ wb,
 // With xs, the standardised features (f - mean) / std are also written as
 // [hi | lo] BF16, the input of the first layer (mlp_standardise_split_kernel's
 // arithmetic).
+// qnorm: the squared norms of the rotated queries when already computed
+// (the split kernel's), else each block sums its row.
 __global__ void probe_features_kernel(const float* __restrict__ qrot, int D,
+                                      const float* __restrict__ qnorm,
                                       const float* __restrict__ near_d, int nq,
                                       float* __restrict__ feats, const float* __restrict__ mean,
                                       const float* __restrict__ stdv,
                                       __nv_bfloat16* __restrict__ xs) {
     const int q = blockIdx.x;
     if (q >= nq) return;
-    __shared__ float red[8];
     const float* v = qrot + (size_t)q * D;
-    float s = 0.f;
-    for (int i = threadIdx.x; i < D; i += blockDim.x) s = fmaf(v[i], v[i], s);
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
-    __syncthreads();
-    float qn = 0.f;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) qn += red[w];
+    float qn;
+    if (qnorm) {
+        qn = qnorm[q];
+    } else {
+        __shared__ float red[8];
+        float s = 0.f;
+        for (int i = threadIdx.x; i < D; i += blockDim.x) s = fmaf(v[i], v[i], s);
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+        __syncthreads();
+        qn = 0.f;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) qn += red[w];
+    }
     const float inv = qn > 0.f ? 16.f / sqrtf(qn) : 0.f;
     float* f = feats + (size_t)q * kMlpIn;
     __nv_bfloat16* xr = xs ? xs + (size_t)q * 2 * kMlpIn : nullptr;

@@ -85,7 +85,7 @@ __global__ void chain_layout_kernel(const float* __restrict__ in, int rows, int 
 __device__ __forceinline__ float l2sqr16_chain(const float4* __restrict__ q4,
                                                const float4* __restrict__ c4, int D, int l) {
     float acc = 0.f;
-#pragma unroll 4
+#pragma unroll 2
     for (int s = 0; s < (D >> 6); ++s) {
         const float4 c = __ldg(c4 + s * 16 + l);
         const float4 x = q4[s * 16 + l];
