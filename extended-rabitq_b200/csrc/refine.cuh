@@ -81,7 +81,9 @@ __device__ __forceinline__ void ip_step(float2 acc[2], const float4& u, uint32_t
 // quad, in the reference's order (IP*_fxu* in inc/utils/space.hpp): the 16
 // accumulators acc[l] take the dims l, l+16, l+32, ... in turn; lane r holds
 // acc[4r..4r+3].  Rows are in the lane-interleaved layout of layout.cuh;
-// each lane streams its own uint4s, two ahead.  uq4 = unit_q as float4.
+// each lane streams its own uint4s one ahead (a loop unrolled by 3, so the
+// compiler renames the buffers instead of copying them, then the last pass,
+// which fetches nothing).  uq4 = unit_q as float4.
 // Returns the sums (the reduce tree: acc[l] + acc[l+8], then + 4, then
 // (0 + 2) + (1 + 3)) in every lane of the quad.
 template <int SB, int NC>
@@ -94,20 +96,17 @@ __device__ __forceinline__ void ex_ip_quad(const float4* __restrict__ uq4, const
 #pragma unroll
     for (int c = 0; c < NC; ++c) acc[c][0] = acc[c][1] = make_float2(0.f, 0.f);
     const uint4* rows[2] = {row0 + r, row1 + r};
-    uint4 cur[NC], nxt[NC];
+    uint4 cur[NC];
 #pragma unroll
-    for (int c = 0; c < NC; ++c) {
-        cur[c] = __ldg(rows[c]);
-        nxt[c] = U > 1 ? __ldg(rows[c] + 4) : cur[c];
-    }
+    for (int c = 0; c < NC; ++c) cur[c] = __ldg(rows[c]);
     const int Uf = steps / SPU;      // uint4s whose steps are all real
-    const int Upf = min(Uf, U - 2);  // passes that fetch the uint4 two ahead
+    const int Upf = min(Uf, U - 1);  // passes that fetch the next uint4
     int u = 0;
 #pragma unroll 3
     for (; u < Upf; ++u) {
         uint4 nn[NC];
 #pragma unroll
-        for (int c = 0; c < NC; ++c) nn[c] = __ldg(rows[c] + 4 * (u + 2));
+        for (int c = 0; c < NC; ++c) nn[c] = __ldg(rows[c] + 4 * (u + 1));
 #pragma unroll
         for (int t = 0; t < SPU; ++t) {
             const float4 q = uq4[4 * (u * SPU + t) + r];
@@ -115,20 +114,15 @@ __device__ __forceinline__ void ex_ip_quad(const float4* __restrict__ uq4, const
             for (int c = 0; c < NC; ++c) ip_step(acc[c], q, step_word<SB>(cur[c], t));
         }
 #pragma unroll
-        for (int c = 0; c < NC; ++c) {
-            cur[c] = nxt[c];
-            nxt[c] = nn[c];
-        }
+        for (int c = 0; c < NC; ++c) cur[c] = nn[c];
     }
-    for (; u < Uf; ++u) {  // the last passes: nothing left to fetch
+    for (; u < Uf; ++u) {  // the last pass: nothing left to fetch
 #pragma unroll
         for (int t = 0; t < SPU; ++t) {
             const float4 q = uq4[4 * (u * SPU + t) + r];
 #pragma unroll
             for (int c = 0; c < NC; ++c) ip_step(acc[c], q, step_word<SB>(cur[c], t));
         }
-#pragma unroll
-        for (int c = 0; c < NC; ++c) cur[c] = nxt[c];
     }
     for (int t = 0; t < steps - Uf * SPU; ++t) {  // a partly filled last uint4
         const float4 q = uq4[4 * (Uf * SPU + t) + r];
