@@ -2187,7 +2187,7 @@ struct erq_plan {
 namespace {
 
 erq_plan_tuning default_tuning(uint64_t nq) {
-    erq_plan_tuning t;
+    erq_plan_tuning t{};
     t.queries_per_item = nq >= 1024 ? 4 : 1;
     t.blocks_per_item = 16;
     t.warps = nq >= 1024 ? 8 : 4;
@@ -2448,7 +2448,7 @@ erq_status erq_plan_autotune(erq_plan* p, const float* queries, uint64_t n, int 
     erq_status s = ERQ_OK;
     for (const ScanShape& sh : kScanShapes) {
         for (int cb : kChunkChoices) {
-            erq_plan_tuning t;
+            erq_plan_tuning t = default_tuning(n);  // refinement form by batch size
             t.queries_per_item = (uint32_t)sh.qb;
             t.blocks_per_item = (uint32_t)cb;
             t.warps = (uint32_t)sh.warps;
