@@ -787,7 +787,7 @@ erq_status launch_probe_tc(const erq_index* idx, const Batch& b, uint64_t nprobe
         epi.col_norm = idx->cn;
         ERQ_TRY(gemm_tc(b.qsplit, idx->c_split, b.dist, (int)b.nq, K, 3 * D, epi, kGemm, st));
     }
-    ProbeArgs a;
+    ProbeArgs a{};
     a.approx = b.dist;
     a.qrot = b.qrot;
     a.centroids = idx->c_chain;
@@ -852,7 +852,7 @@ erq_status launch_probe(const erq_index* idx, const Batch& b, uint64_t nprobe, c
 
 erq_status launch_scan(const erq_index* idx, const Batch& b, uint64_t nprobe, cudaStream_t st,
                        const int* q_nprobe = nullptr, const uint32_t* order = nullptr) {
-    ScanArgs a;
+    ScanArgs a{};
     a.order = order;
     a.onorm = idx->onorm;
     a.c_size = idx->c_size;
@@ -886,7 +886,7 @@ erq_status launch_refine(const erq_index* idx, const Batch& b, uint64_t nprobe, 
                          uint32_t* out_ids, float* out_dists, cudaStream_t st,
                          const int* q_nprobe = nullptr, const uint32_t* order = nullptr,
                          int refine_warps = 0) {
-    RefineArgs a;
+    RefineArgs a{};
     a.order = order;
     a.bmin = b.bmin;
     a.stats = g_refine_stats_on.load() ? refine_stats_counter() : nullptr;
@@ -2234,7 +2234,7 @@ erq_status launch_scan_batched(erq_plan* p, uint64_t nq, const erq_plan_tuning& 
         lt.finish();
     }
     ERQ_CUDA(cudaMemsetAsync(p->counter, 0, sizeof(uint32_t), st));
-    ScanBatchArgs a;
+    ScanBatchArgs a{};
     a.qrot = p->b.qrot;
     a.centroids = idx->centroids;
     a.probe_cid = p->b.probe_cid;
