@@ -213,7 +213,9 @@ def cpu_searcher(index_path):
     import oracle
 
     if oracle.reference_available(stock=True) and cpu_has_avx512():
-        return oracle.Reference(index_path, stock=True), "reference", ""
+        return (oracle.Reference(index_path, stock=True), "reference",
+                "reference compiled with its own -Ofast flags but -march=x86-64-v4 (AVX-512) "
+                "in place of -march=native, so the binary runs on any AVX-512 host")
     note = ("reference build missing" if not oracle.reference_available(stock=True)
             else "host lacks AVX-512; reference cannot run")
     oracle.build_oracle()
@@ -247,6 +249,52 @@ def time_cpu(searcher, kind, query_raw, k, nprobe, threads, budget_s, max_n):
     searcher.search(qr, k, nprobe, nthreads=threads)
     t2 = time.perf_counter()
     return n / (t2 - t0), n, t2 - t0, t1 - t0, t2 - t1
+
+
+PARITY_QUERIES = 200
+
+
+def reference_parity(index_path, idx, query, k, nprobe, model=None, confidence=None):
+    """Results of the GPU search on the first PARITY_QUERIES queries against the
+    reference's own IVF::search (strict IEEE build) on the same index file and
+    the same rotated-query bytes: the plain search at `nprobe`, and with a
+    probe model the learned search query by query at the depth it chose.
+    Outside every timed region."""
+    import oracle
+
+    from erq_b200 import learned
+
+    if oracle.reference_available():
+        ref, kind = oracle.Reference(index_path), "reference IVF::search, strict IEEE build"
+
+        def ref_search(q, kk, npb):
+            return ref.search_dists(q, kk, npb)
+    else:
+        oracle.build_oracle()
+        ref, kind = oracle.Oracle(index_path), "C restatement (reference build missing)"
+
+        def ref_search(q, kk, npb):
+            return ref.search(q, kk, npb, nthreads=os.cpu_count() or 1)
+    qrot = idx.rotate(query[:PARITY_QUERIES])
+    out = {"queries": int(qrot.shape[0]), "against": kind}
+
+    def compare(ids, d, depth):
+        ids_eq = dist_eq = True
+        for u in np.unique(depth):
+            sel = np.flatnonzero(depth == u)
+            ri, rd = ref_search(qrot[sel], k, int(u))
+            ids_eq &= bool((ids[sel] == ri).all())
+            dist_eq &= bool((d[sel].view(np.uint32) == rd.view(np.uint32)).all())
+        return {"ids_equal": ids_eq, "dist_bits_equal": dist_eq}
+
+    ids, d = idx.search_batch(qrot, k, nprobe)
+    out["plain"] = dict(nprobe=nprobe, **compare(ids, d, np.full(qrot.shape[0], nprobe)))
+    if model is not None:
+        ids, d, used = learned.search_learned(idx, model, qrot, k, nprobe_fallback=nprobe,
+                                              confidence=confidence)
+        out["learned"] = dict(mean_nprobe=round(float(used.mean()), 3), **compare(ids, d, used))
+    ref.close()
+    return out
 
 
 # ------------------------------------------------------------------ helpers
@@ -452,6 +500,8 @@ def run_ours(args, cfg, name):
 
     # --- learned per-query depth, batched
     learned_info = None
+    learned_for_parity = (None, None)
+    model = None
     if not args.no_learned and cfg.get("train_queries"):
         model, meta = learned_model(idx, d, cfg, nprobe)
         plan_l = Plan(idx, max_batch=nq, k=k, nprobe=nprobe, model=model, raw=True)
@@ -499,8 +549,8 @@ def run_ours(args, cfg, name):
             modes["learned"] = {"ms": ms_l, "prof": prof_l, "clocks": clocks_l, "recall": r_l,
                                 "ids": ids_l, "scan_bytes": scan_bytes_l, "e2e_ms": e2e_l,
                                 "refine_bytes": cand_l * cand_bytes}
+            learned_for_parity = (model, conf)
         plan_l.free()
-        model.free()
     mode = min(modes, key=lambda m: modes[m]["ms"])
     chosen = modes[mode]
 
@@ -545,6 +595,12 @@ def run_ours(args, cfg, name):
                          f"{threads} threads, {sec:.1f}s (rotate {rot_s:.2f}s + search "
                          f"{srch_s:.2f}s)" + (f"; {note}" if note else "")}
         searcher.close()
+    parity = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        parity = reference_parity(index_path, idx, query, k, nprobe, *learned_for_parity)
+        log(f"parity sample: {parity}")
+    if model is not None:
+        model.free()
     if rank == 0:
         ms = chosen["ms"]
         out = {
@@ -577,6 +633,7 @@ def run_ours(args, cfg, name):
             "kernels_ms_per_step": {kk: round(v[1] / args.steps, 4) for kk, v in prof.items()
                                     if v[0]},
             "cpu_baseline": cpu,
+            "parity": parity,
             "clocks": chosen["clocks"],
         }
         print(json.dumps(out), flush=True)

@@ -599,6 +599,10 @@ erq_status tensor_map_bf16(CUtensorMap* m, const void* ptr, uint64_t rows, uint6
 
 // C[M][N] = A[M][Kd] * B[N][Kd]^T (BF16, FP32 accumulate) with an epilogue,
 // on tcgen05 (gemm_tc.cuh).  Kd must be a multiple of 64.
+// Polls per pipeline wait of the tcgen05 GEMM; lowered only by
+// erq_debug_set_gemm_wait_limit to exercise the timeout path.
+std::atomic<uint32_t> g_tc_wait_limit{kTcWaitLimit};
+
 erq_status gemm_tc(const __nv_bfloat16* A, const __nv_bfloat16* B, float* C, int M, int N, int Kd,
                    const GemmEpilogue& epi, int kernel_id, cudaStream_t st) {
     if (M <= 0 || N <= 0) return ERQ_OK;
@@ -622,7 +626,8 @@ erq_status gemm_tc(const __nv_bfloat16* A, const __nv_bfloat16* B, float* C, int
     }
     dim3 grid((unsigned)div_up(N, kTcBN), (unsigned)div_up(M, kTcBM));
     LaunchTimer t(kernel_id, st);
-    gemm_tc_kernel<<<grid, kTcThreads, gemm_tc_smem_bytes(), st>>>(ta, tb, C, M, N, Kd, epi, status);
+    gemm_tc_kernel<<<grid, kTcThreads, gemm_tc_smem_bytes(), st>>>(ta, tb, C, M, N, Kd, epi, status,
+                                                                    g_tc_wait_limit.load());
     t.finish();
     ERQ_CUDA(cudaGetLastError());
     return ERQ_OK;
@@ -1408,8 +1413,12 @@ erq_status erq_search_noalloc(const erq_index* idx, const float* rotated_queries
                     "queries must be 16-byte aligned and ids/dists 4-byte aligned");
     const uint64_t need = noalloc_bytes(idx, nq, nprobe);
     if (need > kNoAllocScratchBytes) {
-        uint64_t fit = 0;
-        while (fit < nq && noalloc_bytes(idx, fit + 1, nprobe) <= kNoAllocScratchBytes) ++fit;
+        // largest batch that fits: noalloc_bytes grows with nq, so bisect
+        uint64_t fit = 0, hi = nq;  // noalloc_bytes(fit) fits, noalloc_bytes(hi) does not
+        while (hi - fit > 1) {
+            const uint64_t mid = fit + (hi - fit) / 2;
+            if (noalloc_bytes(idx, mid, nprobe) <= kNoAllocScratchBytes) fit = mid; else hi = mid;
+        }
         return fail(ERQ_ERR_INVALID_ARGUMENT,
                     "%llu queries at nprobe=%llu need %llu bytes of scratch; the static scratch "
                     "holds %llu bytes (at most %llu queries per call here)",
@@ -1479,6 +1488,9 @@ erq_status erq_debug_centroid_dists(const erq_index* idx, const float* qrot, uin
     Scratch s(st, idx->pool);
     float* q = nullptr;
     float* d = nullptr;
+    if (div_up(nq, kCdTQ) > 65535)
+        return fail(ERQ_ERR_INVALID_ARGUMENT, "at most %llu queries per call",
+                    (unsigned long long)(65535ull * kCdTQ));
     ERQ_TRY(s.alloc(&q, nq * idx->D));
     ERQ_TRY(s.alloc(&d, nq * idx->K));
     ERQ_CUDA(cudaMemcpyAsync(q, qrot, nq * idx->D * 4, cudaMemcpyHostToDevice, st));
@@ -2031,6 +2043,11 @@ erq_status erq_debug_gemm_bf16(const uint16_t* A, const uint16_t* B, uint64_t M,
     return ERQ_OK;
 }
 
+erq_status erq_debug_set_gemm_wait_limit(uint32_t polls) {
+    g_tc_wait_limit.store(polls ? polls : kTcWaitLimit);
+    return ERQ_OK;
+}
+
 erq_status erq_debug_probe_fallbacks(int device, uint64_t* count, int reset) {
     if (!count) return fail(ERQ_ERR_INVALID_ARGUMENT, "count is NULL");
     DeviceGuard guard;
@@ -2167,7 +2184,20 @@ struct erq_plan {
     cudaStream_t cap = nullptr;
     bool use_graphs = true;
     std::mutex mu;
-    std::map<uint64_t, cudaGraphExec_t> graphs;
+    std::map<uint64_t, cudaGraphExec_t> graphs;  // by 2 * batch size + buffer slot
+    // Host-buffer pipelining: a batch with host buffers runs as chunks; chunk
+    // i uses buffer slot i % 2 (slot 0 = qin/ids/dists/used above, slot 1 =
+    // the buffers below, slot_rows queries), so the copy of chunk i + 1's
+    // queries in and chunk i - 1's results out overlap chunk i's search.
+    uint64_t slot_rows = 0;  // 0: plan too small to pipeline
+    float* qin1 = nullptr;
+    uint32_t* ids1 = nullptr;
+    float* dists1 = nullptr;
+    int* used1 = nullptr;
+    int pipe_chunks = 0;     // erq_plan_set_pipeline: 0 = by batch size, 1 = off
+    cudaStream_t h2d = nullptr, d2h = nullptr;
+    cudaEvent_t ev_start = nullptr, ev_end = nullptr;
+    cudaEvent_t ev_in[2] = {}, ev_comp[2] = {}, ev_out[2] = {};
 
     void drop_graphs() {
         for (auto& g : graphs) cudaGraphExecDestroy(g.second);
@@ -2180,6 +2210,11 @@ struct erq_plan {
         cudaDeviceSynchronize();
         drop_graphs();
         if (cap) cudaStreamDestroy(cap);
+        if (h2d) cudaStreamDestroy(h2d);
+        if (d2h) cudaStreamDestroy(d2h);
+        for (cudaEvent_t e : {ev_start, ev_end, ev_in[0], ev_in[1], ev_comp[0], ev_comp[1], ev_out[0],
+                              ev_out[1]})
+            if (e) cudaEventDestroy(e);
         if (prev >= 0) cudaSetDevice(prev);
     }
 };
@@ -2305,15 +2340,41 @@ erq_status plan_pipeline(erq_plan* p, uint64_t nq, const erq_plan_tuning& t, cud
     return ERQ_OK;
 }
 
-// Graph of the pipeline for batch size nq, captured on first use.
-erq_status plan_graph(erq_plan* p, uint64_t nq, cudaGraphExec_t* out) {
-    auto it = p->graphs.find(nq);
+// Points the plan's query and result buffers at slot 1 for its lifetime.
+struct SlotSwap {
+    erq_plan* p;
+    float* q;
+    uint32_t* i;
+    float* d;
+    int* u;
+    SlotSwap(erq_plan* pl, int slot) : p(pl), q(pl->qin), i(pl->ids), d(pl->dists), u(pl->used) {
+        if (slot) {
+            p->qin = p->qin1;
+            p->ids = p->ids1;
+            p->dists = p->dists1;
+            p->used = p->used1;
+        }
+    }
+    ~SlotSwap() {
+        p->qin = q;
+        p->ids = i;
+        p->dists = d;
+        p->used = u;
+    }
+};
+
+// Graph of the pipeline for batch size nq on buffer slot `slot`, captured on
+// first use.
+erq_status plan_graph(erq_plan* p, uint64_t nq, int slot, cudaGraphExec_t* out) {
+    const uint64_t key = 2 * nq + (uint64_t)slot;
+    auto it = p->graphs.find(key);
     if (it != p->graphs.end()) {
         *out = it->second;
         return ERQ_OK;
     }
     const erq_plan_tuning t = plan_tuning(p, nq);
     cudaGraph_t g = nullptr;
+    SlotSwap sw(p, slot);
     ERQ_CUDA(cudaStreamBeginCapture(p->cap, cudaStreamCaptureModeThreadLocal));
     erq_status s = plan_pipeline(p, nq, t, p->cap);
     cudaError_t e = cudaStreamEndCapture(p->cap, &g);
@@ -2326,8 +2387,72 @@ erq_status plan_graph(erq_plan* p, uint64_t nq, cudaGraphExec_t* out) {
     e = cudaGraphInstantiate(&ge, g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return fail(ERQ_ERR_CUDA, "graph instantiation failed: %s", cudaGetErrorString(e));
-    p->graphs[nq] = ge;
+    p->graphs[key] = ge;
     *out = ge;
+    return ERQ_OK;
+}
+
+// Search of nq queries on buffer slot `slot`, asynchronous on st (queries
+// already staged in the slot).
+erq_status plan_run(erq_plan* p, uint64_t nq, int slot, cudaStream_t st) {
+    if (p->use_graphs) {
+        cudaGraphExec_t ge = nullptr;
+        ERQ_TRY(plan_graph(p, nq, slot, &ge));
+        ERQ_CUDA(cudaGraphLaunch(ge, st));
+        return ERQ_OK;
+    }
+    SlotSwap sw(p, slot);
+    return plan_pipeline(p, nq, plan_tuning(p, nq), st);
+}
+
+// Chunks a batch of nq queries with host buffers runs as (1: no pipelining).
+uint64_t plan_chunks(const erq_plan* p, uint64_t nq) {
+    if (!p->slot_rows || p->pipe_chunks == 1) return 1;
+    uint64_t c = p->pipe_chunks ? (uint64_t)p->pipe_chunks : (nq >= 8192 ? 4 : (nq >= 4096 ? 2 : 1));
+    c = std::min<uint64_t>(c, nq);
+    while (c > 1 && div_up(nq, c) > p->slot_rows) --c;  // a chunk must fit slot 1
+    return c;
+}
+
+// Search with host buffers as `chunks` pipelined chunks: H2D copies on p->h2d,
+// the searches on st, D2H copies on p->d2h; chunk i uses slot i % 2 once
+// chunk i - 2 has left it.  Returns with the copies ordered before st's next
+// work.
+erq_status plan_search_pipelined(erq_plan* p, const float* queries, uint64_t nq, uint64_t chunks,
+                                 uint32_t* ids, float* dists, uint32_t* nprobe_used,
+                                 cudaStream_t st) {
+    const uint64_t cols = p->raw ? p->idx->DIM : p->idx->D;
+    const uint64_t step = div_up(nq, chunks);
+    ERQ_CUDA(cudaEventRecord(p->ev_start, st));
+    ERQ_CUDA(cudaStreamWaitEvent(p->h2d, p->ev_start, 0));
+    ERQ_CUDA(cudaStreamWaitEvent(p->d2h, p->ev_start, 0));
+    for (uint64_t c = 0, q0 = 0; q0 < nq; ++c, q0 += step) {
+        const int slot = (int)(c & 1);
+        const uint64_t n = std::min(step, nq - q0);
+        float* qin = slot ? p->qin1 : p->qin;
+        if (c >= 2) ERQ_CUDA(cudaStreamWaitEvent(p->h2d, p->ev_comp[slot], 0));
+        ERQ_CUDA(cudaMemcpyAsync(qin, queries + q0 * cols, n * cols * sizeof(float),
+                                 cudaMemcpyDefault, p->h2d));
+        ERQ_CUDA(cudaEventRecord(p->ev_in[slot], p->h2d));
+        ERQ_CUDA(cudaStreamWaitEvent(st, p->ev_in[slot], 0));
+        if (c >= 2) ERQ_CUDA(cudaStreamWaitEvent(st, p->ev_out[slot], 0));
+        ERQ_TRY(plan_run(p, n, slot, st));
+        ERQ_CUDA(cudaEventRecord(p->ev_comp[slot], st));
+        ERQ_CUDA(cudaStreamWaitEvent(p->d2h, p->ev_comp[slot], 0));
+        ERQ_CUDA(cudaMemcpyAsync(ids + q0 * p->k, slot ? p->ids1 : p->ids,
+                                 n * p->k * sizeof(uint32_t), cudaMemcpyDefault, p->d2h));
+        if (dists)
+            ERQ_CUDA(cudaMemcpyAsync(dists + q0 * p->k, slot ? p->dists1 : p->dists,
+                                     n * p->k * sizeof(float), cudaMemcpyDefault, p->d2h));
+        if (nprobe_used)
+            ERQ_CUDA(cudaMemcpyAsync(nprobe_used + q0, slot ? p->used1 : p->used,
+                                     n * sizeof(uint32_t), cudaMemcpyDefault, p->d2h));
+        ERQ_CUDA(cudaEventRecord(p->ev_out[slot], p->d2h));
+    }
+    ERQ_CUDA(cudaEventRecord(p->ev_end, p->d2h));
+    ERQ_CUDA(cudaStreamWaitEvent(st, p->ev_end, 0));
+    ERQ_CUDA(cudaEventRecord(p->ev_end, p->h2d));
+    ERQ_CUDA(cudaStreamWaitEvent(st, p->ev_end, 0));
     return ERQ_OK;
 }
 
@@ -2392,6 +2517,20 @@ erq_status erq_plan_create(const erq_index* idx, const erq_probe_model* model, u
         ERQ_CUDA(cudaMemcpy(p->used, np.data(), max_batch * sizeof(int), cudaMemcpyHostToDevice));
     }
     ERQ_CUDA(cudaStreamCreateWithFlags(&p->cap, cudaStreamNonBlocking));
+    if (max_batch >= 4096) {  // a second buffer slot for pipelined host-buffer searches
+        p->slot_rows = div_up(max_batch, 2);
+        ERQ_TRY(p->arena.alloc(&p->qin1, p->slot_rows * (p->raw ? idx->DIM : idx->D)));
+        ERQ_TRY(p->arena.alloc(&p->ids1, p->slot_rows * k));
+        ERQ_TRY(p->arena.alloc(&p->dists1, p->slot_rows * k));
+        ERQ_TRY(p->arena.alloc(&p->used1, p->slot_rows));
+        std::vector<int> np(p->slot_rows, (int)p->nprobe);
+        ERQ_CUDA(cudaMemcpy(p->used1, np.data(), p->slot_rows * sizeof(int), cudaMemcpyHostToDevice));
+        ERQ_CUDA(cudaStreamCreateWithFlags(&p->h2d, cudaStreamNonBlocking));
+        ERQ_CUDA(cudaStreamCreateWithFlags(&p->d2h, cudaStreamNonBlocking));
+        for (cudaEvent_t* e : {&p->ev_start, &p->ev_end, &p->ev_in[0], &p->ev_in[1], &p->ev_comp[0],
+                               &p->ev_comp[1], &p->ev_out[0], &p->ev_out[1]})
+            ERQ_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    }
     *out = p.release();
     return ERQ_OK;
 }
@@ -2442,7 +2581,10 @@ erq_status erq_plan_autotune(erq_plan* p, const float* queries, uint64_t n, int 
     ERQ_TRY(plan_stage_queries(p, queries, n, st));
     cudaEvent_t e0, e1;
     ERQ_CUDA(cudaEventCreate(&e0));
-    ERQ_CUDA(cudaEventCreate(&e1));
+    if (cudaEventCreate(&e1) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return fail(ERQ_ERR_CUDA, "cudaEventCreate failed");
+    }
     float best = 1e30f;
     erq_plan_tuning bt = default_tuning(n);
     erq_status s = ERQ_OK;
@@ -2516,22 +2658,24 @@ erq_status erq_plan_search(erq_plan* p, const float* queries, uint64_t nq, uint3
     DeviceGuard guard;
     ERQ_TRY(guard.set(p->idx->device));
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    if (p->use_graphs) {
-        cudaGraphExec_t ge = nullptr;
-        ERQ_TRY(plan_graph(p, nq, &ge));
-        ERQ_TRY(plan_stage_queries(p, queries, nq, st));
-        ERQ_CUDA(cudaGraphLaunch(ge, st));
-    } else {
-        ERQ_TRY(plan_stage_queries(p, queries, nq, st));
-        ERQ_TRY(plan_pipeline(p, nq, plan_tuning(p, nq), st));
-    }
     const bool host = !is_device_ptr(ids) || (dists && !is_device_ptr(dists)) ||
                       (nprobe_used && !is_device_ptr(nprobe_used)) || !is_device_ptr(queries);
-    ERQ_CUDA(cudaMemcpyAsync(ids, p->ids, nq * p->k * sizeof(uint32_t), cudaMemcpyDefault, st));
-    if (dists)
-        ERQ_CUDA(cudaMemcpyAsync(dists, p->dists, nq * p->k * sizeof(float), cudaMemcpyDefault, st));
-    if (nprobe_used)  // a plan without a model keeps nprobe in every entry
-        ERQ_CUDA(cudaMemcpyAsync(nprobe_used, p->used, nq * sizeof(uint32_t), cudaMemcpyDefault, st));
+    const uint64_t chunks = host ? plan_chunks(p, nq) : 1;
+    if (chunks > 1) {
+        ERQ_TRY(plan_search_pipelined(p, queries, nq, chunks, ids, dists, nprobe_used, st));
+    } else {
+        if (p->use_graphs) {  // capture (first use) before staging: capture runs nothing
+            cudaGraphExec_t ge = nullptr;
+            ERQ_TRY(plan_graph(p, nq, 0, &ge));
+        }
+        ERQ_TRY(plan_stage_queries(p, queries, nq, st));
+        ERQ_TRY(plan_run(p, nq, 0, st));
+        ERQ_CUDA(cudaMemcpyAsync(ids, p->ids, nq * p->k * sizeof(uint32_t), cudaMemcpyDefault, st));
+        if (dists)
+            ERQ_CUDA(cudaMemcpyAsync(dists, p->dists, nq * p->k * sizeof(float), cudaMemcpyDefault, st));
+        if (nprobe_used)  // a plan without a model keeps nprobe in every entry
+            ERQ_CUDA(cudaMemcpyAsync(nprobe_used, p->used, nq * sizeof(uint32_t), cudaMemcpyDefault, st));
+    }
     if (host) {
         uint32_t* hw = nullptr;
         ERQ_TRY(tc_status_fetch(st, &hw));
@@ -2542,6 +2686,14 @@ erq_status erq_plan_search(erq_plan* p, const float* queries, uint64_t nq, uint3
 }
 
 uint64_t erq_plan_device_bytes(const erq_plan* p) { return p ? p->arena.bytes : 0; }
+
+erq_status erq_plan_set_pipeline(erq_plan* p, int chunks) {
+    if (!p) return fail(ERQ_ERR_INVALID_ARGUMENT, "plan is NULL");
+    if (chunks < 0 || chunks > 64) return fail(ERQ_ERR_INVALID_ARGUMENT, "chunks outside 0..64");
+    std::lock_guard<std::mutex> g(p->mu);
+    p->pipe_chunks = chunks;
+    return ERQ_OK;
+}
 
 erq_status erq_plan_set_graphs(erq_plan* p, int on) {
     if (!p) return fail(ERQ_ERR_INVALID_ARGUMENT, "plan is NULL");

@@ -12,8 +12,8 @@
 //            warp the 32 TMEM lanes of its quadrant) and apply the epilogue of
 //            gemm.cuh (plain, distance ranking, bias + ReLU).
 // Every mbarrier wait is bounded; a wait that runs out sets bit 0 of
-// *status, and the CTA stops issuing work and frees its TMEM.  Loads come from
-// this GPU's own memory only (no cluster multicast).
+// *status, and the CTA stops issuing work and frees its TMEM.  Every TMA load
+// reads this GPU's own memory into this CTA's own shared memory.
 #pragma once
 
 #include <cuda.h>
@@ -28,7 +28,7 @@ constexpr int kTcThreads = 192;
 constexpr uint32_t kTcABytes = kTcBM * kTcBK * 2;   // 16 KB
 constexpr uint32_t kTcBBytes = kTcBN * kTcBK * 2;   // 32 KB
 constexpr uint32_t kTcStageBytes = kTcABytes + kTcBBytes;
-constexpr uint32_t kTcWaitLimit = 1u << 26;
+constexpr uint32_t kTcWaitLimit = 1u << 26;  // polls per pipeline wait (the default)
 
 // 1024 bytes of alignment slack + the ring + barriers and the TMEM address
 __host__ __device__ constexpr size_t gemm_tc_smem_bytes() {
@@ -87,7 +87,8 @@ __device__ __forceinline__ void tc_fence_after() {
 
 __global__ void __launch_bounds__(kTcThreads, kTcMinBlocks) gemm_tc_kernel(
     const __grid_constant__ CUtensorMap tma_a, const __grid_constant__ CUtensorMap tma_b,
-    float* __restrict__ Cout, int M, int N, int Kd, GemmEpilogue epi, uint32_t* status) {
+    float* __restrict__ Cout, int M, int N, int Kd, GemmEpilogue epi, uint32_t* status,
+    uint32_t wait_limit) {
     extern __shared__ uint8_t smem_raw[];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t raw = (uint32_t)__cvta_generic_to_shared(smem_raw);
@@ -125,7 +126,7 @@ __global__ void __launch_bounds__(kTcThreads, kTcMinBlocks) gemm_tc_kernel(
         if (lane == 0) {
             for (int kt = 0; kt < nk; ++kt) {
                 const int s = kt % kTcStages, r = kt / kTcStages;
-                if (r > 0 && !mbar_wait(empty0 + 8 * s, (r - 1) & 1, kTcWaitLimit)) {
+                if (r > 0 && !mbar_wait(empty0 + 8 * s, (r - 1) & 1, wait_limit)) {
                     *flag = 1u;
                     break;
                 }
@@ -142,7 +143,7 @@ __global__ void __launch_bounds__(kTcThreads, kTcMinBlocks) gemm_tc_kernel(
             const uint32_t idesc = umma_idesc_bf16(kTcBM, kTcBN);
             for (int kt = 0; kt < nk; ++kt) {
                 const int s = kt % kTcStages, r = kt / kTcStages;
-                if (!mbar_wait(full0 + 8 * s, r & 1, kTcWaitLimit) || *flag) {
+                if (!mbar_wait(full0 + 8 * s, r & 1, wait_limit) || *flag) {
                     *flag = 1u;
                     break;
                 }
@@ -171,7 +172,7 @@ __global__ void __launch_bounds__(kTcThreads, kTcMinBlocks) gemm_tc_kernel(
                          : "memory");
         }
     } else {
-        const bool ok = mbar_wait(accum, 0, kTcWaitLimit) && !*flag;
+        const bool ok = mbar_wait(accum, 0, wait_limit) && !*flag;
         if (!ok) *flag = 1u;
         tc_fence_after();
         const int q = warp & 3;  // TMEM lane quadrant this warp may read
@@ -216,11 +217,14 @@ __global__ void __launch_bounds__(kTcThreads, kTcMinBlocks) gemm_tc_kernel(
             }
         }
     }
-    // a CTA that gave up still lets its TMA copies land before it exits
+    // A CTA that gave up still lets its TMA copies land, and its issued MMAs
+    // finish (the accumulator barrier's commit follows them), before it frees
+    // its TMEM and exits.  These drains always use the full limit.
     if (warp == 0 && lane == 0 && *flag) {
         for (int kt = max(0, issued - kTcStages); kt < issued; ++kt)
             mbar_wait(full0 + 8 * (kt % kTcStages), (kt / kTcStages) & 1, kTcWaitLimit);
     }
+    if (warp == 1 && lane == 0 && *flag) mbar_wait(accum, 0, kTcWaitLimit);
     tc_fence_before();
     __syncthreads();
     if (warp == 1) {

@@ -13,6 +13,7 @@ LIB_PATH = os.path.join(PKG_ROOT, "lib", "liberq.so")
 
 # erq_status values (include/erq.h)
 ERQ_OK = 0
+ERQ_ERR_TIMEOUT = 7
 STATUS_NAMES = {
     0: "ERQ_OK",
     1: "ERQ_ERR_INVALID_ARGUMENT",
@@ -36,7 +37,7 @@ EXPORTED_SYMBOLS = (
     "erq_search_learned_raw",
     "erq_debug_probe_model_grads", "erq_debug_probe_model_params",
     "erq_plan_create", "erq_plan_free", "erq_plan_set_learned", "erq_plan_autotune",
-    "erq_plan_set_tuning", "erq_plan_get_tuning", "erq_plan_search", "erq_plan_device_bytes", "erq_plan_set_graphs", "erq_debug_gemm_bf16", "erq_debug_probe_fallbacks", "erq_debug_refine_stats",
+    "erq_plan_set_tuning", "erq_plan_get_tuning", "erq_plan_search", "erq_plan_device_bytes", "erq_plan_set_graphs", "erq_plan_set_pipeline", "erq_debug_gemm_bf16", "erq_debug_set_gemm_wait_limit", "erq_debug_probe_fallbacks", "erq_debug_refine_stats",
 )
 
 
@@ -131,10 +132,14 @@ def load_library(path: str | None = None) -> C.CDLL:
     lib.erq_plan_device_bytes.restype = u64
     lib.erq_debug_gemm_bf16.argtypes = [vp, vp, u64, u64, u64, vp, C.c_int]
     lib.erq_debug_gemm_bf16.restype = C.c_int
+    lib.erq_debug_set_gemm_wait_limit.argtypes = [C.c_uint32]
+    lib.erq_debug_set_gemm_wait_limit.restype = C.c_int
     lib.erq_debug_probe_fallbacks.argtypes = [C.c_int, C.POINTER(C.c_uint64), C.c_int]
     lib.erq_debug_probe_fallbacks.restype = C.c_int
     lib.erq_debug_refine_stats.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_uint64)]
     lib.erq_debug_refine_stats.restype = C.c_int
+    lib.erq_plan_set_pipeline.argtypes = [vp, C.c_int]
+    lib.erq_plan_set_pipeline.restype = C.c_int
     lib.erq_plan_set_graphs.argtypes = [vp, C.c_int]
     lib.erq_plan_set_graphs.restype = C.c_int
     lib.erq_profile_enable.argtypes = [C.c_int]

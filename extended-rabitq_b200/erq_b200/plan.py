@@ -71,6 +71,10 @@ class Plan:
     def set_graphs(self, on: bool) -> None:
         check(self._lib.erq_plan_set_graphs(self._h, 1 if on else 0))
 
+    def set_pipeline(self, chunks: int) -> None:
+        """Pieces a host-buffer batch runs as (0: by batch size, 1: one piece)."""
+        check(self._lib.erq_plan_set_pipeline(self._h, chunks))
+
     def device_bytes(self) -> int:
         return int(self._lib.erq_plan_device_bytes(self._h))
 

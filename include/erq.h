@@ -194,6 +194,12 @@ ERQ_API uint64_t erq_plan_device_bytes(const erq_plan* plan);
 /* on = 0 launches the kernels one by one instead of replaying a graph (same
  * results; lets the kernel profiler of erq_debug.h time each launch). */
 ERQ_API erq_status erq_plan_set_graphs(erq_plan* plan, int on);
+/* How erq_plan_search runs a batch with host buffers: as `chunks` pieces
+ * whose host-to-device copies, searches and device-to-host copies overlap
+ * (two buffer slots, two copy streams), 1 for one piece, 0 (the default) for
+ * 4 pieces from 8192 queries and 2 from 4096.  Plans with max_batch below 4096
+ * never split.  Results are the same in every case. */
+ERQ_API erq_status erq_plan_set_pipeline(erq_plan* plan, int chunks);
 
 /* erq_search without any memory allocation.  Has no counterpart in the
  * reference: it is for callers that cannot allocate device memory while a
@@ -208,7 +214,9 @@ ERQ_API erq_status erq_plan_set_graphs(erq_plan* plan, int on);
  * does not fit (about nq * (4K + 128 * blocks of the nprobe largest clusters)
  * bytes) fails with ERQ_ERR_INVALID_ARGUMENT and a message giving the largest
  * batch that fits.  The first call on a device looks up the array's device
- * address; make that first call before any stream capture.  Every call uses
+ * address and keeps it for the life of the process, so the library must not
+ * be used across a cudaDeviceReset of that device; make that first call
+ * before any stream capture.  Every call uses
  * the same array: calls that overlap on the GPU (different streams, or
  * different threads without ordering) race and must be serialised by the
  * caller.  Results equal erq_search's. */

@@ -10,7 +10,9 @@
 //   ivf.search(&rotated[i * D], nullptr, k, nprobe, results);   // IVF::search
 //
 // Differences a caller sees:
-//   * rotate takes raw row-major buffers instead of Eigen matrices;
+//   * rotate also takes raw row-major buffers (the matrix form accepts any
+//     row-major matrix type with rows()/cols()/data(), Eigen's FloatRowMat
+//     included, with the output already sized rows x D);
 //   * errors throw erq::Error (the reference asserts or aborts);
 //   * search_batch answers many queries in one call (the GPU's fast path);
 //   * building an index (IVF(n, dim, k, b) + construct + save) stays with the
@@ -18,8 +20,10 @@
 #pragma once
 
 #include <cstdint>
+#include <cstring>
 #include <stdexcept>
 #include <string>
+#include <vector>
 
 #include "erq.h"
 
@@ -43,12 +47,38 @@ class Rotator {
     void rotate(const float* queries, size_t nq, float* rotated, void* stream = nullptr) const {
         check(erq_rotate(index_, queries, nq, rotated, stream));
     }
+
+    // Rotator::rotate(const FloatRowMat& A, FloatRowMat& RAND_A)
+    // (inc/index/Rotator.hpp:60-63): RAND_A = A * P for row-major matrices.
+    // A holds one query per row, DIM columns or already zero-padded to D
+    // (src/test_search.cpp:83-90 passes the padded form); RAND_A must be
+    // rows x D, as test_search allocates it.
+    template <class Mat>
+    void rotate(const Mat& A, Mat& RAND_A) const {
+        const size_t nq = static_cast<size_t>(A.rows());
+        const size_t cols = static_cast<size_t>(A.cols());
+        if (cols != DIM_ && cols != D_)
+            throw Error(ERQ_ERR_INVALID_ARGUMENT, "rotate: matrix has " + std::to_string(cols) +
+                                                      " columns; expected DIM or padded D");
+        if (static_cast<size_t>(RAND_A.rows()) != nq || static_cast<size_t>(RAND_A.cols()) != D_)
+            throw Error(ERQ_ERR_INVALID_ARGUMENT, "rotate: output must be rows x padded D");
+        if (cols == DIM_) {
+            rotate(A.data(), nq, RAND_A.data());
+            return;
+        }
+        // padded input: the columns past DIM are zero, so rotate the first DIM
+        std::vector<float> q(nq * DIM_);
+        for (size_t i = 0; i < nq; ++i)
+            std::memcpy(&q[i * DIM_], A.data() + i * cols, DIM_ * sizeof(float));
+        rotate(q.data(), nq, RAND_A.data());
+    }
     size_t size() const;
 
    private:
     friend class IVF;
     const erq_index* index_ = nullptr;
     size_t D_ = 0;
+    size_t DIM_ = 0;
 };
 
 inline size_t Rotator::size() const { return D_; }
@@ -70,6 +100,7 @@ class IVF {
         check(erq_index_get_info(index_, &info_));
         rot_.index_ = index_;
         rot_.D_ = info_.padded_dim;
+        rot_.DIM_ = info_.dim;
     }
 
     // IVF::search (inc/index/IVF.hpp:295-324): one rotated query (D floats);

@@ -14,7 +14,7 @@ code through oracle/ref_harness.cpp:
                 threshold), EX-bit inner products (IP_FUNC), the sequence of
                 refined candidates, and the final ids and distances of IVF::search
 
-Usage (needs /root/reference and `make -C oracle`):
+Usage (needs the reference sources and `make -C oracle REF=<reference checkout>`):
     python tests/golden/make_golden.py
 """
 from __future__ import annotations

@@ -25,6 +25,21 @@ def test_facade_header_compiles(tmp_path):
                     str(src)], check=True)
 
 
+def test_facade_rotate_takes_row_major_matrices(tmp_path):
+    """src/test_search.cpp:83-92 rotates with `rp.rotate(padded_query,
+    rotated_query)` on Eigen row-major matrices; the facade's Rotator accepts
+    the same call (here with the oracle's Eigen-subset stand-in)."""
+    src = tmp_path / "r.cpp"
+    src.write_text(
+        '#include "third/Eigen/Dense"\n#include "erq_ivf.hpp"\n'
+        'using FloatRowMat = Eigen::Matrix<float, Eigen::Dynamic, Eigen::Dynamic, Eigen::RowMajor>;\n'
+        'int main() { erq::IVF ivf; FloatRowMat padded_query(2, 64); padded_query.setZero();\n'
+        '  FloatRowMat rotated_query(2, 64); erq::Rotator& rp = ivf.rotator();\n'
+        '  if (ivf.k()) rp.rotate(padded_query, rotated_query); return 0; }\n')
+    subprocess.run(["g++", "-std=c++17", "-fsyntax-only", "-I", os.path.join(REPO, "include"),
+                    "-I", os.path.join(REPO, "oracle", "shim"), str(src)], check=True)
+
+
 def test_driver_builds():
     subprocess.run(["make", "-s", "-C", PKG, "bin/erq_test_search"], check=True)
     assert os.access(DRIVER, os.X_OK)

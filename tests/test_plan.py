@@ -198,3 +198,34 @@ def test_probe_rarely_falls_back(uneven):
     L.probe_fallbacks(0, reset=True)
     idx.search_batch(qr, 100, 6, with_dists=False)
     assert L.probe_fallbacks(0, reset=True) <= 0.02 * len(qr)
+
+
+def test_host_buffers_pipelined_in_chunks(uneven):
+    """A host-buffer batch runs as chunks whose copies overlap the searches
+    (two buffer slots, two copy streams); every chunking gives the one-piece
+    results, with and without graphs, and repeated calls reuse the slots."""
+    from erq_b200 import Plan
+
+    idx, q, qr, _ = uneven
+    k, nprobe = 100, 6
+    nq = 4099  # odd, so that the chunks differ in size
+    rng = np.random.default_rng(41)
+    qs = np.ascontiguousarray(qr[rng.integers(0, qr.shape[0], nq)])
+    ref_ids, ref_d = idx.search_batch(qs, k, nprobe)
+    plan = Plan(idx, max_batch=nq, k=k, nprobe=nprobe)
+    qh = torch.from_numpy(qs).pin_memory()
+    ids_h = torch.empty((nq, k), dtype=torch.int32).pin_memory()
+    d_h = torch.empty((nq, k), dtype=torch.float32).pin_memory()
+    u_h = torch.empty(nq, dtype=torch.int32).pin_memory()
+    for graphs in (True, False):
+        plan.set_graphs(graphs)
+        for chunks in (0, 1, 2, 3, 4, 7):
+            plan.set_pipeline(chunks)
+            for _ in range(2):
+                ids_h.fill_(-1)
+                d_h.fill_(-1.0)
+                plan.search_buffers(qh, ids_h, d_h, u_h)
+                assert (ids_h.numpy().view(np.uint32) == ref_ids).all(), (graphs, chunks)
+                assert (bits(d_h.numpy()) == bits(ref_d)).all(), (graphs, chunks)
+                assert (u_h.numpy() == nprobe).all()
+    plan.free()

@@ -10,6 +10,7 @@ the second reusing the array the first one left behind.  This file is named
 to be collected last.
 """
 import ctypes as C
+import re
 
 import numpy as np
 import pytest
@@ -67,6 +68,21 @@ def test_noalloc_rejects_what_it_cannot_hold():
     assert _call(lib, idx, q, 10, idx.K, ids, None, stream) == 1
     msg = lib.erq_last_error().decode()
     assert "static scratch" in msg and "queries per call" in msg
+    # the batch the message reports fits exactly: that many queries run and
+    # equal erq_search, one more is refused
+    fit = int(re.search(r"at most (\d+) queries per call", msg).group(1))
+    assert 0 < fit < nq
+    gen = torch.Generator().manual_seed(7)
+    qf = torch.randn((fit + 1, idx.D), generator=gen, dtype=torch.float32).cuda()
+    ids_f = torch.full((fit + 1, 10), -1, dtype=torch.int32, device="cuda")
+    d_f = torch.full((fit + 1, 10), -1.0, dtype=torch.float32, device="cuda")
+    assert _call(lib, idx, qf, 10, idx.K, ids_f, d_f, stream) == 1
+    assert _call(lib, idx, qf[:fit], 10, idx.K, ids_f, d_f, stream) == 0, lib.erq_last_error()
+    torch.cuda.synchronize()
+    ref_ids, ref_d = idx.search_batch(qf[:fit], 10, idx.K, stream=stream)
+    torch.cuda.synchronize()
+    assert (ids_f[:fit].cpu().numpy() == ref_ids.cpu().numpy()).all()
+    assert (d_f[:fit].cpu().numpy().view(np.uint32) == ref_d.cpu().numpy().view(np.uint32)).all()
     # host buffers are refused: copying them would need device memory
     qh = torch.zeros((4, idx.D), dtype=torch.float32)
     ih = torch.empty((4, 10), dtype=torch.int32)
