@@ -252,6 +252,9 @@ def time_cpu(searcher, kind, query_raw, k, nprobe, threads, budget_s, max_n):
 
 
 PARITY_QUERIES = 200
+# A query whose most likely probe depth has a probability below this falls
+# back to the fixed nprobe (8 depths: a uniform guess gives each 0.125).
+LEARNED_MIN_PROB = 0.25
 
 
 def reference_parity(index_path, idx, query, k, nprobe, model=None, confidence=None):
@@ -291,7 +294,7 @@ def reference_parity(index_path, idx, query, k, nprobe, model=None, confidence=N
     out["plain"] = dict(nprobe=nprobe, **compare(ids, d, np.full(qrot.shape[0], nprobe)))
     if model is not None:
         ids, d, used = learned.search_learned(idx, model, qrot, k, nprobe_fallback=nprobe,
-                                              confidence=confidence)
+                                              confidence=confidence, min_prob=LEARNED_MIN_PROB)
         out["learned"] = dict(mean_nprobe=round(float(used.mean()), 3), **compare(ids, d, used))
     ref.close()
     return out
@@ -365,21 +368,25 @@ def learned_model(idx, d, cfg, plain_nprobe):
     training on the GPU by the library's kernels."""
     from erq_b200 import learned
 
-    path = os.path.join(d, "probe.model")
+    bins = learned.scaled_bins(plain_nprobe, cfg["K"])
+    path = os.path.join(d, "probe-" + "-".join(map(str, bins)) + ".model")
     if os.path.exists(path):
         return learned.ProbeModel.load(path), json.load(open(path + ".json"))
     t0 = time.time()
     train_q = np.load(os.path.join(d, "train_query.npy"))
     rot = idx.rotate(train_q)
     del train_q
-    bins = learned.DEFAULT_BINS
     labels = learned.make_labels(idx, rot, cfg["k"], bins)
+    agree = learned.exhaustive_agreement(idx, rot[:1000], cfg["k"], bins[-1])
     feats = learned.probe_features(idx, rot)
     del rot
     model = learned.ProbeModel.train(feats, labels, bins, epochs=8, batch=1024, lr=1e-3,
                                      seed=cfg["seed"] + 3)
     hist = np.bincount(labels, minlength=len(bins)).tolist()
     meta = {"train_queries": int(labels.size), "label_hist": hist, "bins": list(bins),
+            "labels": f"smallest depth whose top-{cfg['k']} set equals that at the deepest "
+                      f"bin ({bins[-1]} probes)",
+            "deepest_bin_equals_exhaustive": round(agree, 4),
             "final_loss": round(model.final_loss, 4), "train_s": round(time.time() - t0, 1)}
     model.save(path)
     json.dump(meta, open(path + ".json", "w"))
@@ -428,7 +435,7 @@ def run_ours(args, cfg, name):
     block_bytes = 4 * arr.D + 128
     cand_bytes = arr.D * arr.EX // 8 + 8  # EX-code row + xipnorm + id per exact candidate
     qrot_h = idx.rotate(query)
-    cids, _ = idx.debug_probe(qrot_h, max(nprobe, learned.DEFAULT_BINS[-1]))
+    cids, _ = idx.debug_probe(qrot_h, max(nprobe, learned.scaled_bins(nprobe, arr.K)[-1]))
     del arr
 
     stream = torch.cuda.current_stream()
@@ -510,7 +517,7 @@ def run_ours(args, cfg, name):
         # probes the fewest clusters
         for conf in (0.005, 0.01, 0.02, 0.05, 0.1, 0.2, 0.3, 0.4, 0.5, 0.6, 0.7, 0.8, 0.9,
                      0.95, 0.99):
-            plan_l.set_learned(conf)
+            plan_l.set_learned(conf, LEARNED_MIN_PROB)
             ids_l, _, used = plan_l.search(query, with_dists=False, with_nprobe=True)
             r = metrics.recall_at_k(ids_l, gt, k)
             log(f"learned confidence={conf}: recall@{k}={r:.4f}, mean nprobe "
@@ -520,7 +527,9 @@ def run_ours(args, cfg, name):
                 break
         if best is not None:
             conf, r_l, ids_l, used = best
-            plan_l.set_learned(conf)
+            plan_l.set_learned(conf, LEARNED_MIN_PROB)
+            model_fallback = learned.fallback_rate(model, learned.probe_features(idx, qrot_h),
+                                                   LEARNED_MIN_PROB)
             L.probe_fallbacks(local, reset=True)
             plan_l.set_graphs(False)  # counting is fixed into a graph when it is captured
             L.refine_stats(local, enable=True)
@@ -539,7 +548,9 @@ def run_ours(args, cfg, name):
                             "confidence": conf, "mean_nprobe": round(float(used.mean()), 4),
                             "recall@100": round(r_l, 5),
                             "ms_per_step": round(ms_l / args.steps, 4), "tuning": tune_l,
-                            "probe_fallback_rate": round(learned_fallback_rate, 5),
+                            "min_prob": LEARNED_MIN_PROB,
+                            "model_fallback_rate": round(model_fallback, 5),
+                            "exact_probe_fallback_rate": round(learned_fallback_rate, 5),
                             "refine_per_query": {kk: round(v / nq, 2) for kk, v in rst_l.items()},
                             "kernels_ms_per_step": {kk: round(v[1] / args.steps, 4)
                                                     for kk, v in prof_l.items() if v[0]},
@@ -615,7 +626,7 @@ def run_ours(args, cfg, name):
                                    f"{cfg['bits']}-bit, {nq} queries per step, top-{k}",
                        "mode": mode, "nprobe": nprobe, "recall@100": round(chosen["recall"], 5),
                        "distance_ratio": round(ratio, 5), "queries_per_step": nq,
-                       "probe_fallback_rate": round(fallback_rate, 5),
+                       "exact_probe_fallback_rate": round(fallback_rate, 5),
                        "parallelism": f"replicas x{world} (queries replicated per GPU)",
                        "l2": "inputs larger than L2: every step streams "
                              f"{chosen['scan_bytes'] / 1e9:.1f} GB of packed codes from a "

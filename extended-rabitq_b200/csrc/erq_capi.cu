@@ -349,7 +349,7 @@ erq_status load_impl(const char* path, erq_index* idx) {
         cudaError_t e = cudaMalloc(&raw, std::max<uint64_t>(blocks * raw_block, 16));
         if (e != cudaSuccess) return fail(ERQ_ERR_OUT_OF_MEMORY, "cudaMalloc for short codes failed");
         erq_status s = read_to_device(f.get(), raw, blocks * raw_block, staging, "the short codes");
-        if (s == ERQ_OK) s = dev_alloc(idx, &idx->codes, blocks * 4 * D);
+        if (s == ERQ_OK) s = dev_alloc(idx, &idx->codes, blocks * code_block_bytes((int)D));
         if (s == ERQ_OK) s = dev_alloc(idx, &idx->onorm, blocks * kFastSize);
         if (s == ERQ_OK && blocks > 0) {
             transform_blocks_kernel<<<1184, 256>>>(raw, idx->codes, idx->onorm, blocks, (int)D);
@@ -454,7 +454,6 @@ erq_status load_impl(const char* path, erq_index* idx) {
 }
 
 // ------------------------------------------------------------ pipeline
-size_t scan_smem_bytes(int D) { return 256 + (size_t)(D / 64) * 512 + (size_t)D * 4 + 64; }
 size_t refine_smem_bytes(int D, int k, bool wide = false) {
     const int kpad = (k + 31) & ~31;
     return refine_smem_bytes_per_query(D, kpad, wide ? kWideWindowBlocks : kWindowBlocks);
@@ -559,7 +558,7 @@ erq_status tc_status_check(uint32_t* host_word) {
         uint32_t* dword = nullptr;
         ERQ_TRY(tc_status_ptr(&dword));
         ERQ_CUDA(cudaMemset(dword, 0, sizeof(uint32_t)));
-        return fail(ERQ_ERR_TIMEOUT, "a bounded wait in the tcgen05 GEMM ran out; results are incomplete");
+        return fail(ERQ_ERR_TIMEOUT, "a bounded wait in a kernel (tcgen05 GEMM or staged scan) ran out; results are incomplete");
     }
     return ERQ_OK;
 }
@@ -876,6 +875,7 @@ erq_status launch_scan(const erq_index* idx, const Batch& b, uint64_t nprobe, cu
     a.q_nprobe = q_nprobe;
     a.D = (int)idx->D;
     a.nprobe = (int)nprobe;
+    ERQ_TRY(tc_status_ptr(&a.status));
     const uint64_t pairs = b.nq * nprobe;
     if (pairs > 0x7fffffffull) return fail(ERQ_ERR_INVALID_ARGUMENT, "too many (query, probe) pairs");
     LaunchTimer t(kScan, st);
@@ -2135,27 +2135,56 @@ struct Arena {
 struct ScanShape {
     int qb, warps;
 };
-constexpr ScanShape kScanShapes[] = {{1, 4}, {2, 4}, {4, 4}, {2, 8}, {4, 8}, {8, 8}};
+constexpr ScanShape kScanShapes[] = {{1, 4}, {1, 8}, {2, 4}, {2, 8}, {4, 4}, {4, 8}};
+constexpr int kNumScanShapes = sizeof(kScanShapes) / sizeof(kScanShapes[0]);
 constexpr int kChunkChoices[] = {8, 16, 32, 64};
 
+// Calls f with the kernel instantiation for (QB, W) and D's table stride
+// class (one instantiation serves every D when QB = 1).
+template <int QB, int W, typename F>
+erq_status with_scan_batched(int D, F&& f) {
+    if constexpr (QB == 1) {
+        return f(scan_batched_kernel<1, W, 0>, scan_batch_smem_bytes(1, W, 0, D));
+    } else {
+        switch (scan_qstride(D)) {
+            case 16384:
+                return f(scan_batched_kernel<QB, W, 16384>, scan_batch_smem_bytes(QB, W, 16384, D));
+            case 32768:
+                return f(scan_batched_kernel<QB, W, 32768>, scan_batch_smem_bytes(QB, W, 32768, D));
+            default:
+                return f(scan_batched_kernel<QB, W, 45056>, scan_batch_smem_bytes(QB, W, 45056, D));
+        }
+    }
+}
+
+// Resident blocks per SM of shape (QB, W) at this D; 0 when its shared
+// memory exceeds what a block may have (the shape is then never used).
 template <int QB, int W>
 erq_status scan_batched_configure(int D, int* per_sm) {
-    const size_t smem = scan_batch_smem_bytes(QB, D);
-    ERQ_CUDA(cudaFuncSetAttribute(scan_batched_kernel<QB, W>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    ERQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, scan_batched_kernel<QB, W>, W * 32,
-                                                           smem));
-    *per_sm = std::max(1, *per_sm);
-    return ERQ_OK;
+    *per_sm = 0;
+    int dev = 0, optin = 0;
+    ERQ_CUDA(cudaGetDevice(&dev));
+    ERQ_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    return with_scan_batched<QB, W>(D, [&](auto kern, size_t smem) -> erq_status {
+        if (smem > (size_t)optin) return ERQ_OK;
+        ERQ_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        ERQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, kern, W * 32, smem));
+        return ERQ_OK;
+    });
 }
 
 template <int QB, int W>
 erq_status scan_batched_launch(const ScanBatchArgs& a, int blocks, cudaStream_t st) {
-    LaunchTimer t(kScan, st);
-    scan_batched_kernel<QB, W><<<(unsigned)blocks, W * 32, scan_batch_smem_bytes(QB, a.D), st>>>(a);
-    t.finish();
-    ERQ_CUDA(cudaGetLastError());
-    return ERQ_OK;
+    if (blocks <= 0)
+        return fail(ERQ_ERR_UNSUPPORTED, "scan tile (%d queries, %d warps) does not fit at D=%d", QB,
+                    W, a.D);
+    return with_scan_batched<QB, W>(a.D, [&](auto kern, size_t smem) -> erq_status {
+        LaunchTimer t(kScan, st);
+        kern<<<(unsigned)blocks, W * 32, smem, st>>>(a);
+        t.finish();
+        ERQ_CUDA(cudaGetLastError());
+        return ERQ_OK;
+    });
 }
 
 }  // namespace
@@ -2167,7 +2196,7 @@ struct erq_plan {
     bool raw = false;
     float confidence = 0.9f, min_prob = 0.f;
     int sms = 148;
-    int per_sm[6] = {};  // resident scan blocks per SM, by kScanShapes entry
+    int per_sm[kNumScanShapes] = {};  // resident scan blocks per SM, by kScanShapes entry
     std::map<uint64_t, erq_plan_tuning> tunings;  // by the batch size tuned for
     Arena arena;
     Batch b;
@@ -2293,14 +2322,15 @@ erq_status launch_scan_batched(erq_plan* p, uint64_t nq, const erq_plan_tuning& 
     a.nprobe = (int)p->nprobe_run;
     a.CB = (int)t.blocks_per_item;
     (void)nq;
+    ERQ_TRY(tc_status_ptr(&a.status));
     const int qb = (int)t.queries_per_item, w = (int)t.warps;
     auto grid = [&](int i) { return p->sms * p->per_sm[i]; };
     if (qb == 1 && w == 4) return scan_batched_launch<1, 4>(a, grid(0), st);
-    if (qb == 2 && w == 4) return scan_batched_launch<2, 4>(a, grid(1), st);
-    if (qb == 4 && w == 4) return scan_batched_launch<4, 4>(a, grid(2), st);
+    if (qb == 1 && w == 8) return scan_batched_launch<1, 8>(a, grid(1), st);
+    if (qb == 2 && w == 4) return scan_batched_launch<2, 4>(a, grid(2), st);
     if (qb == 2 && w == 8) return scan_batched_launch<2, 8>(a, grid(3), st);
-    if (qb == 4 && w == 8) return scan_batched_launch<4, 8>(a, grid(4), st);
-    if (qb == 8 && w == 8) return scan_batched_launch<8, 8>(a, grid(5), st);
+    if (qb == 4 && w == 4) return scan_batched_launch<4, 4>(a, grid(4), st);
+    if (qb == 4 && w == 8) return scan_batched_launch<4, 8>(a, grid(5), st);
     return fail(ERQ_ERR_INVALID_ARGUMENT, "unsupported scan tile (%d queries, %d warps)", qb, w);
 }
 
@@ -2493,11 +2523,11 @@ erq_status erq_plan_create(const erq_index* idx, const erq_probe_model* model, u
     {
         const int D = (int)idx->D;
         ERQ_TRY((scan_batched_configure<1, 4>(D, &p->per_sm[0])));
-        ERQ_TRY((scan_batched_configure<2, 4>(D, &p->per_sm[1])));
-        ERQ_TRY((scan_batched_configure<4, 4>(D, &p->per_sm[2])));
+        ERQ_TRY((scan_batched_configure<1, 8>(D, &p->per_sm[1])));
+        ERQ_TRY((scan_batched_configure<2, 4>(D, &p->per_sm[2])));
         ERQ_TRY((scan_batched_configure<2, 8>(D, &p->per_sm[3])));
-        ERQ_TRY((scan_batched_configure<4, 8>(D, &p->per_sm[4])));
-        ERQ_TRY((scan_batched_configure<8, 8>(D, &p->per_sm[5])));
+        ERQ_TRY((scan_batched_configure<4, 4>(D, &p->per_sm[4])));
+        ERQ_TRY((scan_batched_configure<4, 8>(D, &p->per_sm[5])));
     }
     ERQ_TRY(alloc_batch(p->arena, idx, max_batch, p->nprobe_run, p->b));
     ERQ_TRY(p->arena.alloc(&p->qin, max_batch * (p->raw ? idx->DIM : idx->D)));
@@ -2588,7 +2618,9 @@ erq_status erq_plan_autotune(erq_plan* p, const float* queries, uint64_t n, int 
     float best = 1e30f;
     erq_plan_tuning bt = default_tuning(n);
     erq_status s = ERQ_OK;
-    for (const ScanShape& sh : kScanShapes) {
+    for (int si = 0; si < kNumScanShapes && s == ERQ_OK; ++si) {
+        const ScanShape& sh = kScanShapes[si];
+        if (!p->per_sm[si]) continue;  // does not fit at this D
         for (int cb : kChunkChoices) {
             erq_plan_tuning t = default_tuning(n);  // refinement form by batch size
             t.queries_per_item = (uint32_t)sh.qb;

@@ -19,6 +19,7 @@
 #include <cuda.h>
 
 #include "gemm.cuh"
+#include "mbarrier.cuh"
 
 namespace erq {
 
@@ -33,29 +34,6 @@ constexpr uint32_t kTcWaitLimit = 1u << 26;  // polls per pipeline wait (the def
 // 1024 bytes of alignment slack + the ring + barriers and the TMEM address
 __host__ __device__ constexpr size_t gemm_tc_smem_bytes() {
     return 1024 + (size_t)kTcStages * kTcStageBytes + 256;
-}
-
-__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
-                 : "memory");
-}
-// true once the phase with this parity has completed; false after `limit` polls
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, uint32_t limit) {
-    for (uint32_t i = 0; i < limit; ++i) {
-        uint32_t done;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}"
-            : "=r"(done)
-            : "r"(bar), "r"(parity)
-            : "memory");
-        if (done) return true;
-    }
-    return false;
 }
 
 __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y,
@@ -107,7 +85,7 @@ __global__ void __launch_bounds__(kTcThreads, kTcMinBlocks) gemm_tc_kernel(
         }
         mbar_init(accum, 1);
         *flag = 0u;
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        mbar_init_fence();
     }
     if (warp == 1) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(

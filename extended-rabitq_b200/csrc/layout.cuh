@@ -9,14 +9,12 @@
 //                        perm0 = {0,8,1,9,...,7,15}; nibble bit 3 = dim 4g+0
 //   bytes [4D, 4D+128): 32 floats ||o - c|| (one per vector, vector order)
 //
-// Device layout (chosen for the scan kernel):
-//   codes: one 4D-byte block per 32 vectors, regrouped per 64-dim chunk c
-//          (groups 16c..16c+15, 256 bytes) so that warp lane L = 16h + j
-//          loads 8 contiguous bytes = byte j of groups 16c+8h+0..7:
-//            dev[c*256 + L*8 + u] = file[(16c + 8h + u)*16 + j]
-//          A warp reads one chunk with one coalesced 256-byte load, every
-//          half-warp then walks one group at a time (16 lanes sharing one
-//          16-entry table: broadcast-friendly shared-memory lookups).
+// Device layout (chosen for the scan kernels, scan.cuh): dims in groups of
+// six, idx_t(v) = sum_{j<6} bit(v, 6t + j) << j (0 past D); per 32-vector
+// block, chunks of 16 groups, 512 bytes each: lane v's 16 bytes at 16v, byte
+// i = 2 * idx_{16k+i}(v) + 128 * (i & 1) (the entry's byte offset in the
+// group's 128-byte table, odd groups in the upper half of a 256-byte window).
+//   codes: code_block_bytes(D) = 512 * ceil(ceil(D/6)/16) bytes per block
 //   onorm: 32 floats per block, split out of the block.
 //
 // EX-bit codes.  File layout: one row of D*EX/8 bytes per vector, 64-dim
@@ -35,26 +33,44 @@
 #pragma once
 
 #include "common.cuh"
+#include "scan.cuh"
 
 namespace erq {
+
+// Byte of a file group's 16 bytes that holds vector v's nibble (low nibble
+// for v < 16, high for v >= 16): the inverse of perm0 = {0,8,1,9,...,7,15}
+// (inc/index/fastscan/pack_codes.hpp:44).
+__device__ __forceinline__ uint32_t fastscan_byte_of(uint32_t v) {
+    const uint32_t w = v & 15;
+    return w < 8 ? 2 * w : 2 * (w - 8) + 1;
+}
 
 // One thread per output byte of the code region.
 __global__ void transform_blocks_kernel(const uint8_t* __restrict__ raw,
                                         uint8_t* __restrict__ codes,
                                         float* __restrict__ onorm, uint64_t nblocks, int D) {
-    const uint64_t code_bytes = 4ull * D;
-    const uint64_t raw_block = code_bytes + kFastSize * sizeof(float);
-    const uint64_t total = nblocks * code_bytes;
+    const uint64_t file_code = 4ull * D;
+    const uint64_t raw_block = file_code + kFastSize * sizeof(float);
+    const uint32_t bb = code_block_bytes(D);
+    const uint64_t total = nblocks * bb;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total;
          i += (uint64_t)gridDim.x * blockDim.x) {
-        const uint64_t b = i / code_bytes;
-        const uint32_t r = (uint32_t)(i - b * code_bytes);
-        const uint32_t c = r >> 8;          // 64-dim chunk
-        const uint32_t L = (r >> 3) & 31;   // lane
-        const uint32_t u = r & 7;           // byte within the lane's 8
-        const uint32_t h = L >> 4, j = L & 15;
-        const uint32_t g = 16 * c + 8 * h + u;
-        codes[i] = raw[b * raw_block + 16ull * g + j];
+        const uint64_t b = i / bb;
+        const uint32_t r = (uint32_t)(i - b * bb);
+        const uint32_t k = r >> 9, v = (r >> 4) & 31, byte = r & 15;
+        const uint32_t t = 16 * k + byte;
+        const uint8_t* fb = raw + b * raw_block;
+        const uint32_t jv = fastscan_byte_of(v), hi = v >> 4;
+        uint32_t idx = 0;
+        for (int j = 0; j < kHexDims; ++j) {
+            const uint32_t dim = kHexDims * t + j;
+            if (dim >= (uint32_t)D) break;
+            const uint32_t g = dim >> 2, rr = dim & 3;
+            const uint32_t x = fb[16 * g + jv];
+            const uint32_t nib = hi ? (x >> 4) : (x & 15u);
+            idx |= ((nib >> (3 - rr)) & 1u) << j;  // nibble bit 3 = dim 4g + 0
+        }
+        codes[i] = (uint8_t)(2 * idx + 128 * (byte & 1));
     }
     const uint64_t nf = nblocks * kFastSize;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nf;
@@ -62,7 +78,7 @@ __global__ void transform_blocks_kernel(const uint8_t* __restrict__ raw,
         const uint64_t b = i / kFastSize;
         const uint32_t v = (uint32_t)(i - b * kFastSize);
         float f;
-        memcpy(&f, raw + b * raw_block + code_bytes + 4ull * v, sizeof(float));
+        memcpy(&f, raw + b * raw_block + file_code + 4ull * v, sizeof(float));
         onorm[i] = f;
     }
 }

@@ -3,7 +3,10 @@
 Labels come from the plain search itself: for a query, the label is the
 smallest class c whose probe count bins[c] gives the same top-k set as the
 deepest class bins[-1] (the depth at which the plain method's result stops
-changing, measured on the class grid).  The MLP (trained on the GPU by the
+changing, measured on the class grid).  The deepest class stands in for
+exhaustive probing; ``exhaustive_agreement`` measures how often its top-k
+already is the exhaustive one.  ``scaled_bins`` spreads the classes
+geometrically up to twice the workload's fixed nprobe.  The MLP (trained on the GPU by the
 library's own forward/backward kernels) maps a query's features (a sketch of
 the rotated query and its 64 nearest exact centroid distances) to a
 distribution over the classes; the learned search scans the smallest depth
@@ -23,6 +26,46 @@ DEFAULT_BINS = (1, 2, 3, 4, 6, 8, 12, 16)
 N_FEATURES = 320
 N_BINS = 8
 N_PARAMS = 150024
+
+
+def scaled_bins(nprobe: int, K: int) -> tuple:
+    """The 8 probe depths of a workload whose fixed nprobe is `nprobe`: up to
+    twice nprobe (at least 16, at most K), geometric from 1/64 of the top, so
+    that a model can both cut and deepen the fixed search.  DEFAULT_BINS when
+    the top is 16 or less."""
+    top = min(K, max(16, 2 * nprobe))
+    if top <= 16:
+        return tuple(min(b, K) for b in DEFAULT_BINS)
+    lo = max(1.0, top / 64.0)
+    r = (top / lo) ** (1.0 / (N_BINS - 1))
+    bins = []
+    for i in range(N_BINS):
+        b = int(round(lo * r ** i))
+        b = max(b, bins[-1] + 1 if bins else 1)
+        bins.append(b)
+    bins[-1] = top
+    for i in range(N_BINS - 2, -1, -1):  # strictly increasing below the top
+        bins[i] = min(bins[i], bins[i + 1] - 1)
+    return tuple(bins)
+
+
+def exhaustive_agreement(ivf, rotated_queries, k: int, depth: int) -> float:
+    """Fraction of queries whose top-k set at `depth` probes equals the
+    top-k set of the exhaustive search (every cluster probed): how well the
+    deepest label bin stands in for exhaustive probing."""
+    q = np.ascontiguousarray(rotated_queries, np.float32).reshape(-1, ivf.D)
+    a, _ = ivf.search_batch(q, k, min(depth, ivf.K), with_dists=False)
+    b, _ = ivf.search_batch(q, k, ivf.K, with_dists=False)
+    return float(np.all(np.sort(a, 1) == np.sort(b, 1), axis=1).mean())
+
+
+def fallback_rate(model, features, min_prob: float) -> float:
+    """Fraction of queries whose most likely depth has probability below
+    min_prob, which the learned search sends to the fixed nprobe."""
+    if min_prob <= 0:
+        return 0.0
+    p = model.predict(features)
+    return float((p.max(axis=1) < min_prob).mean())
 
 
 def probe_features(ivf, rotated_queries) -> np.ndarray:
