@@ -3,8 +3,7 @@
 //   rotate_kernel       Rotator::rotate            inc/index/Rotator.hpp:60-63
 //   centroid_dist_kernel L2Sqr16 for every (query, centroid)
 //                                                  inc/utils/space.hpp:18-39
-//   select_probe_kernel  partial_sort of the nprobe nearest centroids
-//                                                  inc/index/Initializer.hpp:55-68
+// (the nprobe nearest of these exact distances: probe_exact_kernel, probe.cuh)
 #pragma once
 
 #include "common.cuh"
@@ -126,61 +125,6 @@ __global__ void __launch_bounds__(256) centroid_dist_kernel(const float* __restr
             const int q = q0 + 4 * qg + i, cc = c0 + cg + 4 * j;
             if (l == 0 && q < nq && cc < K) dist[(size_t)q * K + cc] = s;
         }
-}
-
-// ------------------------------------------------------- probe selection
-// One block per query: bitonic sort of (distance, id) keys in shared memory,
-// then the nprobe smallest in ascending order.  Also lays out the per-query
-// scan workspace: s_off[q][p] = q_slot*stride + sum of 32*blocks(c_p') for
-// p' < p, the int32 offset where the scan of (q, p) writes its sums.
-__global__ void select_probe_kernel(const float* __restrict__ dist, int nq, int K, int Kpow2,
-                                    int nprobe, const uint32_t* __restrict__ c_nblocks,
-                                    uint64_t stride, uint32_t* __restrict__ probe_cid,
-                                    float* __restrict__ probe_sqy, uint64_t* __restrict__ s_off) {
-    extern __shared__ uint64_t keys[];
-    const int q = blockIdx.x;
-    const float* dq = dist + (size_t)q * K;
-    for (int i = threadIdx.x; i < Kpow2; i += blockDim.x)
-        keys[i] = i < K ? dist_key(dq[i], (uint32_t)i) : ~0ull;
-    __syncthreads();
-    for (int size = 2; size <= Kpow2; size <<= 1) {
-        for (int stride_ = size >> 1; stride_ > 0; stride_ >>= 1) {
-            for (int t = threadIdx.x; t < (Kpow2 >> 1); t += blockDim.x) {
-                const int lo = 2 * t - (t & (stride_ - 1));
-                const int hi = lo + stride_;
-                const bool up = (lo & size) == 0;
-                const uint64_t a = keys[lo], b = keys[hi];
-                if ((a > b) == up) {
-                    keys[lo] = b;
-                    keys[hi] = a;
-                }
-            }
-            __syncthreads();
-        }
-    }
-    // outputs + exclusive prefix of 32*nblocks over the probe order (warp 0)
-    if (threadIdx.x < 32) {
-        uint64_t run = (uint64_t)q * stride;
-        for (int p0 = 0; p0 < nprobe; p0 += 32) {
-            const int p = p0 + threadIdx.x;
-            uint32_t nbv = 0;
-            if (p < nprobe) {
-                const uint64_t key = keys[p];
-                const uint32_t cid = (uint32_t)(key & 0xffffffffu);
-                probe_cid[(size_t)q * nprobe + p] = cid;
-                probe_sqy[(size_t)q * nprobe + p] = __uint_as_float((uint32_t)(key >> 32));
-                nbv = 32u * c_nblocks[cid];
-            }
-            uint32_t incl = nbv;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const uint32_t n = __shfl_up_sync(0xffffffffu, incl, o);
-                if ((int)threadIdx.x >= o) incl += n;
-            }
-            if (p < nprobe) s_off[(size_t)q * nprobe + p] = run + (incl - nbv);
-            run += __shfl_sync(0xffffffffu, incl, 31);
-        }
-    }
 }
 
 }  // namespace erq

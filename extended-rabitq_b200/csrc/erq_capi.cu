@@ -5,7 +5,7 @@
 // layout.cuh, and drive the search pipeline of IVF::search
 // (inc/index/IVF.hpp:295-324) over batches of queries:
 //
-//   centroid_dist_kernel -> select_probe_kernel -> scan_kernel -> refine_kernel
+//   centroid_dist_kernel -> probe_exact_kernel -> scan_kernel -> refine_kernel
 //
 // Per-call scratch comes from the stream-ordered allocator on the caller's
 // stream, so concurrent calls on different streams never share workspace.
@@ -31,6 +31,7 @@
 #include "coarse.cuh"
 #include "gemm.cuh"
 #include "gemm_tc.cuh"
+#include "kmeans.cuh"
 #include "mlp.cuh"
 #include "probe.cuh"
 #include "layout.cuh"
@@ -42,7 +43,7 @@
 using namespace erq;
 
 // probe selection sorts all K centroid keys in shared memory (8 bytes each)
-constexpr uint64_t kMaxClusters = 16384;
+constexpr uint64_t kMaxClusters = 1ull << 24;
 
 // ------------------------------------------------------------------ errors
 namespace {
@@ -294,11 +295,10 @@ erq_status load_impl(const char* path, erq_index* idx) {
     if (idx->DIM == 0 || idx->K == 0)
         return fail(ERQ_ERR_FORMAT, "bad header: DIM=%llu K=%llu", (unsigned long long)idx->DIM,
                     (unsigned long long)idx->K);
-    if (idx->K >= 20000)
-        return fail(ERQ_ERR_UNSUPPORTED,
-                    "K=%llu >= 20000: the reference keeps an HNSW coarse quantiser in a side file "
-                    "for such indexes, which this library does not read",
-                    (unsigned long long)idx->K);
+    // K >= 20000: the reference loads an HNSW graph over the centroids from a
+    // side file (inc/index/IVF.hpp:157-161, 274-291) and probes approximately;
+    // this library ignores the side file and probes every K exactly (the
+    // Flat path's semantics, inc/index/Initializer.hpp:55-68).
     if (idx->K > kMaxClusters)
         return fail(ERQ_ERR_UNSUPPORTED, "K=%llu exceeds the %llu clusters the probe selection supports",
                     (unsigned long long)idx->K, (unsigned long long)kMaxClusters);
@@ -493,14 +493,14 @@ int next_pow2(int x) {
 
 erq_status configure_kernels(int D, int K, int k) {
     const int kp2 = next_pow2(K);
-    ERQ_CUDA(cudaFuncSetAttribute(select_probe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  kp2 * 8));
+
     ERQ_CUDA(cudaFuncSetAttribute(scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)scan_smem_bytes(D)));
     ERQ_CUDA(cudaFuncSetAttribute(probe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)probe_smem_bytes(D, kp2, K <= kProbeStageKeys ? K : 0)));
-    ERQ_CUDA(cudaFuncSetAttribute(probe_fallback_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)probe_fallback_smem_bytes(D, kp2)));
+                                  (int)probe_smem_bytes(D, std::min(kp2, kProbeSortSmemKeys),
+                                                        K <= kProbeStageKeys ? K : 0)));
+    ERQ_CUDA(cudaFuncSetAttribute(probe_exact_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)probe_exact_smem_bytes(D, std::min(kp2, kProbeSortSmemKeys))));
     ERQ_TRY(configure_refine<2>(D));
     ERQ_TRY(configure_refine<3>(D));
     ERQ_TRY(configure_refine<4>(D));
@@ -552,6 +552,19 @@ erq_status tc_status_fetch(cudaStream_t st, uint32_t** host_word) {
     *host_word = pinned[dev];
     return ERQ_OK;
 }
+// The status word read now (the caller has synchronised its work).
+erq_status tc_status_check_now() {
+    uint32_t* dword = nullptr;
+    ERQ_TRY(tc_status_ptr(&dword));
+    uint32_t v = 0;
+    ERQ_CUDA(cudaMemcpy(&v, dword, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    if (v) {
+        ERQ_CUDA(cudaMemset(dword, 0, sizeof(uint32_t)));
+        return fail(ERQ_ERR_TIMEOUT, "a bounded wait in a kernel ran out; results are incomplete");
+    }
+    return ERQ_OK;
+}
+
 erq_status tc_status_check(uint32_t* host_word) {
     if (host_word && *host_word) {
         *host_word = 0;
@@ -654,15 +667,33 @@ struct Batch {
     uint32_t* order_q = nullptr;      // [nq]
     float* bmin = nullptr;            // smallest lower bound per scanned block (S / 32 entries)
     uint32_t* fb_flag = nullptr;      // [nq] queries whose probe needs all K exact distances
+    uint64_t* sortbuf = nullptr;      // [nq][sort_cap] probe sort keys too many for shared memory
+    uint64_t sort_cap = 0;
 };
+
+int probe_candidates(uint64_t nprobe);
+
+// Sort keys per query the probe kernels keep in global memory (0: all fit in
+// shared memory): the selection of probe_kernel (Msel candidates, with the 64
+// feature ranks when `features`) and the nprobe slots of probe_exact_kernel.
+uint64_t probe_sort_cap(const erq_index* idx, uint64_t nprobe, bool features) {
+    const int K = (int)idx->K;
+    const int n = (int)std::min<uint64_t>(nprobe, idx->K);
+    const int msel = features ? std::max(probe_candidates(n), kProbeFeatRank) : probe_candidates(n);
+    const int spow2 = next_pow2(msel + 1 > K ? K : msel);
+    const int npow2 = next_pow2(n);
+    const int cap = std::max(spow2, npow2);
+    return cap > kProbeSortSmemKeys ? (uint64_t)cap : 0;
+}
 
 // Largest query batch whose scan workspace fits the budget.
 uint64_t batch_queries(const erq_index* idx, uint64_t nprobe, uint64_t nq) {
     const uint64_t per_q = 32ull * idx->top_blocks[nprobe] * sizeof(int32_t) +
                            idx->K * sizeof(float) + nprobe * 24 + 6 * idx->D + 4 +
                            idx->top_blocks[nprobe] * sizeof(float);
+    const uint64_t per_q_all = per_q + probe_sort_cap(idx, nprobe, true) * sizeof(uint64_t);
     const uint64_t budget = 3ull << 30;
-    uint64_t b = std::max<uint64_t>(1, budget / std::max<uint64_t>(per_q, 1));
+    uint64_t b = std::max<uint64_t>(1, budget / std::max<uint64_t>(per_q_all, 1));
     return std::min(b, nq);
 }
 
@@ -686,6 +717,8 @@ erq_status alloc_batch(Alloc& s, const erq_index* idx, uint64_t nq, uint64_t npr
     ERQ_TRY(s.alloc(&b.order_q, nq));
     ERQ_TRY(s.alloc(&b.bmin, nq * idx->top_blocks[nprobe]));
     ERQ_TRY(s.alloc(&b.fb_flag, nq));
+    b.sort_cap = probe_sort_cap(idx, nprobe, true);
+    if (b.sort_cap) ERQ_TRY(s.alloc(&b.sortbuf, nq * b.sort_cap));
     return ERQ_OK;
 }
 
@@ -819,16 +852,25 @@ erq_status launch_probe_tc(const erq_index* idx, const Batch& b, uint64_t nprobe
     if (!b.fb_flag) return fail(ERQ_ERR_INVALID_ARGUMENT, "probe batch without fallback flags");
     a.fallback_flag = b.fb_flag;
     a.stage_keys = K <= kProbeStageKeys ? 1 : 0;
+    a.exact_rows = b.dist;
+    const int npow2 = next_pow2((int)std::min<uint64_t>(nprobe, (uint64_t)K));
+    if (a.Spow2 > kProbeSortSmemKeys || npow2 > kProbeSortSmemKeys) {
+        if (!b.sortbuf || b.sort_cap < (uint64_t)std::max(a.Spow2, npow2))
+            return fail(ERQ_ERR_INVALID_ARGUMENT, "probe batch without a large enough sort buffer");
+        a.sort_global = b.sortbuf;
+        a.sort_cap = b.sort_cap;
+    }
     {
         LaunchTimer t(kProbe, st);
-        probe_kernel<<<(unsigned)b.nq, kProbeThreads, probe_smem_bytes(D, a.Spow2, a.stage_keys ? K : 0),
-                       st>>>(a);
+        probe_kernel<<<(unsigned)b.nq, kProbeThreads,
+                       probe_smem_bytes(D, a.sort_global ? 0 : a.Spow2, a.stage_keys ? K : 0), st>>>(a);
         t.finish();
         ERQ_CUDA(cudaGetLastError());
     }
     {
         LaunchTimer t(kProbe, st);
-        probe_fallback_kernel<<<(unsigned)b.nq, kProbeThreads, probe_fallback_smem_bytes(D, a.Kpow2), st>>>(a);
+        probe_exact_kernel<<<(unsigned)b.nq, kProbeThreads,
+                             probe_exact_smem_bytes(D, a.sort_global ? 0 : npow2), st>>>(a, 1, npow2);
         t.finish();
         ERQ_CUDA(cudaGetLastError());
     }
@@ -842,13 +884,30 @@ erq_status launch_probe(const erq_index* idx, const Batch& b, uint64_t nprobe, c
     centroid_dist_kernel<<<g1, 256, 0, st>>>(b.qrot, (int)b.nq, idx->centroids, K, D, b.dist);
     t1.finish();
     ERQ_CUDA(cudaGetLastError());
-    const int kp2 = next_pow2(K);
-    const int thr = std::min(1024, std::max(128, kp2 / 8));
-    const uint64_t stride = 32ull * idx->top_blocks[nprobe];
+    ProbeArgs a{};
+    a.qrot = b.qrot;
+    a.centroids = idx->c_chain;  // unused: the rows already hold exact distances
+    a.c_nblocks = idx->c_nblocks;
+    a.stride = 32ull * idx->top_blocks[nprobe];
+    a.probe_cid = b.probe_cid;
+    a.probe_sqy = b.probe_sqy;
+    a.s_off = b.s_off;
+    a.nq = (int)b.nq;
+    a.K = K;
+    a.Kpow2 = next_pow2(K);
+    a.D = D;
+    a.nprobe = (int)nprobe;
+    a.exact_rows = b.dist;
+    const int npow2 = next_pow2((int)std::min<uint64_t>(nprobe, (uint64_t)K));
+    if (npow2 > kProbeSortSmemKeys) {
+        if (!b.sortbuf || b.sort_cap < (uint64_t)npow2)
+            return fail(ERQ_ERR_INVALID_ARGUMENT, "probe batch without a large enough sort buffer");
+        a.sort_global = b.sortbuf;
+        a.sort_cap = b.sort_cap;
+    }
     LaunchTimer t2(kSelectProbe, st);
-    select_probe_kernel<<<(unsigned)b.nq, thr, (size_t)kp2 * 8, st>>>(
-        b.dist, (int)b.nq, K, kp2, (int)nprobe, idx->c_nblocks, stride, b.probe_cid, b.probe_sqy,
-        b.s_off);
+    probe_exact_kernel<<<(unsigned)b.nq, kProbeThreads, probe_exact_smem_bytes(D, a.sort_global ? 0 : npow2),
+                         st>>>(a, 0, npow2);
     t2.finish();
     ERQ_CUDA(cudaGetLastError());
     return ERQ_OK;
@@ -1267,6 +1326,136 @@ erq_status features_device(const erq_index* idx, const Batch& b, uint64_t nprobe
 
 }  // namespace
 
+// ------------------------------------------------------------- k-means
+// splitmix64 (Steele, Lea and Flood, 2014): the random stream of the
+// k-means initialisation and of its empty-cluster splits.
+uint64_t splitmix64_next(uint64_t& s) {
+    uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+double splitmix64_uniform(uint64_t& s) {  // in [0, 1), 53 random bits
+    return (double)(splitmix64_next(s) >> 11) * (1.0 / 9007199254740992.0);
+}
+
+// Device buffers of one clustering run, freed on scope exit.
+struct KmBuffers {
+    std::vector<void*> owned;
+    template <typename T>
+    erq_status alloc(T** p, size_t count) {
+        void* q = nullptr;
+        cudaError_t e = cudaMalloc(&q, std::max<size_t>(count * sizeof(T), 16));
+        if (e != cudaSuccess)
+            return fail(e == cudaErrorMemoryAllocation ? ERQ_ERR_OUT_OF_MEMORY : ERQ_ERR_CUDA,
+                        "cudaMalloc(%zu bytes) for k-means failed: %s", count * sizeof(T),
+                        cudaGetErrorString(e));
+        owned.push_back(q);
+        *p = static_cast<T*>(q);
+        return ERQ_OK;
+    }
+    ~KmBuffers() {
+        for (void* q : owned) cudaFree(q);
+    }
+};
+
+// Lloyd iterations (kmeans.cuh).  cent: device [k][dim], updated in place;
+// rng: the split stream; counts_host: the last iteration's cluster sizes
+// before its splits (optional); final_assign: one more assignment to the
+// final centroids.
+erq_status km_iterate(const float* x, uint64_t n, uint64_t dim, uint64_t k, int iters, float* cent,
+                      uint32_t* assign, uint64_t& rng, uint32_t* counts_host, bool final_assign,
+                      cudaStream_t st) {
+    const uint64_t Cp = (dim + 63) / 64 * 64;
+    const uint64_t R = std::min<uint64_t>(n, std::max<uint64_t>(1024, (256ull << 20) / std::max<uint64_t>(k, 1)));
+    KmBuffers b;
+    __nv_bfloat16 *c_split = nullptr, *x_split = nullptr;
+    float *cn = nullptr, *xn = nullptr, *dist = nullptr;
+    unsigned long long* sums = nullptr;
+    uint32_t* counts = nullptr;
+    unsigned* amax = nullptr;
+    ERQ_TRY(b.alloc(&c_split, k * 3 * Cp));
+    ERQ_TRY(b.alloc(&cn, k));
+    ERQ_TRY(b.alloc(&x_split, R * 3 * Cp));
+    ERQ_TRY(b.alloc(&xn, R));
+    ERQ_TRY(b.alloc(&dist, R * k));
+    ERQ_TRY(b.alloc(&sums, k * dim));
+    ERQ_TRY(b.alloc(&counts, k));
+    ERQ_TRY(b.alloc(&amax, 1));
+    // fixed-point scale 2^s: n * max|x| * 2^s < 2^62, s <= 32
+    ERQ_CUDA(cudaMemsetAsync(amax, 0, sizeof(unsigned), st));
+    abs_max_kernel<<<1184, 256, 0, st>>>(x, n * dim, amax);
+    ERQ_CUDA(cudaGetLastError());
+    unsigned amax_bits = 0;
+    ERQ_CUDA(cudaMemcpyAsync(&amax_bits, amax, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    ERQ_CUDA(cudaStreamSynchronize(st));
+    float amax_f = 0.f;
+    std::memcpy(&amax_f, &amax_bits, sizeof(float));
+    const double top = std::max(1e-30, (double)amax_f) * (double)n;
+    const double scale = std::ldexp(1.0, std::min(32, (int)std::floor(61.0 - std::log2(top))));
+    std::vector<uint32_t> cnt(k);
+    auto assign_all = [&]() -> erq_status {
+        split_rows_kernel<<<(unsigned)k, 256, 0, st>>>(cent, (int)k, (int)dim, (int)Cp, false, c_split, cn);
+        ERQ_CUDA(cudaGetLastError());
+        for (uint64_t r0 = 0; r0 < n; r0 += R) {
+            const uint64_t rows = std::min(R, n - r0);
+            split_rows_kernel<<<(unsigned)rows, 256, 0, st>>>(x + r0 * dim, (int)rows, (int)dim, (int)Cp,
+                                                              true, x_split, xn);
+            ERQ_CUDA(cudaGetLastError());
+            GemmEpilogue epi;
+            epi.row_norm = xn;
+            epi.col_norm = cn;
+            ERQ_TRY(gemm_tc(x_split, c_split, dist, (int)rows, (int)k, (int)(3 * Cp), epi, kGemm, st));
+            argmin_rows_kernel<<<(unsigned)div_up(rows * 32, 256), 256, 0, st>>>(dist, (int)rows, (int)k,
+                                                                                 assign + r0);
+            ERQ_CUDA(cudaGetLastError());
+        }
+        return ERQ_OK;
+    };
+    for (int it = 0; it < iters; ++it) {
+        ERQ_TRY(assign_all());
+        ERQ_CUDA(cudaMemsetAsync(sums, 0, k * dim * sizeof(unsigned long long), st));
+        ERQ_CUDA(cudaMemsetAsync(counts, 0, k * sizeof(uint32_t), st));
+        kmeans_accumulate_kernel<<<(unsigned)div_up(n, 8), 256, 0, st>>>(x, (int)n, (int)dim, scale,
+                                                                          assign, sums, counts);
+        ERQ_CUDA(cudaGetLastError());
+        kmeans_update_kernel<<<1184, 256, 0, st>>>(sums, counts, (int)k, (int)dim, scale, cent);
+        ERQ_CUDA(cudaGetLastError());
+        ERQ_CUDA(cudaMemcpyAsync(cnt.data(), counts, k * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        ERQ_CUDA(cudaStreamSynchronize(st));
+        ERQ_TRY(tc_status_check_now());
+        if (counts_host) std::copy(cnt.begin(), cnt.end(), counts_host);
+        // empty clusters: split a populated one, chosen with probability
+        // proportional to (size - 1)
+        std::vector<double> c(cnt.begin(), cnt.end());
+        for (uint64_t ci = 0; ci < k; ++ci) {
+            if (c[ci] != 0) continue;
+            double total = 0;
+            for (uint64_t j = 0; j < k; ++j) total += std::max(c[j] - 1.0, 0.0);
+            uint64_t cj = 0;
+            if (total > 0) {
+                const double u = splitmix64_uniform(rng) * total;
+                double run = 0;
+                for (cj = 0; cj + 1 < k; ++cj) {
+                    run += std::max(c[cj] - 1.0, 0.0);
+                    if (u < run) break;
+                }
+            } else {
+                cj = (uint64_t)(std::max_element(c.begin(), c.end()) - c.begin());
+            }
+            kmeans_split_kernel<<<(unsigned)div_up(dim, 256), 256, 0, st>>>(cent, (int)dim, (int)ci,
+                                                                            (int)cj, 1.f / 1024.f);
+            ERQ_CUDA(cudaGetLastError());
+            c[ci] = std::floor(c[cj] / 2);
+            c[cj] -= c[ci];
+        }
+    }
+    if (final_assign) ERQ_TRY(assign_all());
+    ERQ_CUDA(cudaStreamSynchronize(st));
+    ERQ_TRY(tc_status_check_now());
+    return ERQ_OK;
+}
+
 // ------------------------------------------------- allocation-free search
 // Scratch of erq_search_noalloc: one fixed array in this module's device
 // memory (every GPU that loads the library holds it until the process
@@ -1296,10 +1485,17 @@ erq_status noalloc_scratch(int device, uint8_t** out) {
 uint64_t align256(uint64_t b) { return (b + 255) & ~255ull; }
 
 // Scratch bytes one call needs for nq queries at this nprobe.
+// Sort keys per query of the exact probe beyond shared memory (0: none).
+uint64_t noalloc_sort_cap(const erq_index* idx, uint64_t nprobe) {
+    const int npow2 = next_pow2((int)std::min<uint64_t>(nprobe, idx->K));
+    return npow2 > kProbeSortSmemKeys ? (uint64_t)npow2 : 0;
+}
+
 uint64_t noalloc_bytes(const erq_index* idx, uint64_t nq, uint64_t nprobe) {
     const uint64_t np = nq * nprobe;
     return align256(nq * idx->K * 4) + 2 * align256(np * 4) + align256(np * 8) +
-           align256(nq * 32ull * idx->top_blocks[nprobe] * 4) + 2 * align256(np * 4);
+           align256(nq * 32ull * idx->top_blocks[nprobe] * 4) + 2 * align256(np * 4) +
+           align256(nq * noalloc_sort_cap(idx, nprobe) * 8);
 }
 }  // namespace
 
@@ -1447,6 +1643,8 @@ erq_status erq_search_noalloc(const erq_index* idx, const float* rotated_queries
     b.S = reinterpret_cast<int32_t*>(take(nq * 32ull * idx->top_blocks[nprobe] * 4));
     b.delta = reinterpret_cast<float*>(take(np * 4));
     b.sumq = reinterpret_cast<float*>(take(np * 4));
+    b.sort_cap = noalloc_sort_cap(idx, nprobe);
+    if (b.sort_cap) b.sortbuf = reinterpret_cast<uint64_t*>(take(nq * b.sort_cap * 8));
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     ERQ_TRY(launch_probe(idx, b, nprobe, st));
     ERQ_TRY(launch_scan(idx, b, nprobe, st));
@@ -2040,6 +2238,79 @@ erq_status erq_debug_gemm_bf16(const uint16_t* A, const uint16_t* B, uint64_t M,
     ERQ_CUDA(cudaMemcpy(&st, status, 4, cudaMemcpyDeviceToHost));
     if (st) return fail(ERQ_ERR_TIMEOUT, "a wait in the tcgen05 GEMM reached its limit");
     ERQ_CUDA(cudaMemcpy(C, c, M * N * 4, cudaMemcpyDeviceToHost));
+    return ERQ_OK;
+}
+
+erq_status erq_kmeans(const float* data, uint64_t n, uint64_t dim, uint64_t k, int iters,
+                      uint64_t seed, float* centroids, uint32_t* assign, int device) {
+    if (!data || !centroids) return fail(ERQ_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (n == 0 || dim == 0 || k == 0 || k > n || iters < 0 || n > 0x7fffffffull ||
+        dim > (uint64_t)kMaxD * 8 || k > 0x7fffffffull)
+        return fail(ERQ_ERR_INVALID_ARGUMENT, "bad k-means shape (n=%llu dim=%llu k=%llu)",
+                    (unsigned long long)n, (unsigned long long)dim, (unsigned long long)k);
+    DeviceGuard guard;
+    ERQ_TRY(guard.set(device));
+    cudaStream_t st = nullptr;
+    KmBuffers b;
+    const float* x = data;
+    if (!is_device_ptr(data)) {
+        float* xd = nullptr;
+        ERQ_TRY(b.alloc(&xd, n * dim));
+        ERQ_CUDA(cudaMemcpy(xd, data, n * dim * sizeof(float), cudaMemcpyHostToDevice));
+        x = xd;
+    }
+    float* cent = nullptr;
+    uint32_t* asg = nullptr;
+    uint64_t* rows = nullptr;
+    ERQ_TRY(b.alloc(&cent, k * dim));
+    ERQ_TRY(b.alloc(&asg, n));
+    ERQ_TRY(b.alloc(&rows, k));
+    // initial centroids: k distinct points (partial Fisher-Yates shuffle)
+    uint64_t rng = seed;
+    {
+        std::vector<uint64_t> perm(n);
+        std::iota(perm.begin(), perm.end(), 0ull);
+        for (uint64_t i = 0; i < k; ++i) std::swap(perm[i], perm[i + splitmix64_next(rng) % (n - i)]);
+        ERQ_CUDA(cudaMemcpy(rows, perm.data(), k * sizeof(uint64_t), cudaMemcpyHostToDevice));
+    }
+    gather_rows_kernel<<<1184, 256, 0, st>>>(x, (int)dim, rows, (int)k, cent);
+    ERQ_CUDA(cudaGetLastError());
+    ERQ_TRY(km_iterate(x, n, dim, k, iters, cent, asg, rng, nullptr, true, st));
+    ERQ_CUDA(cudaMemcpy(centroids, cent, k * dim * sizeof(float), cudaMemcpyDefault));
+    if (assign) ERQ_CUDA(cudaMemcpy(assign, asg, n * sizeof(uint32_t), cudaMemcpyDefault));
+    return ERQ_OK;
+}
+
+erq_status erq_kmeans_step(const float* data, uint64_t n, uint64_t dim, uint64_t k,
+                           const float* centroids_in, uint64_t seed, float* centroids_out,
+                           uint32_t* assign, uint32_t* counts, int device) {
+    if (!data || !centroids_in || !centroids_out || !assign || !counts)
+        return fail(ERQ_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (n == 0 || dim == 0 || k == 0 || n > 0x7fffffffull || dim > (uint64_t)kMaxD * 8 ||
+        k > 0x7fffffffull)
+        return fail(ERQ_ERR_INVALID_ARGUMENT, "bad k-means shape");
+    DeviceGuard guard;
+    ERQ_TRY(guard.set(device));
+    cudaStream_t st = nullptr;
+    KmBuffers b;
+    const float* x = data;
+    if (!is_device_ptr(data)) {
+        float* xd = nullptr;
+        ERQ_TRY(b.alloc(&xd, n * dim));
+        ERQ_CUDA(cudaMemcpy(xd, data, n * dim * sizeof(float), cudaMemcpyHostToDevice));
+        x = xd;
+    }
+    float* cent = nullptr;
+    uint32_t* asg = nullptr;
+    ERQ_TRY(b.alloc(&cent, k * dim));
+    ERQ_TRY(b.alloc(&asg, n));
+    ERQ_CUDA(cudaMemcpy(cent, centroids_in, k * dim * sizeof(float), cudaMemcpyDefault));
+    uint64_t rng = seed;
+    std::vector<uint32_t> cnt(k);
+    ERQ_TRY(km_iterate(x, n, dim, k, 1, cent, asg, rng, cnt.data(), false, st));
+    ERQ_CUDA(cudaMemcpy(centroids_out, cent, k * dim * sizeof(float), cudaMemcpyDefault));
+    ERQ_CUDA(cudaMemcpy(assign, asg, n * sizeof(uint32_t), cudaMemcpyDefault));
+    ERQ_CUDA(cudaMemcpy(counts, cnt.data(), k * sizeof(uint32_t), cudaMemcpyDefault));
     return ERQ_OK;
 }
 

@@ -45,11 +45,17 @@ struct ProbeArgs {
     int check_rank;           // rank whose exactness the bound check proves (>= nprobe)
     int stage_keys;           // nonzero: probe_kernel copies the K order keys to shared
                               // memory once (K <= kProbeStageKeys)
+    uint64_t* sort_global;    // optional [nq][sort_cap]: sort keys in global memory, for
+                              // selections too large for shared memory
+    uint64_t sort_cap;        // keys per query in sort_global
+    float* exact_rows;        // [nq][K]: probe_exact_kernel's exact distances (it may
+                              // overwrite the estimates there)
 };
 
 constexpr int kProbeThreads = 256;
 constexpr int kProbeFeatRank = 64;  // estimates written to near_d
 constexpr int kProbeStageKeys = 4096;  // largest K whose keys are staged in shared memory
+constexpr int kProbeSortSmemKeys = 16384;  // largest sort kept in shared memory (128 KB)
 
 __device__ __forceinline__ uint32_t order_key(float f) {
     const uint32_t b = __float_as_uint(f);
@@ -171,13 +177,64 @@ __device__ __forceinline__ void sort_prefix(uint64_t* keys, int n) {
 // [Spow2] | hist[256] | misc.  Kst = K rounded up to even when the keys are
 // staged (stage_keys), else 0 and each radix pass re-reads the estimates
 // from global memory.  Spow2 is a power of two >= the number of selected
-// candidates (max(M, 64) with features, else M; K when all are selected).
+// candidates (max(M, 64) with features, else M; K when all are selected);
+// above kProbeSortSmemKeys the sort keys live in sort_global instead (pass
+// Spow2 = 0 here).
 __host__ __device__ constexpr size_t probe_smem_bytes(int D, int Spow2, int Kst) {
     return (size_t)D * 4 + (size_t)((Kst + 1) & ~1) * 4 + (size_t)Spow2 * 8 + 256 * 4 + 64;
 }
-// probe_fallback_kernel: q[D] | sort keys u64 [Kpow2]
-__host__ __device__ constexpr size_t probe_fallback_smem_bytes(int D, int Kpow2) {
-    return (size_t)D * 4 + (size_t)Kpow2 * 8 + 64;
+// probe_exact_kernel: q[D] | hist[256] | misc | sort keys u64 [Npow2] (0 when
+// they live in sort_global)
+__host__ __device__ constexpr size_t probe_exact_smem_bytes(int D, int Npow2) {
+    return (size_t)D * 4 + 256 * 4 + 64 + (size_t)Npow2 * 8;
+}
+
+// Radix select (8 bits per pass) of the rank-th smallest of the K order keys
+// key_of(0..K-1), rank in 1..K; by the whole block, returns synchronised.
+template <typename KeyOf>
+__device__ uint32_t radix_select_key(KeyOf key_of, int K, int rank, uint32_t* hist, int* misc) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    uint32_t prefix = 0, pmask = 0;
+    for (int shift = 24; shift >= 0; shift -= 8) {
+        for (int i = tid; i < 256; i += blockDim.x) hist[i] = 0;
+        __syncthreads();
+        for (int c = tid; c < K; c += blockDim.x) {
+            const uint32_t kk = key_of(c);
+            if ((kk & pmask) == prefix) atomicAdd(&hist[(kk >> shift) & 255u], 1u);
+        }
+        __syncthreads();
+        if (warp == 0) {
+            uint32_t h[8], s = 0;
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                h[i] = hist[8 * lane + i];
+                s += h[i];
+            }
+            uint32_t incl = s;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += v;
+            }
+            const uint32_t excl = incl - s;
+            if (excl < (uint32_t)rank && incl >= (uint32_t)rank) {
+                uint32_t run = excl;
+                int d = 0;
+                for (; d < 8; ++d) {
+                    if (run + h[d] >= (uint32_t)rank) break;
+                    run += h[d];
+                }
+                misc[0] = 8 * lane + d;
+                misc[1] = (int)run;
+            }
+        }
+        __syncthreads();
+        prefix |= (uint32_t)misc[0] << shift;
+        pmask |= 0xffu << shift;
+        rank -= misc[1];
+        __syncthreads();
+    }
+    return prefix;
 }
 
 // Outputs of one query from its sorted (distance, id) keys, and the exclusive
@@ -214,9 +271,10 @@ __global__ void __launch_bounds__(kProbeThreads) probe_kernel(ProbeArgs a) {
     float* qs = reinterpret_cast<float*>(smem_raw);
     uint32_t* ks = reinterpret_cast<uint32_t*>(qs + D);
     const int Kst = a.stage_keys ? (K + 1) & ~1 : 0;
-    uint64_t* sk = reinterpret_cast<uint64_t*>(ks + Kst);
-    uint32_t* hist = reinterpret_cast<uint32_t*>(sk + a.Spow2);
+    uint64_t* sk_s = reinterpret_cast<uint64_t*>(ks + Kst);
+    uint32_t* hist = reinterpret_cast<uint32_t*>(sk_s + (a.sort_global ? 0 : a.Spow2));
     int* misc = reinterpret_cast<int*>(hist + 256);  // [0] digit [1] before [2] count [3] ok
+    uint64_t* sk = a.sort_global ? a.sort_global + (size_t)q * a.sort_cap : sk_s;
 
     for (int i = tid; i < D; i += blockDim.x) qs[chain_pos(i)] = a.qrot[(size_t)q * D + i];
     const float* aq = a.approx + (size_t)q * K;
@@ -231,52 +289,7 @@ __global__ void __launch_bounds__(kProbeThreads) probe_kernel(ProbeArgs a) {
     const int Msel = a.near_d ? max(M, kProbeFeatRank) : M;
     const bool select_all = Msel + 1 > K;
     uint32_t kstar = 0xffffffffu;
-    if (!select_all) {
-        // radix select of the (Msel+1)-th smallest key, 8 bits at a time
-        uint32_t prefix = 0, pmask = 0;
-        int rank = Msel + 1;
-        for (int shift = 24; shift >= 0; shift -= 8) {
-            for (int i = tid; i < 256; i += blockDim.x) hist[i] = 0;
-            __syncthreads();
-            for (int c = tid; c < K; c += blockDim.x) {
-                const uint32_t kk = key_of(c);
-                if ((kk & pmask) == prefix) atomicAdd(&hist[(kk >> shift) & 255u], 1u);
-            }
-            __syncthreads();
-            if (warp == 0) {
-                uint32_t h[8], s = 0;
-#pragma unroll
-                for (int i = 0; i < 8; ++i) {
-                    h[i] = hist[8 * lane + i];
-                    s += h[i];
-                }
-                uint32_t incl = s;
-#pragma unroll
-                for (int o = 1; o < 32; o <<= 1) {
-                    const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
-                    if (lane >= o) incl += v;
-                }
-                const uint32_t excl = incl - s;
-                const bool here = excl < (uint32_t)rank && incl >= (uint32_t)rank;
-                if (here) {
-                    uint32_t run = excl;
-                    int d = 0;
-                    for (; d < 8; ++d) {
-                        if (run + h[d] >= (uint32_t)rank) break;
-                        run += h[d];
-                    }
-                    misc[0] = 8 * lane + d;
-                    misc[1] = (int)run;
-                }
-            }
-            __syncthreads();
-            prefix |= (uint32_t)misc[0] << shift;
-            pmask |= 0xffu << shift;
-            rank -= misc[1];
-            __syncthreads();
-        }
-        kstar = prefix;
-    }
+    if (!select_all) kstar = radix_select_key(key_of, K, Msel + 1, hist, misc);
     // candidates: every centroid whose estimate is below the (Msel+1)-th,
     // keyed by (estimate, id)
     if (tid == 0) misc[2] = 0;
@@ -349,28 +362,69 @@ __global__ void __launch_bounds__(kProbeThreads) probe_kernel(ProbeArgs a) {
     if (misc[3] && warp == 0) probe_outputs(a, q, sk, lane);
 }
 
-// The queries whose cut could not be proven: exact distances of all K
-// centroids, sorted by (distance, id).  Other blocks return at once.
-__global__ void __launch_bounds__(kProbeThreads) probe_fallback_kernel(ProbeArgs a) {
+// The exact nprobe nearest centroids of a query, by (distance, id), from all
+// K exact distances - for the queries whose cut probe_kernel could not prove
+// (fallback_flag set; `compute`: the exact L2Sqr16 values are computed here
+// into the query's row of exact_rows, over its estimates), and for the
+// allocation-free search, whose rows already hold them (fallback_flag null,
+// compute 0).  A radix select finds the nprobe-th smallest key; the keys below
+// it and, among those equal to it, the smallest ids fill nprobe slots, which
+// are sorted (FlatInitializer::centroids_distances' partial_sort,
+// inc/index/Initializer.hpp:55-68, with ties by id).  Sort keys live in
+// shared memory up to kProbeSortSmemKeys, else in sort_global.
+__global__ void __launch_bounds__(kProbeThreads) probe_exact_kernel(ProbeArgs a, int compute, int Npow2) {
     const int q = blockIdx.x;
-    if (!a.fallback_flag[q]) return;
+    if (a.fallback_flag && !a.fallback_flag[q]) return;
     extern __shared__ __align__(16) uint8_t smem_raw[];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int K = a.K, D = a.D;
+    const int K = a.K, D = a.D, n = min(a.nprobe, K);
     float* qs = reinterpret_cast<float*>(smem_raw);
-    uint64_t* sk = reinterpret_cast<uint64_t*>(qs + D);
-    for (int i = tid; i < D; i += blockDim.x) qs[chain_pos(i)] = a.qrot[(size_t)q * D + i];
+    uint32_t* hist = reinterpret_cast<uint32_t*>(qs + D);
+    int* misc = reinterpret_cast<int*>(hist + 256);
+    uint64_t* sk = a.sort_global ? a.sort_global + (size_t)q * a.sort_cap
+                                 : reinterpret_cast<uint64_t*>(misc + 16);
+    float* row = a.exact_rows + (size_t)q * K;
+    if (compute) {
+        for (int i = tid; i < D; i += blockDim.x) qs[chain_pos(i)] = a.qrot[(size_t)q * D + i];
+        __syncthreads();
+        const int hw = tid >> 4, l = tid & 15, nhw = blockDim.x >> 4;
+        for (int base = 0; base < K; base += nhw) {
+            const int c = base + hw;
+            const float e = l2sqr16_chain(reinterpret_cast<const float4*>(qs),
+                                          reinterpret_cast<const float4*>(a.centroids + (size_t)min(c, K - 1) * D), D, l);
+            if (l == 0 && c < K) row[c] = e;
+        }
+        __syncthreads();
+    }
+    auto key_of = [&](int c) -> uint32_t { return order_key(row[c]); };
+    const uint32_t kstar = radix_select_key(key_of, K, n, hist, misc);
+    if (tid == 0) misc[2] = 0;
     __syncthreads();
-    const int hw = tid >> 4, l = tid & 15, nhw = blockDim.x >> 4;
-    for (int base = 0; base < K; base += nhw) {
-        const int c = base + hw;
-        const float e = l2sqr16_chain(reinterpret_cast<const float4*>(qs), reinterpret_cast<const float4*>(a.centroids + (size_t)min(c, K - 1) * D), D, l);
-        if (l == 0 && c < K) sk[c] = dist_key(e, (uint32_t)c);
+    for (int c = tid; c < K; c += blockDim.x) {
+        const uint32_t kk = key_of(c);
+        if (kk < kstar) sk[atomicAdd(&misc[2], 1)] = dist_key(order_key_value(kk), (uint32_t)c);
     }
     __syncthreads();
-    for (int i = K + tid; i < a.Kpow2; i += blockDim.x) sk[i] = ~0ull;
+    if (warp == 0) {  // ties at the cut: the smallest ids, in ascending order
+        int have = misc[2];
+        for (int base = 0; base < K && have < n; base += 32) {
+            const int c = base + lane;
+            const bool eq = c < K && key_of(c) == kstar;
+            const uint32_t m = __ballot_sync(0xffffffffu, eq);
+            const int r = __popc(m & ((1u << lane) - 1u));
+            if (eq && have + r < n) sk[have + r] = dist_key(order_key_value(kstar), (uint32_t)c);
+            have += __popc(m);
+        }
+    }
     __syncthreads();
-    block_bitonic_sort(sk, a.Kpow2);
+    for (int i = n + tid; i < Npow2; i += blockDim.x) sk[i] = ~0ull;
+    __syncthreads();
+    if (Npow2 <= 64) {
+        if (warp == 0) warp_sort64(sk, n, lane);
+        __syncthreads();
+    } else {
+        block_bitonic_sort(sk, Npow2);
+    }
     if (warp == 0) probe_outputs(a, q, sk, lane);
 }
 

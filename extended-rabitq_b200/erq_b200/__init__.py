@@ -10,6 +10,7 @@ include/erq.h); this package is its Python host side:
 * ``metrics``   - recall@k and the reference's average distance ratio
 * ``plan``      - batched, graph-captured, autotuned search plans
 * ``learned``   - learned probing (probe MLP)
+* ``clustering`` - IVF clustering (k-means) on the GPU
 """
 from ._lib import EXPORTED_SYMBOLS, ErqError, load_library  # noqa: F401
 from .ivf import IVF  # noqa: F401

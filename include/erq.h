@@ -201,6 +201,30 @@ ERQ_API erq_status erq_plan_set_graphs(erq_plan* plan, int on);
  * never split.  Results are the same in every case. */
 ERQ_API erq_status erq_plan_set_pipeline(erq_plan* plan, int chunks);
 
+/* ---------------------------------------------------------------------------
+ * IVF clustering.  Replaces the reference's offline clustering step
+ * (python/ivf.py:5-34, faiss IVF{K},Flat training = Lloyd's k-means with
+ * random initial centroids drawn from the data and empty clusters re-seeded
+ * by splitting a populated one), whose centroid and cluster-id files feed
+ * create_index.  Distances on the tensor cores (split-BF16, about FP32
+ * accuracy), centroid sums in 64-bit fixed point (deterministic: the same
+ * seed gives the same clusters), splitmix64 as the random stream.  Buffers
+ * may be host or device memory; the calls are synchronous. */
+
+/* k-means of data[n][dim] into k clusters: `iters` Lloyd iterations from k
+ * distinct random points, then a last assignment.  centroids: [k][dim];
+ * assign (optional): [n], the nearest final centroid of each point. */
+ERQ_API erq_status erq_kmeans(const float* data, uint64_t n, uint64_t dim, uint64_t k, int iters,
+                              uint64_t seed, float* centroids, uint32_t* assign, int device);
+/* One Lloyd iteration from centroids_in: assign[n] (nearest centroid, ties to
+ * the smaller index), counts[k] (cluster sizes of that assignment),
+ * centroids_out = the means, then the empty clusters split with the random
+ * stream started at `seed`. */
+ERQ_API erq_status erq_kmeans_step(const float* data, uint64_t n, uint64_t dim, uint64_t k,
+                                   const float* centroids_in, uint64_t seed,
+                                   float* centroids_out, uint32_t* assign, uint32_t* counts,
+                                   int device);
+
 /* erq_search without any memory allocation.  Has no counterpart in the
  * reference: it is for callers that cannot allocate device memory while a
  * query runs - engines that hand all GPU memory to their own allocator up
