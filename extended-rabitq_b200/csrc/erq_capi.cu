@@ -35,6 +35,7 @@
 #include "mlp.cuh"
 #include "probe.cuh"
 #include "layout.cuh"
+#include "lowacc.cuh"
 #include "refine.cuh"
 #include "order.cuh"
 #include "scan.cuh"
@@ -214,6 +215,12 @@ struct erq_index {
     uint64_t ex_row = 0;
     float* xipnorm = nullptr;
     uint32_t* ids = nullptr;
+    // 4 factors per vector: the reference's format without HIGH_ACC_FAST_SCAN
+    // (onorm then holds ||o - c||^2; lowacc.cuh)
+    int factors = 1;
+    float* fac_ip = nullptr;
+    float* fac_sumxb = nullptr;
+    float* fac_err = nullptr;
     uint32_t* c_first_block = nullptr;
     uint32_t* c_first_vec = nullptr;
     uint32_t* c_size = nullptr;
@@ -240,7 +247,7 @@ struct erq_index {
         for (void* p : {(void*)P, (void*)centroids, (void*)codes, (void*)onorm, (void*)excode,
                         (void*)xipnorm, (void*)ids, (void*)c_first_block, (void*)c_first_vec,
                         (void*)c_size, (void*)c_nblocks, (void*)c_size_rank, (void*)c_split, (void*)pt_split,
-                        (void*)cn, (void*)c_chain})
+                        (void*)cn, (void*)c_chain, (void*)fac_ip, (void*)fac_sumxb, (void*)fac_err})
             if (p) cudaFree(p);
         if (prev >= 0) cudaSetDevice(prev);
     }
@@ -335,9 +342,28 @@ erq_status load_impl(const char* path, erq_index* idx) {
         idx->top_blocks.assign(K + 1, 0);
         for (uint64_t i = 0; i < K; ++i) idx->top_blocks[i + 1] = idx->top_blocks[i] + nbs[i];
     }
-    // expected remaining size: P, centroids, short data, long codes, factors, ids
+    // The remaining bytes - P, centroids, short data, long codes, factors,
+    // ids - tell the two block formats apart: 1 factor per vector
+    // (HIGH_ACC_FAST_SCAN, the reference drivers' format) or 4.
     const uint64_t code_len = D * EX / 8;
-    const uint64_t raw_block = 4 * D + kFastSize * sizeof(float);
+    {
+        const long here = ftell(f.get());
+        if (here < 0 || fseek(f.get(), 0, SEEK_END) != 0)
+            return fail(ERQ_ERR_IO, "cannot size index file '%s'", path);
+        const uint64_t rest = (uint64_t)ftell(f.get()) - (uint64_t)here;
+        if (fseek(f.get(), here, SEEK_SET) != 0) return fail(ERQ_ERR_IO, "seek failed in '%s'", path);
+        auto need = [&](uint64_t F) {
+            return (D * D + K * D) * 4 + blocks * (4 * D + kFastSize * 4 * F) + N * (code_len + 8);
+        };
+        if (rest == need(1)) idx->factors = 1;
+        else if (rest == need(4)) idx->factors = 4;
+        else
+            return fail(ERQ_ERR_FORMAT, "index file '%s' holds %llu bytes after its cluster table; "
+                        "%llu (one block factor) or %llu (four) expected", path,
+                        (unsigned long long)rest, (unsigned long long)need(1),
+                        (unsigned long long)need(4));
+    }
+    const uint64_t raw_block = 4 * D + kFastSize * sizeof(float) * idx->factors;
 
     std::vector<uint8_t> staging(64ull << 20);
     ERQ_TRY(dev_alloc(idx, &idx->P, D * D));
@@ -351,8 +377,14 @@ erq_status load_impl(const char* path, erq_index* idx) {
         erq_status s = read_to_device(f.get(), raw, blocks * raw_block, staging, "the short codes");
         if (s == ERQ_OK) s = dev_alloc(idx, &idx->codes, blocks * code_block_bytes((int)D));
         if (s == ERQ_OK) s = dev_alloc(idx, &idx->onorm, blocks * kFastSize);
+        if (s == ERQ_OK && idx->factors == 4) s = dev_alloc(idx, &idx->fac_ip, blocks * kFastSize);
+        if (s == ERQ_OK && idx->factors == 4) s = dev_alloc(idx, &idx->fac_sumxb, blocks * kFastSize);
+        if (s == ERQ_OK && idx->factors == 4) s = dev_alloc(idx, &idx->fac_err, blocks * kFastSize);
         if (s == ERQ_OK && blocks > 0) {
-            transform_blocks_kernel<<<1184, 256>>>(raw, idx->codes, idx->onorm, blocks, (int)D);
+            float* extra[3] = {idx->fac_ip, idx->fac_sumxb, idx->fac_err};
+            transform_blocks_kernel<<<1184, 256>>>(raw, idx->codes, idx->onorm, blocks, (int)D,
+                                                   idx->factors, idx->factors == 4 ? 4 : 2,
+                                                   extra[0], extra[1], extra[2]);
             e = cudaGetLastError();
             if (e == cudaSuccess) e = cudaDeviceSynchronize();
             if (e != cudaSuccess)
@@ -501,6 +533,17 @@ erq_status configure_kernels(int D, int K, int k) {
                                                         K <= kProbeStageKeys ? K : 0)));
     ERQ_CUDA(cudaFuncSetAttribute(probe_exact_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)probe_exact_smem_bytes(D, std::min(kp2, kProbeSortSmemKeys))));
+    ERQ_CUDA(cudaFuncSetAttribute(scan_lowacc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)low_scan_smem_bytes(D)));
+    {
+        const int smem = (int)(kLowRefineWarps * low_refine_smem_per_warp(D, kMaxTopK));
+        ERQ_CUDA(cudaFuncSetAttribute(refine_lowacc_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        ERQ_CUDA(cudaFuncSetAttribute(refine_lowacc_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        ERQ_CUDA(cudaFuncSetAttribute(refine_lowacc_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        ERQ_CUDA(cudaFuncSetAttribute(refine_lowacc_kernel<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        ERQ_CUDA(cudaFuncSetAttribute(refine_lowacc_kernel<7>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        ERQ_CUDA(cudaFuncSetAttribute(refine_lowacc_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    }
     ERQ_TRY(configure_refine<2>(D));
     ERQ_TRY(configure_refine<3>(D));
     ERQ_TRY(configure_refine<4>(D));
@@ -656,6 +699,7 @@ struct Batch {
     int32_t* S = nullptr;
     float* delta = nullptr;
     float* sumq = nullptr;
+    float* vl = nullptr;              // [nq][nprobe] lower query range end (4-factor format)
     __nv_bfloat16* qsplit = nullptr;  // [nq][3D] split rotated queries
     float* qn = nullptr;              // [nq]
     // work order (order.cuh)
@@ -689,7 +733,7 @@ uint64_t probe_sort_cap(const erq_index* idx, uint64_t nprobe, bool features) {
 // Largest query batch whose scan workspace fits the budget.
 uint64_t batch_queries(const erq_index* idx, uint64_t nprobe, uint64_t nq) {
     const uint64_t per_q = 32ull * idx->top_blocks[nprobe] * sizeof(int32_t) +
-                           idx->K * sizeof(float) + nprobe * 24 + 6 * idx->D + 4 +
+                           idx->K * sizeof(float) + nprobe * 28 + 6 * idx->D + 4 +
                            idx->top_blocks[nprobe] * sizeof(float);
     const uint64_t per_q_all = per_q + probe_sort_cap(idx, nprobe, true) * sizeof(uint64_t);
     const uint64_t budget = 3ull << 30;
@@ -707,6 +751,7 @@ erq_status alloc_batch(Alloc& s, const erq_index* idx, uint64_t nq, uint64_t npr
     ERQ_TRY(s.alloc(&b.S, nq * 32ull * idx->top_blocks[nprobe]));
     ERQ_TRY(s.alloc(&b.delta, nq * nprobe));
     ERQ_TRY(s.alloc(&b.sumq, nq * nprobe));
+    ERQ_TRY(s.alloc(&b.vl, nq * nprobe));
     ERQ_TRY(s.alloc(&b.qsplit, nq * 3 * idx->D));
     ERQ_TRY(s.alloc(&b.qn, nq));
     ERQ_TRY(s.alloc(&b.keys, nq * nprobe));
@@ -913,8 +958,53 @@ erq_status launch_probe(const erq_index* idx, const Batch& b, uint64_t nprobe, c
     return ERQ_OK;
 }
 
+LowFactors low_factors(const erq_index* idx) {
+    LowFactors f;
+    f.x2 = idx->onorm;
+    f.fip = idx->fac_ip;
+    f.sumxb = idx->fac_sumxb;
+    f.ferr = idx->fac_err;
+    return f;
+}
+
+// The scan of the 4-factor format (lowacc.cuh): width, vl and sum(q - c)/2
+// land in b.delta, b.vl and b.sumq.
+erq_status launch_scan_lowacc(const erq_index* idx, const Batch& b, uint64_t nprobe, cudaStream_t st) {
+    LowScanArgs a{};
+    a.qrot = b.qrot;
+    a.centroids = idx->centroids;
+    a.probe_cid = b.probe_cid;
+    a.probe_sqy = b.probe_sqy;
+    a.codes = idx->codes;
+    a.c_first_block = idx->c_first_block;
+    a.c_nblocks = idx->c_nblocks;
+    a.c_size = idx->c_size;
+    a.s_off = b.s_off;
+    a.S = b.S;
+    a.qp_width = b.delta;
+    a.qp_vl = b.vl;
+    a.qp_half = b.sumq;
+    a.bmin = b.bmin;
+    a.f = low_factors(idx);
+    a.D = (int)idx->D;
+    a.nprobe = (int)nprobe;
+    ERQ_TRY(tc_status_ptr(&a.status));
+    const uint64_t pairs = b.nq * nprobe;
+    if (pairs > 0x7fffffffull) return fail(ERQ_ERR_INVALID_ARGUMENT, "too many (query, probe) pairs");
+    LaunchTimer t(kScan, st);
+    scan_lowacc_kernel<<<(unsigned)pairs, kScanWarps * 32, low_scan_smem_bytes(a.D), st>>>(a);
+    t.finish();
+    ERQ_CUDA(cudaGetLastError());
+    return ERQ_OK;
+}
+
 erq_status launch_scan(const erq_index* idx, const Batch& b, uint64_t nprobe, cudaStream_t st,
                        const int* q_nprobe = nullptr, const uint32_t* order = nullptr) {
+    if (idx->factors == 4) {
+        if (q_nprobe || order)
+            return fail(ERQ_ERR_UNSUPPORTED, "per-query depths and work orders take one-factor indexes");
+        return launch_scan_lowacc(idx, b, nprobe, st);
+    }
     ScanArgs a{};
     a.order = order;
     a.onorm = idx->onorm;
@@ -950,6 +1040,51 @@ erq_status launch_refine(const erq_index* idx, const Batch& b, uint64_t nprobe, 
                          uint32_t* out_ids, float* out_dists, cudaStream_t st,
                          const int* q_nprobe = nullptr, const uint32_t* order = nullptr,
                          int refine_warps = 0) {
+    if (idx->factors == 4) {
+        if (q_nprobe || order)
+            return fail(ERQ_ERR_UNSUPPORTED, "per-query depths and work orders take one-factor indexes");
+        LowRefineArgs a{};
+        a.qrot = b.qrot;
+        a.centroids = idx->centroids;
+        a.probe_cid = b.probe_cid;
+        a.probe_sqy = b.probe_sqy;
+        a.s_off = b.s_off;
+        a.S = b.S;
+        a.qp_width = b.delta;
+        a.qp_vl = b.vl;
+        a.qp_half = b.sumq;
+        a.bmin = b.bmin;
+        a.f = low_factors(idx);
+        a.excode = idx->excode;
+        a.ex_row = idx->ex_row;
+        a.xipnorm = idx->xipnorm;
+        a.ids = idx->ids;
+        a.c_first_block = idx->c_first_block;
+        a.c_first_vec = idx->c_first_vec;
+        a.c_size = idx->c_size;
+        a.out_ids = out_ids;
+        a.out_dists = out_dists;
+        a.nq = (int)b.nq;
+        a.D = (int)idx->D;
+        a.EX = (int)idx->EX;
+        a.nprobe = (int)nprobe;
+        a.k = (int)k;
+        const unsigned grid = (unsigned)div_up(b.nq, kLowRefineWarps);
+        const size_t smem = kLowRefineWarps * low_refine_smem_per_warp(a.D, (a.k + 31) & ~31);
+        LaunchTimer t(kRefine, st);
+        switch (idx->EX) {
+            case 2: refine_lowacc_kernel<2><<<grid, kLowRefineWarps * 32, smem, st>>>(a); break;
+            case 3: refine_lowacc_kernel<3><<<grid, kLowRefineWarps * 32, smem, st>>>(a); break;
+            case 4: refine_lowacc_kernel<4><<<grid, kLowRefineWarps * 32, smem, st>>>(a); break;
+            case 6: refine_lowacc_kernel<6><<<grid, kLowRefineWarps * 32, smem, st>>>(a); break;
+            case 7: refine_lowacc_kernel<7><<<grid, kLowRefineWarps * 32, smem, st>>>(a); break;
+            case 8: refine_lowacc_kernel<8><<<grid, kLowRefineWarps * 32, smem, st>>>(a); break;
+            default: return fail(ERQ_ERR_FORMAT, "bad EX");
+        }
+        t.finish();
+        ERQ_CUDA(cudaGetLastError());
+        return ERQ_OK;
+    }
     RefineArgs a{};
     a.order = order;
     a.bmin = b.bmin;
@@ -1494,7 +1629,7 @@ uint64_t noalloc_sort_cap(const erq_index* idx, uint64_t nprobe) {
 uint64_t noalloc_bytes(const erq_index* idx, uint64_t nq, uint64_t nprobe) {
     const uint64_t np = nq * nprobe;
     return align256(nq * idx->K * 4) + 2 * align256(np * 4) + align256(np * 8) +
-           align256(nq * 32ull * idx->top_blocks[nprobe] * 4) + 2 * align256(np * 4) +
+           align256(nq * 32ull * idx->top_blocks[nprobe] * 4) + 3 * align256(np * 4) +
            align256(nq * noalloc_sort_cap(idx, nprobe) * 8);
 }
 }  // namespace
@@ -1549,6 +1684,7 @@ erq_status erq_index_get_info(const erq_index* idx, erq_index_info* info) {
     info->ex_bits = idx->EX;
     info->device_bytes = idx->device_bytes;
     info->device = idx->device;
+    info->block_factors = idx->factors;
     return ERQ_OK;
 }
 
@@ -1643,6 +1779,7 @@ erq_status erq_search_noalloc(const erq_index* idx, const float* rotated_queries
     b.S = reinterpret_cast<int32_t*>(take(nq * 32ull * idx->top_blocks[nprobe] * 4));
     b.delta = reinterpret_cast<float*>(take(np * 4));
     b.sumq = reinterpret_cast<float*>(take(np * 4));
+    b.vl = reinterpret_cast<float*>(take(np * 4));
     b.sort_cap = noalloc_sort_cap(idx, nprobe);
     if (b.sort_cap) b.sortbuf = reinterpret_cast<uint64_t*>(take(nq * b.sort_cap * 8));
     cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -2021,6 +2158,9 @@ static erq_status search_learned_entry(const erq_index* idx, const erq_probe_mod
     if (!m) return fail(ERQ_ERR_INVALID_ARGUMENT, "model is NULL");
     const float* rotated_queries = queries;
     ERQ_TRY(check_search_args(idx, nq, k, nprobe_fallback, queries, ids));
+    if (idx->factors != 1)
+        return fail(ERQ_ERR_UNSUPPORTED,
+                    "learned probing takes indexes in the HIGH_ACC_FAST_SCAN format (one block factor)");
     if (nq == 0) return ERQ_OK;
     if (m->device != idx->device)
         return fail(ERQ_ERR_INVALID_ARGUMENT, "model and index are on different devices");
@@ -2772,6 +2912,9 @@ erq_status erq_plan_create(const erq_index* idx, const erq_probe_model* model, u
     if (!out) return fail(ERQ_ERR_INVALID_ARGUMENT, "out is NULL");
     *out = nullptr;
     if (!idx) return fail(ERQ_ERR_INVALID_ARGUMENT, "index is NULL");
+    if (idx->factors != 1)
+        return fail(ERQ_ERR_UNSUPPORTED,
+                    "batched plans take indexes in the HIGH_ACC_FAST_SCAN format (one block factor)");
     if (max_batch == 0) return fail(ERQ_ERR_INVALID_ARGUMENT, "max_batch must be positive");
     if (k == 0 || k > (uint64_t)kMaxTopK)
         return fail(ERQ_ERR_INVALID_ARGUMENT, "k=%llu outside 1..%d", (unsigned long long)k, kMaxTopK);

@@ -45,12 +45,17 @@ __device__ __forceinline__ uint32_t fastscan_byte_of(uint32_t v) {
     return w < 8 ? 2 * w : 2 * (w - 8) + 1;
 }
 
-// One thread per output byte of the code region.
+// One thread per output byte of the code region.  `factors` per vector in
+// the file block (1, or 4 without HIGH_ACC_FAST_SCAN: factor 0 goes to onorm,
+// 1-3 to f1..f3); `entry_bytes` of the scan's table entries: 2 (code byte
+// 2 idx + 128 (i & 1), scan.cuh) or 4 (code byte 4 idx, lowacc.cuh).
 __global__ void transform_blocks_kernel(const uint8_t* __restrict__ raw,
                                         uint8_t* __restrict__ codes,
-                                        float* __restrict__ onorm, uint64_t nblocks, int D) {
+                                        float* __restrict__ onorm, uint64_t nblocks, int D,
+                                        int factors, int entry_bytes, float* __restrict__ f1,
+                                        float* __restrict__ f2, float* __restrict__ f3) {
     const uint64_t file_code = 4ull * D;
-    const uint64_t raw_block = file_code + kFastSize * sizeof(float);
+    const uint64_t raw_block = file_code + kFastSize * sizeof(float) * factors;
     const uint32_t bb = code_block_bytes(D);
     const uint64_t total = nblocks * bb;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total;
@@ -70,16 +75,25 @@ __global__ void transform_blocks_kernel(const uint8_t* __restrict__ raw,
             const uint32_t nib = hi ? (x >> 4) : (x & 15u);
             idx |= ((nib >> (3 - rr)) & 1u) << j;  // nibble bit 3 = dim 4g + 0
         }
-        codes[i] = (uint8_t)(2 * idx + 128 * (byte & 1));
+        codes[i] = (uint8_t)(entry_bytes == 4 ? 4 * idx : 2 * idx + 128 * (byte & 1));
     }
     const uint64_t nf = nblocks * kFastSize;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nf;
          i += (uint64_t)gridDim.x * blockDim.x) {
         const uint64_t b = i / kFastSize;
         const uint32_t v = (uint32_t)(i - b * kFastSize);
+        const uint8_t* fac = raw + b * raw_block + file_code;
         float f;
-        memcpy(&f, raw + b * raw_block + file_code + 4ull * v, sizeof(float));
+        memcpy(&f, fac + 4ull * v, sizeof(float));
         onorm[i] = f;
+        if (factors == 4) {
+            memcpy(&f, fac + 4ull * (kFastSize + v), sizeof(float));
+            f1[i] = f;
+            memcpy(&f, fac + 4ull * (2 * kFastSize + v), sizeof(float));
+            f2[i] = f;
+            memcpy(&f, fac + 4ull * (3 * kFastSize + v), sizeof(float));
+            f3[i] = f;
+        }
     }
 }
 

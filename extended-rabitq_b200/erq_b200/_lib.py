@@ -70,6 +70,7 @@ class IndexInfo(C.Structure):
         ("ex_bits", C.c_uint64),
         ("device_bytes", C.c_uint64),
         ("device", C.c_int),
+        ("block_factors", C.c_int),
     ]
 
 

@@ -69,6 +69,7 @@ class IVF:
         self.K, self.EX_BITS = int(info.num_clusters), int(info.ex_bits)
         self.device = int(info.device)
         self.device_bytes = int(info.device_bytes)
+        self.block_factors = int(info.block_factors)
 
     def free(self) -> None:
         if self._h:

@@ -55,6 +55,9 @@ typedef struct erq_index_info {
     uint64_t ex_bits;      /* EX_BITS = total bits - 1, one of 2,3,4,6,7,8 */
     uint64_t device_bytes; /* device memory held by the index */
     int device;            /* CUDA device ordinal */
+    int block_factors;     /* factors per vector in a FastScan block: 1 (the reference
+                              drivers' HIGH_ACC_FAST_SCAN format) or 4 (its format
+                              without that define, searched as inc/index/Searcher.hpp) */
 } erq_index_info;
 
 /* Library version (ERQ_API_VERSION) and status text. */
@@ -63,9 +66,12 @@ ERQ_API const char* erq_status_string(erq_status s);
 /* Message of the last failing call on this thread ("" if none). */
 ERQ_API const char* erq_last_error(void);
 
-/* Load an index file (the reference's IVF::save format, HIGH_ACC_FAST_SCAN
- * layout) onto CUDA device `device`.  Rejects K >= 20000 (the reference then
- * needs an HNSW side file) and D > 2048. */
+/* Load an index file (the reference's IVF::save format) onto CUDA device
+ * `device`.  Reads both block formats the reference
+ * writes (one factor per vector with HIGH_ACC_FAST_SCAN, four without; told
+ * apart by the file size).  Any K: for K >= 20000 the reference probes with an
+ * HNSW graph from a side file, which is not read here - the probe stays exact
+ * (the Flat semantics, inc/index/Initializer.hpp:55-68).  Rejects D > 2048. */
 ERQ_API erq_status erq_index_load(const char* path, int device, erq_index** out);
 ERQ_API erq_status erq_index_get_info(const erq_index* index, erq_index_info* info);
 ERQ_API void erq_index_free(erq_index* index);

@@ -299,3 +299,78 @@ class Reference:
     @classmethod
     def max_threads(cls, stock: bool = False):
         return int(cls.lib(stock).ref_max_threads())
+
+
+REF_LOWACC_SO = os.path.join(HERE, "_ref", "liberq_ref_lowacc.so")
+
+
+class LowAccReference:
+    """The reference's non-HIGH_ACC format and Searcher (oracle/ref_lowacc.cpp):
+    builds indexes with IVF::construct + save and searches them with the
+    reference's own Searcher (inc/index/Searcher.hpp)."""
+
+    _lib = None
+
+    @classmethod
+    def available(cls) -> bool:
+        return os.path.exists(REF_LOWACC_SO)
+
+    @classmethod
+    def lib(cls):
+        if cls._lib is None:
+            if not os.path.exists(REF_LOWACC_SO):
+                raise FileNotFoundError(f"{REF_LOWACC_SO} is not built (make -C oracle ref)")
+            lib = C.CDLL(REF_LOWACC_SO)
+            lib.lref_build.argtypes = [_f32p, C.c_uint64, C.c_uint64, _f32p, C.c_uint64, _u32p,
+                                       C.c_uint64, C.c_char_p]
+            lib.lref_build.restype = C.c_int
+            lib.lref_load.argtypes = [C.c_char_p]
+            lib.lref_load.restype = C.c_void_p
+            lib.lref_free.argtypes = [C.c_void_p]
+            lib.lref_info.argtypes = [C.c_void_p, _u64p]
+            lib.lref_rotate.argtypes = [C.c_void_p, _f32p, C.c_uint64, _f32p]
+            lib.lref_search_dists.argtypes = [C.c_void_p, _f32p, C.c_uint64, C.c_uint64,
+                                              C.c_uint64, _u32p, _f32p]
+            cls._lib = lib
+        return cls._lib
+
+    @classmethod
+    def build(cls, data, centroids, cluster_ids, bits: int, path: str) -> None:
+        """IVF(n, dim, K, bits).construct(data, centroids, cluster_ids).save(path)."""
+        x = _f32(data)
+        c = _f32(centroids)
+        ids = np.ascontiguousarray(cluster_ids, dtype=np.uint32)
+        rc = cls.lib().lref_build(x, x.shape[0], x.shape[1], c, c.shape[0], ids, bits,
+                                  os.fsencode(path))
+        if rc != 0:
+            raise RuntimeError("lref_build failed")
+
+    def __init__(self, path: str):
+        h = self.lib().lref_load(os.fsencode(path))
+        if not h:
+            raise OSError(f"reference IVF::load({path}) failed")
+        self.h = h
+        info = np.zeros(5, np.uint64)
+        self.lib().lref_info(self.h, info)
+        self.N, self.DIM, self.D, self.K, self.EX = (int(x) for x in info)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib().lref_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def rotate(self, q):
+        q = _f32(q).reshape(-1, self.DIM)
+        out = np.zeros((q.shape[0], self.D), np.float32)
+        self.lib().lref_rotate(self.h, q, q.shape[0], out)
+        return out
+
+    def search_dists(self, q, k, nprobe):
+        q = _f32(q).reshape(-1, self.D)
+        ids = np.zeros((q.shape[0], k), np.uint32)
+        d = np.zeros((q.shape[0], k), np.float32)
+        self.lib().lref_search_dists(self.h, q, q.shape[0], k, nprobe, ids, d)
+        return ids, d
