@@ -30,6 +30,7 @@
 #include "../../include/erq_debug.h"
 #include "coarse.cuh"
 #include "gemm.cuh"
+#include "build.cuh"
 #include "gemm_tc.cuh"
 #include "kmeans.cuh"
 #include "mlp.cuh"
@@ -357,6 +358,11 @@ erq_status load_impl(const char* path, erq_index* idx) {
         };
         if (rest == need(1)) idx->factors = 1;
         else if (rest == need(4)) idx->factors = 4;
+        else if (K >= 20000 && (rest == need(1) - K * D * 4 || rest == need(4) - K * D * 4))
+            return fail(ERQ_ERR_UNSUPPORTED,
+                        "index file '%s' (K=%llu) keeps its centroids only in the reference's "
+                        "hnswlib side file, which this library does not read; indexes written by "
+                        "erq_build_index carry them in the main file", path, (unsigned long long)K);
         else
             return fail(ERQ_ERR_FORMAT, "index file '%s' holds %llu bytes after its cluster table; "
                         "%llu (one block factor) or %llu (four) expected", path,
@@ -1474,6 +1480,54 @@ double splitmix64_uniform(uint64_t& s) {  // in [0, 1), 53 random bits
     return (double)(splitmix64_next(s) >> 11) * (1.0 / 9007199254740992.0);
 }
 
+// A D x D orthogonal matrix for erq_build_index when the caller gives none:
+// Householder QR (double) of a matrix of standard normal samples (Box-Muller
+// on the splitmix64 stream), P = Q^T with the signs that make R's diagonal
+// positive.  Any orthogonal rotation serves the quantiser (the reference
+// draws its own, inc/index/Rotator.hpp:14-19).
+void random_rotation(uint64_t D, uint64_t seed, std::vector<float>& P) {
+    uint64_t s = seed;
+    std::vector<double> a(D * D);
+    for (uint64_t i = 0; i < D * D; i += 2) {
+        const double u1 = 1.0 - splitmix64_uniform(s), u2 = splitmix64_uniform(s);
+        const double r = std::sqrt(-2.0 * std::log(u1));
+        a[i] = r * std::cos(6.283185307179586 * u2);
+        if (i + 1 < D * D) a[i + 1] = r * std::sin(6.283185307179586 * u2);
+    }
+    // reflector k: v = column k of a from row k down (after the update), tau
+    std::vector<double> tau(D, 0.0), rdiag(D, 0.0), dot(D);
+    auto reflect = [&](std::vector<double>& m, uint64_t kk, uint64_t j0) {
+        std::fill(dot.begin() + j0, dot.end(), 0.0);
+        for (uint64_t i = kk; i < D; ++i) {
+            const double vi = a[i * D + kk];
+            for (uint64_t j = j0; j < D; ++j) dot[j] += vi * m[i * D + j];
+        }
+        for (uint64_t i = kk; i < D; ++i) {
+            const double vi = a[i * D + kk] * tau[kk];
+            for (uint64_t j = j0; j < D; ++j) m[i * D + j] -= dot[j] * vi;
+        }
+    };
+    for (uint64_t kk = 0; kk < D; ++kk) {
+        double norm = 0;
+        for (uint64_t i = kk; i < D; ++i) norm += a[i * D + kk] * a[i * D + kk];
+        norm = std::sqrt(norm);
+        const double alpha = a[kk * D + kk] > 0 ? -norm : norm;
+        rdiag[kk] = alpha;
+        a[kk * D + kk] -= alpha;
+        double v2 = 0;
+        for (uint64_t i = kk; i < D; ++i) v2 += a[i * D + kk] * a[i * D + kk];
+        tau[kk] = v2 > 0 ? 2.0 / v2 : 0.0;
+        if (kk + 1 < D) reflect(a, kk, kk + 1);
+    }
+    std::vector<double> q(D * D, 0.0);  // Q = H_0 H_1 ... H_{D-1}
+    for (uint64_t i = 0; i < D; ++i) q[i * D + i] = 1.0;
+    for (uint64_t kk = D; kk-- > 0;) reflect(q, kk, 0);
+    // P = Q^T with column signs making R's diagonal positive
+    P.resize(D * D);
+    for (uint64_t i = 0; i < D; ++i)
+        for (uint64_t j = 0; j < D; ++j) P[j * D + i] = (float)(rdiag[j] < 0 ? -q[i * D + j] : q[i * D + j]);
+}
+
 // Device buffers of one clustering run, freed on scope exit.
 struct KmBuffers {
     std::vector<void*> owned;
@@ -2378,6 +2432,153 @@ erq_status erq_debug_gemm_bf16(const uint16_t* A, const uint16_t* B, uint64_t M,
     ERQ_CUDA(cudaMemcpy(&st, status, 4, cudaMemcpyDeviceToHost));
     if (st) return fail(ERQ_ERR_TIMEOUT, "a wait in the tcgen05 GEMM reached its limit");
     ERQ_CUDA(cudaMemcpy(C, c, M * N * 4, cudaMemcpyDeviceToHost));
+    return ERQ_OK;
+}
+
+erq_status erq_build_index(const float* data, uint64_t n, uint64_t dim, const float* centroids,
+                           uint64_t k, const uint32_t* cluster_ids, uint64_t total_bits,
+                           const float* rotation, uint64_t seed, const char* path, int device) {
+    if (!data || !centroids || !cluster_ids || !path)
+        return fail(ERQ_ERR_INVALID_ARGUMENT, "NULL argument");
+    const uint64_t EX = total_bits - 1;
+    if (total_bits < 3 || !(EX == 2 || EX == 3 || EX == 4 || EX == 6 || EX == 7 || EX == 8))
+        return fail(ERQ_ERR_INVALID_ARGUMENT, "total_bits=%llu: 3, 4, 5, 7, 8 or 9 expected",
+                    (unsigned long long)total_bits);
+    const uint64_t D = (dim + 63) / 64 * 64;
+    if (n == 0 || dim == 0 || k == 0 || D > (uint64_t)kMaxD || n >= (1ull << 31) || k > kMaxClusters)
+        return fail(ERQ_ERR_INVALID_ARGUMENT, "bad shape (n=%llu dim=%llu k=%llu)",
+                    (unsigned long long)n, (unsigned long long)dim, (unsigned long long)k);
+    DeviceGuard guard;
+    ERQ_TRY(guard.set(device));
+    // file order: clusters in order, members by ascending data index
+    std::vector<uint32_t> cid_h(n);
+    ERQ_CUDA(cudaMemcpy(cid_h.data(), cluster_ids, n * sizeof(uint32_t), cudaMemcpyDefault));
+    std::vector<uint64_t> sizes(k, 0);
+    for (uint64_t i = 0; i < n; ++i) {
+        if (cid_h[i] >= k) return fail(ERQ_ERR_INVALID_ARGUMENT, "cluster id %u >= k", cid_h[i]);
+        ++sizes[cid_h[i]];
+    }
+    std::vector<uint64_t> first(k + 1, 0);
+    for (uint64_t c = 0; c < k; ++c) first[c + 1] = first[c] + sizes[c];
+    std::vector<uint32_t> order(n), cid_row(n);
+    {
+        std::vector<uint64_t> pos(first.begin(), first.end() - 1);
+        for (uint64_t i = 0; i < n; ++i) {
+            const uint64_t p = pos[cid_h[i]]++;
+            order[p] = (uint32_t)i;
+            cid_row[p] = cid_h[i];
+        }
+    }
+    std::vector<uint32_t> vfirst, vnum;
+    for (uint64_t c = 0; c < k; ++c)
+        for (uint64_t b = 0; b < sizes[c]; b += 32) {
+            vfirst.push_back((uint32_t)(first[c] + b));
+            vnum.push_back((uint32_t)std::min<uint64_t>(32, sizes[c] - b));
+        }
+    const uint64_t nblocks = vfirst.size();
+    // rotation: the caller's D x D matrix, else a seeded random orthogonal one
+    std::vector<float> P(D * D);
+    if (rotation) {
+        ERQ_CUDA(cudaMemcpy(P.data(), rotation, D * D * sizeof(float), cudaMemcpyDefault));
+    } else {
+        random_rotation(D, seed, P);
+    }
+    KmBuffers b;
+    float *x = nullptr, *cent = nullptr, *Pd = nullptr, *cp = nullptr, *xp = nullptr, *onorm = nullptr,
+          *ipn = nullptr, *xip = nullptr;
+    uint32_t *ord = nullptr, *cidr = nullptr, *vf = nullptr, *vn = nullptr;
+    uint64_t* bits = nullptr;
+    uint8_t *code = nullptr, *lng = nullptr, *shrt = nullptr;
+    const uint64_t lrow = D * EX / 8, bb = 4 * D + 128;
+    ERQ_TRY(b.alloc(&x, n * dim));
+    ERQ_TRY(b.alloc(&cent, k * dim));
+    ERQ_TRY(b.alloc(&Pd, D * D));
+    ERQ_TRY(b.alloc(&cp, k * D));
+    ERQ_TRY(b.alloc(&xp, n * D));
+    ERQ_TRY(b.alloc(&onorm, n));
+    ERQ_TRY(b.alloc(&ipn, n));
+    ERQ_TRY(b.alloc(&xip, n));
+    ERQ_TRY(b.alloc(&ord, n));
+    ERQ_TRY(b.alloc(&cidr, n));
+    ERQ_TRY(b.alloc(&vf, std::max<uint64_t>(nblocks, 1)));
+    ERQ_TRY(b.alloc(&vn, std::max<uint64_t>(nblocks, 1)));
+    ERQ_TRY(b.alloc(&bits, n * (D / 64)));
+    ERQ_TRY(b.alloc(&code, n * D));
+    ERQ_TRY(b.alloc(&lng, n * lrow));
+    ERQ_TRY(b.alloc(&shrt, std::max<uint64_t>(nblocks, 1) * bb));
+    ERQ_CUDA(cudaMemcpy(x, data, n * dim * sizeof(float), cudaMemcpyDefault));
+    ERQ_CUDA(cudaMemcpy(cent, centroids, k * dim * sizeof(float), cudaMemcpyDefault));
+    ERQ_CUDA(cudaMemcpy(Pd, P.data(), D * D * sizeof(float), cudaMemcpyHostToDevice));
+    ERQ_CUDA(cudaMemcpy(ord, order.data(), n * 4, cudaMemcpyHostToDevice));
+    ERQ_CUDA(cudaMemcpy(cidr, cid_row.data(), n * 4, cudaMemcpyHostToDevice));
+    if (nblocks) {
+        ERQ_CUDA(cudaMemcpy(vf, vfirst.data(), nblocks * 4, cudaMemcpyHostToDevice));
+        ERQ_CUDA(cudaMemcpy(vn, vnum.data(), nblocks * 4, cudaMemcpyHostToDevice));
+    }
+    {
+        dim3 gc((unsigned)div_up(D, kBuildBN), (unsigned)div_up(k, kBuildBM));
+        build_rotate_kernel<<<gc, 256>>>(cent, (int)dim, nullptr, (int)k, Pd, (int)D, nullptr, nullptr, cp);
+        ERQ_CUDA(cudaGetLastError());
+        for (uint64_t r0 = 0; r0 < n; r0 += 65535ull * kBuildBM) {
+            const uint64_t rows = std::min<uint64_t>(n - r0, 65535ull * kBuildBM);
+            dim3 gx((unsigned)div_up(D, kBuildBN), (unsigned)div_up(rows, kBuildBM));
+            build_rotate_kernel<<<gx, 256>>>(x, (int)dim, ord + r0, (int)rows, Pd, (int)D, cp, cidr + r0,
+                                             xp + r0 * D);
+            ERQ_CUDA(cudaGetLastError());
+        }
+    }
+    build_x2_kernel<<<(unsigned)div_up(n * 16, 256), 256>>>(x, ord, cent, cidr, (int)n, (int)dim, onorm);
+    ERQ_CUDA(cudaGetLastError());
+    build_rows_kernel<<<(unsigned)div_up(n, 128), 128>>>(xp, (int)n, (int)D, bits);
+    ERQ_CUDA(cudaGetLastError());
+    {
+        const uint64_t T = std::min<uint64_t>(n, 65536);
+        double* ht = nullptr;
+        uint16_t* hi = nullptr;
+        uint8_t* cur = nullptr;
+        ERQ_TRY(b.alloc(&ht, T * D));
+        ERQ_TRY(b.alloc(&hi, T * D));
+        ERQ_TRY(b.alloc(&cur, T * D));
+        for (uint64_t r0 = 0; r0 < n; r0 += T) {
+            fast_quantize_kernel<<<(unsigned)div_up(T, 128), 128>>>(xp, (int)n, (int)r0, (int)T, (int)D,
+                                                                    (int)EX, ht, hi, cur, code, ipn);
+            ERQ_CUDA(cudaGetLastError());
+        }
+    }
+    build_long_kernel<<<(unsigned)div_up(n * (D / 64), 128), 128>>>(code, bits, ipn, onorm, (int)n, (int)D,
+                                                                    (int)EX, lng, xip);
+    ERQ_CUDA(cudaGetLastError());
+    if (nblocks) {
+        build_short_kernel<<<2368, 256>>>(bits, onorm, vf, vn, nblocks, (int)D, shrt);
+        ERQ_CUDA(cudaGetLastError());
+    }
+    ERQ_CUDA(cudaDeviceSynchronize());
+    // IVF::save (inc/index/IVF.hpp:219-252)
+    std::unique_ptr<FILE, FileCloser> f(fopen(path, "wb"));
+    if (!f) return fail(ERQ_ERR_IO, "cannot create '%s'", path);
+    auto put = [&](const void* p, size_t bytes) -> erq_status {
+        if (bytes && fwrite(p, 1, bytes, f.get()) != bytes) return fail(ERQ_ERR_IO, "write to '%s' failed", path);
+        return ERQ_OK;
+    };
+    auto put_dev = [&](const void* dptr, size_t bytes) -> erq_status {
+        std::vector<uint8_t> h(std::min<size_t>(bytes, 256ull << 20));
+        for (size_t off = 0; off < bytes; off += h.size()) {
+            const size_t m = std::min(h.size(), bytes - off);
+            ERQ_CUDA(cudaMemcpy(h.data(), static_cast<const uint8_t*>(dptr) + off, m, cudaMemcpyDeviceToHost));
+            ERQ_TRY(put(h.data(), m));
+        }
+        return ERQ_OK;
+    };
+    const uint64_t hdr[4] = {n, dim, k, EX};
+    ERQ_TRY(put(hdr, sizeof(hdr)));
+    ERQ_TRY(put(sizes.data(), k * sizeof(uint64_t)));
+    ERQ_TRY(put(P.data(), D * D * sizeof(float)));
+    ERQ_TRY(put_dev(cp, k * D * sizeof(float)));
+    ERQ_TRY(put_dev(shrt, nblocks * bb));
+    ERQ_TRY(put_dev(lng, n * lrow));
+    ERQ_TRY(put_dev(xip, n * sizeof(float)));
+    ERQ_TRY(put(order.data(), n * sizeof(uint32_t)));
+    if (fflush(f.get()) != 0) return fail(ERQ_ERR_IO, "write to '%s' failed", path);
     return ERQ_OK;
 }
 

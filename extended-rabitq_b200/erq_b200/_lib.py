@@ -29,7 +29,7 @@ STATUS_NAMES = {
 EXPORTED_SYMBOLS = (
     "erq_version", "erq_status_string", "erq_last_error", "erq_index_load",
     "erq_index_get_info", "erq_index_free", "erq_rotate", "erq_search", "erq_search_raw",
-    "erq_search_noalloc", "erq_kmeans", "erq_kmeans_step",
+    "erq_search_noalloc", "erq_kmeans", "erq_kmeans_step", "erq_build_index",
     "erq_debug_scan_capacity", "erq_debug_centroid_dists", "erq_debug_probe", "erq_debug_scan",
     "erq_profile_enable", "erq_profile_reset", "erq_profile_read",
     "erq_probe_features", "erq_probe_model_train", "erq_probe_model_save", "erq_probe_model_load",
@@ -106,6 +106,8 @@ def load_library(path: str | None = None) -> C.CDLL:
     lib.erq_search_raw.restype = C.c_int
     lib.erq_search_noalloc.argtypes = [vp, f32p, u64, u64, u64, u32p, f32p, vp]
     lib.erq_search_noalloc.restype = C.c_int
+    lib.erq_build_index.argtypes = [vp, u64, u64, vp, u64, vp, u64, vp, u64, C.c_char_p, C.c_int]
+    lib.erq_build_index.restype = C.c_int
     lib.erq_kmeans.argtypes = [vp, u64, u64, u64, C.c_int, u64, vp, vp, C.c_int]
     lib.erq_kmeans.restype = C.c_int
     lib.erq_kmeans_step.argtypes = [vp, u64, u64, u64, vp, u64, vp, vp, vp, C.c_int]

@@ -192,3 +192,31 @@ def build_index_torch(base, centroids, cluster_ids, bits: int, P=None, seed: int
         xipnorm=xip.cpu().numpy(),
         ids=order.cpu().numpy().astype(np.uint32),
     )
+
+
+def build_index_gpu(base, centroids, cluster_ids, bits: int, path, P=None, seed: int = 0,
+                    device: int = 0) -> None:
+    """IVF(n, dim, k, bits) + construct + save on the GPU (erq_build_index):
+    the reference's index bytes for the same data, centroids, cluster ids and
+    rotation P (drawn from ``seed`` when None).  Arrays: numpy or torch."""
+    import ctypes as C
+    import os
+
+    from ._lib import check, load_library
+
+    def ptr(a):
+        return None if a is None else C.c_void_p(
+            a.data_ptr() if hasattr(a, "data_ptr") else a.ctypes.data)
+
+    if not hasattr(base, "data_ptr"):
+        base = np.ascontiguousarray(base, np.float32)
+    if not hasattr(centroids, "data_ptr"):
+        centroids = np.ascontiguousarray(centroids, np.float32)
+    if not hasattr(cluster_ids, "data_ptr"):
+        cluster_ids = np.ascontiguousarray(cluster_ids, np.uint32)
+    if P is not None and not hasattr(P, "data_ptr"):
+        P = np.ascontiguousarray(P, np.float32)
+    n, dim = base.shape
+    check(load_library().erq_build_index(ptr(base), n, dim, ptr(centroids), centroids.shape[0],
+                                         ptr(cluster_ids), bits, ptr(P), seed,
+                                         os.fsencode(os.fspath(path)), device))

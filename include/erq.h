@@ -231,6 +231,22 @@ ERQ_API erq_status erq_kmeans_step(const float* data, uint64_t n, uint64_t dim, 
                                    float* centroids_out, uint32_t* assign, uint32_t* counts,
                                    int device);
 
+/* ---------------------------------------------------------------------------
+ * Index construction on the GPU: IVF(n, dim, k, total_bits) + construct +
+ * save (inc/index/IVF.hpp:116-153, 219-252; src/create_index.cpp:45-49),
+ * HIGH_ACC_FAST_SCAN format.  data[n][dim], centroids[k][dim] (raw, as
+ * create_index reads them), cluster_ids[n] < k; buffers host or device.
+ * `rotation` (D x D row-major, D = dim rounded up to 64; queries are rotated
+ * as q * rotation) may be NULL, in which case a random orthogonal matrix is
+ * drawn from `seed`.  Given the same rotation, the file equals the
+ * reference's byte for byte, except the block factors of the lanes past a
+ * cluster's end, which the reference leaves unset and this writes as 0.
+ * Every step follows the reference's arithmetic (see build.cuh).  Synchronous. */
+ERQ_API erq_status erq_build_index(const float* data, uint64_t n, uint64_t dim,
+                                   const float* centroids, uint64_t k, const uint32_t* cluster_ids,
+                                   uint64_t total_bits, const float* rotation, uint64_t seed,
+                                   const char* path, int device);
+
 /* erq_search without any memory allocation.  Has no counterpart in the
  * reference: it is for callers that cannot allocate device memory while a
  * query runs - engines that hand all GPU memory to their own allocator up
