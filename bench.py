@@ -56,9 +56,16 @@ CONFIGS = {
     "zipf1536-2M-7bit": dict(
         gen="sphere", n=2_000_000, dim=1536, comps=4096, sigma=0.05, zipf=1.1, K=4096,
         bits=7, nq=8192, k=100, seed=20242, nprobe=None, recall_target=0.95,
-        train_queries=0, save_base=False, latency_batches=(1, 64, 1024, 8192),
+        train_queries=40_000, save_base=False, latency_batches=(1, 64, 1024, 8192),
         data="synthetic: seeded 4096-component unit-sphere mixture with Zipf(1.1) component "
-             "weights, tangent sigma 0.05, 2M base + 8192 queries, d=1536"),
+             "weights, tangent sigma 0.05, 2M base + 8192 queries (+40k training queries for "
+             "the probe model), d=1536"),
+    # the headline data at 4 bits (EX = 3)
+    "sphere1536-1M-4bit": dict(
+        gen="sphere", n=1_000_000, dim=1536, comps=4096, sigma=0.05, zipf=None, K=4096,
+        bits=4, nq=10_000, k=100, seed=20241, nprobe=None, recall_target=0.95,
+        train_queries=0, save_base=False,
+        data="synthetic: the 1M x 1536 unit-sphere mixture of the headline workload, 4-bit"),
     # the small CPU-runnable case
     "gauss128-100k-4bit": dict(
         gen="gauss", n=100_000, dim=128, comps=256, sigma=0.3, zipf=None, K=1024,
@@ -457,7 +464,9 @@ def run_ours(args, cfg, name):
     assert (ids_d.cpu().numpy().view(np.uint32) == ids0).all()
     plain = {"value": round(world * nq * args.steps / (ms_p / 1e3), 1), "nprobe": nprobe,
              "recall@100": round(recall, 5), "ms_per_step": round(ms_p / args.steps, 4),
-             "refine_per_query": {kk: round(v / nq, 2) for kk, v in rst_plain.items()}}
+             "refine_per_query": {kk: round(v / nq, 2) for kk, v in rst_plain.items()},
+             "kernels_ms_per_step": {kk: round(v[1] / args.steps, 4) for kk, v in prof_p.items()
+                                     if v[0]}}
     ms_pe = None
     if not args.no_e2e:
         ms_pe, _, _ = timed(plain_host, args.steps, args.warmup, world, stream)
@@ -472,7 +481,10 @@ def run_ours(args, cfg, name):
         def dev():
             plan.search_buffers(qd, ids_d, dist_d, stream=stream)
 
-        def host():
+        def host():  # pinned host buffers, each call's copy-in under the search before
+            plan.search_buffers_async(qh, ids_h, dist_h, stream=stream)
+
+        def host_sync():  # each call returns with its results in host memory
             plan.search_buffers(qh, ids_h, dist_h, stream=stream)
 
         ms, _, clocks = timed(dev, args.steps, args.warmup, world, stream, local)
@@ -481,6 +493,9 @@ def run_ours(args, cfg, name):
         if not args.no_e2e:
             e2e, _, _ = timed(host, args.steps, args.warmup, world, stream)
             assert (ids_h.numpy().view(np.uint32) == expect).all()
+            e2e_sync, _, _ = timed(host_sync, args.steps, args.warmup, world, stream)
+            assert (ids_h.numpy().view(np.uint32) == expect).all()
+            plan.e2e_sync_ms = e2e_sync
         # per-kernel times: the same steps with the kernels launched one by one
         plan.set_graphs(False)
         _, prof, _ = timed(dev, args.steps, 1, world, stream)
@@ -497,9 +512,12 @@ def run_ours(args, cfg, name):
         ms_b, e2e_b, clocks_b, prof_b = plan_mode(plan_b, ids0)
         batched = {"value": round(world * nq * args.steps / (ms_b / 1e3), 1), "nprobe": nprobe,
                    "recall@100": round(recall, 5), "ms_per_step": round(ms_b / args.steps, 4),
-                   "tuning": tune_b}
+                   "tuning": tune_b,
+                   "kernels_ms_per_step": {kk: round(v[1] / args.steps, 4) for kk, v in prof_b.items()
+                                           if v[0]}}
         if e2e_b is not None:
             batched["e2e"] = round(world * nq * args.steps / (e2e_b / 1e3), 1)
+            batched["e2e_sync"] = round(world * nq * args.steps / (plan_b.e2e_sync_ms / 1e3), 1)
         modes["batched"] = {"ms": ms_b, "prof": prof_b, "clocks": clocks_b, "recall": recall,
                             "ids": ids0, "scan_bytes": scan_bytes_plain, "e2e_ms": e2e_b,
                             "refine_bytes": cand_plain * cand_bytes}
@@ -557,6 +575,7 @@ def run_ours(args, cfg, name):
                             "model": meta}
             if e2e_l is not None:
                 learned_info["e2e"] = round(world * nq * args.steps / (e2e_l / 1e3), 1)
+                learned_info["e2e_sync"] = round(world * nq * args.steps / (plan_l.e2e_sync_ms / 1e3), 1)
             modes["learned"] = {"ms": ms_l, "prof": prof_l, "clocks": clocks_l, "recall": r_l,
                                 "ids": ids_l, "scan_bytes": scan_bytes_l, "e2e_ms": e2e_l,
                                 "refine_bytes": cand_l * cand_bytes}
@@ -637,7 +656,11 @@ def run_ours(args, cfg, name):
             "e2e": None if e2e_ms is None else {
                 "value": round(world * nq * args.steps / (e2e_ms / 1e3), 1), "unit": "queries/s",
                 "h2d_bytes_per_step": int(nq * query.shape[1] * 4),
-                "d2h_bytes_per_step": int(nq * k * 8)},
+                "d2h_bytes_per_step": int(nq * k * 8),
+                "api": ("erq_search_raw, pinned host buffers, one synchronous call per step"
+                        if mode == "plain" else
+                        "erq_plan_search_async, pinned host buffers: a step's query copy-in "
+                        "overlaps the previous step's search; results copied out every step")},
             "gpu_launches": int(launches),
             "roofline": rooflines.get(dominant),
             "roofline_other": {kn: r for kn, r in rooflines.items() if kn != dominant},
@@ -647,9 +670,179 @@ def run_ours(args, cfg, name):
             "parity": parity,
             "clocks": chosen["clocks"],
         }
-        print(json.dumps(out), flush=True)
     idx.free()
     dist_finish(world)
+    return out if rank == 0 else None
+
+
+# ------------------------------------------------- secondary workloads
+def _timed_calls(fn, calls, warmup):
+    """Per-call device times (ms) of fn() on the current stream."""
+    import torch
+
+    for _ in range(warmup):
+        fn()
+    st = torch.cuda.current_stream()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(calls)]
+    torch.cuda.synchronize()
+    for c in range(calls):
+        ev[c][0].record(st)
+        fn()
+        ev[c][1].record(st)
+    torch.cuda.synchronize()
+    return np.array([a.elapsed_time(b) for a, b in ev])
+
+
+def secondary_small(args):
+    """100k x 128, 4-bit, nprobe 16/32/64: one query per call (p50/p99 and
+    QPS) and the whole 1,000-query batch per call, with recall@100."""
+    import torch
+
+    from erq_b200 import IVF, metrics
+
+    name = "gauss128-100k-4bit"
+    cfg = CONFIGS[name]
+    d = prepare(name, cfg)
+    idx = IVF(os.path.join(d, "ivf.index"))
+    query = np.load(os.path.join(d, "query.npy"))
+    gt = np.load(os.path.join(d, "gt.npy"))
+    qd = torch.from_numpy(query).cuda()
+    k = cfg["k"]
+    ids = torch.empty((query.shape[0], k), dtype=torch.int32, device="cuda")
+    dist = torch.empty((query.shape[0], k), dtype=torch.float32, device="cuda")
+    st = torch.cuda.current_stream()
+    out = {}
+    for nprobe in (16, 32, 64):
+        r_ids, _ = idx.search_raw(query, k, nprobe, with_dists=False)
+        rec = metrics.recall_at_k(r_ids, gt, k)
+        calls = iter(range(1 << 30))
+
+        def one_query():
+            i = next(calls) % query.shape[0]
+            idx.search_raw(qd[i:i + 1], k, nprobe, ids=ids[:1], dists=dist[:1], stream=st)
+
+        one = _timed_calls(one_query, 300, 10)
+        batch = _timed_calls(lambda: idx.search_raw(qd, k, nprobe, ids=ids, dists=dist, stream=st),
+                             20, 3)
+        out[str(nprobe)] = {"recall@100": round(rec, 5),
+                            "one_query_per_call": {"qps": round(1e3 / one.mean(), 1),
+                                                   "p50_ms": round(float(np.percentile(one, 50)), 4),
+                                                   "p99_ms": round(float(np.percentile(one, 99)), 4)},
+                            "batch_1000_qps": round(1e3 * query.shape[0] / batch.mean(), 1)}
+    idx.free()
+    return {"workload": f"{name}: 100000x128, K=1024, 4-bit, top-100, one query per call and "
+                        "1000-query batches", "nprobe": out}
+
+
+def secondary_4bit(args):
+    """The headline data at 4 bits: plain per-query and batched plan QPS at
+    the smallest nprobe reaching recall@100 >= 0.95 (10k queries per call)."""
+    import torch
+
+    from erq_b200 import IVF, Plan
+
+    name = "sphere1536-1M-4bit"
+    cfg = CONFIGS[name]
+    d = prepare(name, cfg)
+    idx = IVF(os.path.join(d, "ivf.index"))
+    query = np.load(os.path.join(d, "query.npy"))
+    gt = np.load(os.path.join(d, "gt.npy"))
+    nprobe, rec, ids0 = choose_nprobe(idx, query, gt, cfg)
+    qd = torch.from_numpy(query).cuda()
+    k, nq = cfg["k"], query.shape[0]
+    ids = torch.empty((nq, k), dtype=torch.int32, device="cuda")
+    dist = torch.empty((nq, k), dtype=torch.float32, device="cuda")
+    st = torch.cuda.current_stream()
+    plain = _timed_calls(lambda: idx.search_raw(qd, k, nprobe, ids=ids, dists=dist, stream=st), 10, 3)
+    plan = Plan(idx, max_batch=nq, k=k, nprobe=nprobe, raw=True)
+    plan.autotune(query, reps=2)
+    batched = _timed_calls(lambda: plan.search_buffers(qd, ids, dist, stream=st), 10, 3)
+    assert (ids.cpu().numpy().view(np.uint32) == ids0).all()
+    plan.free()
+    idx.free()
+    return {"workload": f"{name}: 1000000x1536, K=4096, 4-bit, 10000 queries per call, top-100",
+            "nprobe": nprobe, "recall@100": round(rec, 5),
+            "plain_qps": round(1e3 * nq / plain.mean(), 1),
+            "batched_qps": round(1e3 * nq / batched.mean(), 1)}
+
+
+def secondary_zipf_learned(args):
+    """Zipf 2M x 1536, 7-bit, batches of 8192: the batched plain plan at the
+    smallest nprobe reaching recall@100 >= 0.95 against the batched learned
+    plan at the lowest confidence reaching it (probe depths scaled to the
+    workload, fallback below LEARNED_MIN_PROB)."""
+    import torch
+
+    from erq_b200 import IVF, Plan, learned, metrics
+
+    name = "zipf1536-2M-7bit"
+    cfg = CONFIGS[name]
+    d = prepare(name, cfg)
+    idx = IVF(os.path.join(d, "ivf.index"))
+    query = np.load(os.path.join(d, "query.npy"))
+    gt = np.load(os.path.join(d, "gt.npy"))
+    nprobe, rec, ids0 = choose_nprobe(idx, query, gt, cfg)
+    k, nq = cfg["k"], query.shape[0]
+    qd = torch.from_numpy(query).cuda()
+    ids = torch.empty((nq, k), dtype=torch.int32, device="cuda")
+    st = torch.cuda.current_stream()
+    plan = Plan(idx, max_batch=nq, k=k, nprobe=nprobe, raw=True)
+    plan.autotune(query, reps=1)
+    plain = _timed_calls(lambda: plan.search_buffers(qd, ids, stream=st), 5, 3)
+    plan.free()
+    model, meta = learned_model(idx, d, cfg, nprobe)
+    plan_l = Plan(idx, max_batch=nq, k=k, nprobe=nprobe, model=model, raw=True)
+    best = None
+    for conf in (0.005, 0.01, 0.02, 0.05, 0.1, 0.2, 0.3, 0.4, 0.5, 0.6, 0.7, 0.8, 0.9, 0.95, 0.99):
+        plan_l.set_learned(conf, LEARNED_MIN_PROB)
+        ids_l, _, used = plan_l.search(query, with_dists=False, with_nprobe=True)
+        r = metrics.recall_at_k(ids_l, gt, k)
+        log(f"zipf learned confidence={conf}: recall@{k}={r:.4f}, mean nprobe {used.mean():.1f}")
+        if r >= cfg["recall_target"]:
+            best = (conf, r, used)
+            break
+    res = {"workload": f"{name}: 2000000x1536, K=4096 Zipf(1.1) clusters, 7-bit, batches of "
+                       f"{nq}, top-100",
+           "plain": {"nprobe": nprobe, "recall@100": round(rec, 5),
+                     "qps": round(1e3 * nq / plain.mean(), 1)},
+           "model": meta}
+    if best is not None:
+        conf, r_l, used = best
+        plan_l.set_learned(conf, LEARNED_MIN_PROB)
+        plan_l.autotune(query, reps=1)
+        lt = _timed_calls(lambda: plan_l.search_buffers(qd, ids, stream=st), 5, 3)
+        feats = learned.probe_features(idx, idx.rotate(query))
+        res["learned"] = {"confidence": conf, "recall@100": round(r_l, 5),
+                          "mean_nprobe": round(float(used.mean()), 2),
+                          "min_prob": LEARNED_MIN_PROB,
+                          "model_fallback_rate": round(learned.fallback_rate(model, feats,
+                                                                             LEARNED_MIN_PROB), 5),
+                          "qps": round(1e3 * nq / lt.mean(), 1)}
+        res["learned_over_plain"] = round(res["learned"]["qps"] / res["plain"]["qps"], 3)
+    plan_l.free()
+    model.free()
+    idx.free()
+    return res
+
+
+def run_secondary(args):
+    """The other workloads of the benchmark suite, each guarded: a failure is
+    reported in its entry and does not touch the headline line."""
+    import torch
+
+    out = {}
+    for key, fn in (("gauss128-100k-4bit", secondary_small), ("sphere1536-1M-4bit", secondary_4bit),
+                    ("zipf1536-2M-7bit-learned", secondary_zipf_learned)):
+        t0 = time.time()
+        try:
+            out[key] = fn(args)
+        except Exception as e:  # noqa: BLE001 - recorded, the headline stands
+            out[key] = {"error": f"{type(e).__name__}: {e}"}
+        out[key]["wall_s"] = round(time.time() - t0, 1)
+        log(f"secondary {key}: {out[key]}")
+        torch.cuda.empty_cache()
+    return out
 
 
 # ---------------------------------------------------- batched latency mode
@@ -826,6 +1019,9 @@ def main():
     ap.add_argument("--nprobe", type=int, default=0,
                     help="start the recall sweep at this nprobe")
     ap.add_argument("--prep-only", action="store_true")
+    ap.add_argument("--no-secondary", action="store_true",
+                    help="skip the other workloads (small 128-d, 4-bit, Zipf learned) reported "
+                         "under 'secondary' of the headline run")
     args = ap.parse_args()
     if args.warmup < 3 and not args.prep_only:
         log("warm-up raised to the minimum of 3 steps")
@@ -840,7 +1036,11 @@ def main():
         if cfg.get("latency_batches"):
             run_latency(args, cfg, args.config)
         else:
-            run_ours(args, cfg, args.config)
+            out = run_ours(args, cfg, args.config)
+            if out is not None:
+                if args.gpus == 1 and args.config == DEFAULT_CONFIG and not args.no_secondary:
+                    out["secondary"] = run_secondary(args)
+                print(json.dumps(out), flush=True)
 
 
 if __name__ == "__main__":

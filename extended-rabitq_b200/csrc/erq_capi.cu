@@ -2835,7 +2835,9 @@ struct erq_plan {
     uint32_t* ids1 = nullptr;
     float* dists1 = nullptr;
     int* used1 = nullptr;
-    int pipe_chunks = 0;     // erq_plan_set_pipeline: 0 = by batch size, 1 = off
+    int pipe_chunks = 1;     // erq_plan_set_pipeline: 1 = one piece (default), 0 = by size
+    int next_slot = 0;       // erq_plan_search_async: the slot of the next call
+    bool slot_used[2] = {false, false};
     cudaStream_t h2d = nullptr, d2h = nullptr;
     cudaEvent_t ev_start = nullptr, ev_end = nullptr;
     cudaEvent_t ev_in[2] = {}, ev_comp[2] = {}, ev_out[2] = {};
@@ -3162,8 +3164,8 @@ erq_status erq_plan_create(const erq_index* idx, const erq_probe_model* model, u
         ERQ_CUDA(cudaMemcpy(p->used, np.data(), max_batch * sizeof(int), cudaMemcpyHostToDevice));
     }
     ERQ_CUDA(cudaStreamCreateWithFlags(&p->cap, cudaStreamNonBlocking));
-    if (max_batch >= 4096) {  // a second buffer slot for pipelined host-buffer searches
-        p->slot_rows = div_up(max_batch, 2);
+    {  // a second buffer slot for pipelined and asynchronous host-buffer searches
+        p->slot_rows = max_batch;
         ERQ_TRY(p->arena.alloc(&p->qin1, p->slot_rows * (p->raw ? idx->DIM : idx->D)));
         ERQ_TRY(p->arena.alloc(&p->ids1, p->slot_rows * k));
         ERQ_TRY(p->arena.alloc(&p->dists1, p->slot_rows * k));
@@ -3308,6 +3310,8 @@ erq_status erq_plan_search(erq_plan* p, const float* queries, uint64_t nq, uint3
     const bool host = !is_device_ptr(ids) || (dists && !is_device_ptr(dists)) ||
                       (nprobe_used && !is_device_ptr(nprobe_used)) || !is_device_ptr(queries);
     const uint64_t chunks = host ? plan_chunks(p, nq) : 1;
+    for (int sl = 0; sl < 2; ++sl)  // a synchronous call orders after any earlier async one
+        if (p->slot_used[sl]) ERQ_CUDA(cudaStreamWaitEvent(st, p->ev_comp[sl], 0));
     if (chunks > 1) {
         ERQ_TRY(plan_search_pipelined(p, queries, nq, chunks, ids, dists, nprobe_used, st));
     } else {
@@ -3333,6 +3337,42 @@ erq_status erq_plan_search(erq_plan* p, const float* queries, uint64_t nq, uint3
 }
 
 uint64_t erq_plan_device_bytes(const erq_plan* p) { return p ? p->arena.bytes : 0; }
+
+erq_status erq_plan_search_async(erq_plan* p, const float* queries, uint64_t nq, uint32_t* ids,
+                                 float* dists, uint32_t* nprobe_used, void* stream) {
+    if (!p) return fail(ERQ_ERR_INVALID_ARGUMENT, "plan is NULL");
+    if (nq == 0) return ERQ_OK;
+    if (!queries || !ids) return fail(ERQ_ERR_INVALID_ARGUMENT, "queries and ids are required");
+    if (nq > p->max_batch)
+        return fail(ERQ_ERR_INVALID_ARGUMENT, "batch of %llu exceeds the plan's max_batch %llu",
+                    (unsigned long long)nq, (unsigned long long)p->max_batch);
+    std::lock_guard<std::mutex> g(p->mu);
+    DeviceGuard guard;
+    ERQ_TRY(guard.set(p->idx->device));
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int slot = p->next_slot;
+    p->next_slot ^= 1;
+    const uint64_t cols = p->raw ? p->idx->DIM : p->idx->D;
+    // queries in on the copy stream, once the slot's last search has read them
+    if (p->slot_used[slot]) ERQ_CUDA(cudaStreamWaitEvent(p->h2d, p->ev_comp[slot], 0));
+    ERQ_CUDA(cudaMemcpyAsync(slot ? p->qin1 : p->qin, queries, nq * cols * sizeof(float),
+                             cudaMemcpyDefault, p->h2d));
+    ERQ_CUDA(cudaEventRecord(p->ev_in[slot], p->h2d));
+    // the search and the results out on the caller's stream
+    ERQ_CUDA(cudaStreamWaitEvent(st, p->ev_in[slot], 0));
+    ERQ_TRY(plan_run(p, nq, slot, st));
+    ERQ_CUDA(cudaEventRecord(p->ev_comp[slot], st));
+    p->slot_used[slot] = true;
+    ERQ_CUDA(cudaMemcpyAsync(ids, slot ? p->ids1 : p->ids, nq * p->k * sizeof(uint32_t),
+                             cudaMemcpyDefault, st));
+    if (dists)
+        ERQ_CUDA(cudaMemcpyAsync(dists, slot ? p->dists1 : p->dists, nq * p->k * sizeof(float),
+                                 cudaMemcpyDefault, st));
+    if (nprobe_used)
+        ERQ_CUDA(cudaMemcpyAsync(nprobe_used, slot ? p->used1 : p->used, nq * sizeof(uint32_t),
+                                 cudaMemcpyDefault, st));
+    return ERQ_OK;
+}
 
 erq_status erq_plan_set_pipeline(erq_plan* p, int chunks) {
     if (!p) return fail(ERQ_ERR_INVALID_ARGUMENT, "plan is NULL");

@@ -54,7 +54,7 @@ __host__ __device__ constexpr uint32_t hex_table_bytes(int D) { return (uint32_t
 // qq entries (padded with zeros to whole chunks)
 __host__ __device__ constexpr int hex_qq_len(int D) { return hex_chunks(D) * 16 * kHexDims; }
 
-constexpr int kUnitChunks = 4;                   // chunks per staged copy
+constexpr int kUnitChunks = 2;                   // chunks per staged copy
 constexpr uint32_t kUnitBytes = kUnitChunks * 512;
 constexpr int kRing = 4;                         // staged copies per warp
 constexpr uint32_t kScanWaitLimit = 1u << 24;    // polls before a wait gives up
@@ -188,24 +188,33 @@ __device__ void hex_prepare(const float* __restrict__ q, const float* __restrict
     }
     __syncthreads();
 
-    // 3. tables: task (t, m) writes entries 8m .. 8m+7 of table t
+    // 3. tables, one thread per table: entry 8m + l = H[m] + L[l] with
+    //    L[l] = sum of q0..q2 over the bits of l minus their negative part and
+    //    H[m] the same of q3..q5; the eight 16-byte rows go out in an order
+    //    rotated by t, so the lanes of a warp store to distinct banks
     int vsum = 0;
-    const int ntask = hex_chunks(D) * 16 * 8;
-    for (int task = tid; task < ntask; task += NT) {
-        const int t = task >> 3, m = task & 7;
+    const int ntab = hex_chunks(D) * 16;
+    for (int t = tid; t < ntab; t += NT) {
         const int16_t* qt = qq + kHexDims * t;
         const int q0 = qt[0], q1 = qt[1], q2 = qt[2], q3 = qt[3], q4 = qt[4], q5 = qt[5];
-        const int vmin = min(q0, 0) + min(q1, 0) + min(q2, 0) + min(q3, 0) + min(q4, 0) + min(q5, 0);
-        const int hv = ((m & 1) ? q3 : 0) + ((m & 2) ? q4 : 0) + ((m & 4) ? q5 : 0) - vmin;
-        const int l1 = q0 + hv, l2 = q1 + hv, l3 = q0 + q1 + hv, l4 = q2 + hv;
-        const int l5 = q0 + q2 + hv, l6 = q1 + q2 + hv, l7 = q0 + q1 + q2 + hv;
-        uint4 e;
-        e.x = ((uint32_t)hv & 0xffffu) | ((uint32_t)l1 << 16);
-        e.y = ((uint32_t)l2 & 0xffffu) | ((uint32_t)l3 << 16);
-        e.z = ((uint32_t)l4 & 0xffffu) | ((uint32_t)l5 << 16);
-        e.w = ((uint32_t)l6 & 0xffffu) | ((uint32_t)l7 << 16);
-        reinterpret_cast<uint4*>(tab + 128 * t)[m] = e;
-        if (m == 0) vsum += vmin;
+        const int vlo = min(q0, 0) + min(q1, 0) + min(q2, 0);
+        const int vhi = min(q3, 0) + min(q4, 0) + min(q5, 0);
+        const uint32_t l0 = (uint32_t)(-vlo), l1 = (uint32_t)(q0 - vlo), l2 = (uint32_t)(q1 - vlo);
+        const uint32_t l3 = (uint32_t)(q0 + q1 - vlo), l4 = (uint32_t)(q2 - vlo);
+        const uint32_t l5 = (uint32_t)(q0 + q2 - vlo), l6 = (uint32_t)(q1 + q2 - vlo);
+        const uint32_t l7 = (uint32_t)(q0 + q1 + q2 - vlo);
+        // two 16-bit entries per word; H + L < 2^16, so a 32-bit add never carries
+        const uint32_t p0 = l0 | (l1 << 16), p1 = l2 | (l3 << 16), p2 = l4 | (l5 << 16),
+                       p3 = l6 | (l7 << 16);
+        uint4* row = reinterpret_cast<uint4*>(tab + 128 * t);
+#pragma unroll
+        for (int s8 = 0; s8 < 8; ++s8) {
+            const int m = (s8 + t) & 7;
+            const uint32_t h = (uint32_t)(((m & 1) ? q3 : 0) + ((m & 2) ? q4 : 0) + ((m & 4) ? q5 : 0) - vhi);
+            const uint32_t hd = h * 0x10001u;
+            row[m] = make_uint4(p0 + hd, p1 + hd, p2 + hd, p3 + hd);
+        }
+        vsum += vlo + vhi;
     }
     vsum = __reduce_add_sync(0xffffffffu, vsum);
     if (lane == 0 && vsum) atomicAdd(shift_acc, vsum);

@@ -37,7 +37,7 @@ EXPORTED_SYMBOLS = (
     "erq_search_learned_raw",
     "erq_debug_probe_model_grads", "erq_debug_probe_model_params",
     "erq_plan_create", "erq_plan_free", "erq_plan_set_learned", "erq_plan_autotune",
-    "erq_plan_set_tuning", "erq_plan_get_tuning", "erq_plan_search", "erq_plan_device_bytes", "erq_plan_set_graphs", "erq_plan_set_pipeline", "erq_debug_gemm_bf16", "erq_debug_set_gemm_wait_limit", "erq_debug_probe_fallbacks", "erq_debug_refine_stats",
+    "erq_plan_set_tuning", "erq_plan_get_tuning", "erq_plan_search", "erq_plan_device_bytes", "erq_plan_set_graphs", "erq_plan_set_pipeline", "erq_plan_search_async", "erq_debug_gemm_bf16", "erq_debug_set_gemm_wait_limit", "erq_debug_probe_fallbacks", "erq_debug_refine_stats",
 )
 
 
@@ -145,6 +145,8 @@ def load_library(path: str | None = None) -> C.CDLL:
     lib.erq_debug_probe_fallbacks.restype = C.c_int
     lib.erq_debug_refine_stats.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_uint64)]
     lib.erq_debug_refine_stats.restype = C.c_int
+    lib.erq_plan_search_async.argtypes = [vp, vp, u64, vp, vp, vp, vp]
+    lib.erq_plan_search_async.restype = C.c_int
     lib.erq_plan_set_pipeline.argtypes = [vp, C.c_int]
     lib.erq_plan_set_pipeline.restype = C.c_int
     lib.erq_plan_set_graphs.argtypes = [vp, C.c_int]

@@ -72,8 +72,15 @@ class Plan:
         check(self._lib.erq_plan_set_graphs(self._h, 1 if on else 0))
 
     def set_pipeline(self, chunks: int) -> None:
-        """Pieces a host-buffer batch runs as (0: by batch size, 1: one piece)."""
+        """Pieces a host-buffer batch runs as (1: one piece, 0: by batch size)."""
         check(self._lib.erq_plan_set_pipeline(self._h, chunks))
+
+    def search_buffers_async(self, queries, ids, dists=None, nprobe_used=None, stream=None) -> None:
+        """search_buffers without waiting (erq_plan_search_async): results are
+        valid once ``stream`` is synchronised; host buffers should be pinned."""
+        st = None if stream is None else C.c_void_p(stream.cuda_stream)
+        check(self._lib.erq_plan_search_async(self._h, _ptr(queries), int(queries.shape[0]),
+                                              _ptr(ids), _ptr(dists), _ptr(nprobe_used), st))
 
     def device_bytes(self) -> int:
         return int(self._lib.erq_plan_device_bytes(self._h))

@@ -202,10 +202,20 @@ ERQ_API uint64_t erq_plan_device_bytes(const erq_plan* plan);
 ERQ_API erq_status erq_plan_set_graphs(erq_plan* plan, int on);
 /* How erq_plan_search runs a batch with host buffers: as `chunks` pieces
  * whose host-to-device copies, searches and device-to-host copies overlap
- * (two buffer slots, two copy streams), 1 for one piece, 0 (the default) for
- * 4 pieces from 8192 queries and 2 from 4096.  Plans with max_batch below 4096
- * never split.  Results are the same in every case. */
+ * (two buffer slots, two copy streams); 1 (the default) for one piece, 0 for
+ * 4 pieces from 8192 queries and 2 from 4096.  Results are the same in every
+ * case. */
 ERQ_API erq_status erq_plan_set_pipeline(erq_plan* plan, int chunks);
+/* erq_plan_search that returns without waiting, also with host buffers: the
+ * queries are copied in on the plan's copy stream into one of two buffer
+ * slots (alternating between calls), the search and the copy of the results
+ * out run on `stream`.  So the copy-in of a call overlaps the search of the
+ * one before.  Host buffers must be pinned for the copies to overlap; the
+ * queries must stay unchanged and the results must not be read until
+ * `stream` has been synchronised.  Results equal erq_plan_search's. */
+ERQ_API erq_status erq_plan_search_async(erq_plan* plan, const float* queries, uint64_t nq,
+                                         uint32_t* ids, float* dists, uint32_t* nprobe_used,
+                                         void* stream);
 
 /* ---------------------------------------------------------------------------
  * IVF clustering.  Replaces the reference's offline clustering step

@@ -71,10 +71,9 @@ int orc_index_load(const char* path, orc_index** out) {
         rc = -2;
         goto fail;
     }
-    if (idx->K >= 20000) {
-        rc = -4;
-        goto fail;
-    }
+    /* K >= 20000: the reference would probe with HNSW (inc/index/IVF.hpp:157-161);
+     * files that carry their centroids in the main file are probed here with
+     * the Flat search's semantics, as the GPU library does. */
     idx->D = (idx->DIM + 63) / 64 * 64;
     const uint64_t D = idx->D, K = idx->K, N = idx->N;
     idx->sizes = (uint64_t*)malloc(sizeof(uint64_t) * K);

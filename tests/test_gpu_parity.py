@@ -192,9 +192,14 @@ def test_errors_are_reported(tmp_path):
     (tmp_path / "trunc.index").write_bytes(data[: len(data) // 2])
     with pytest.raises(ErqError, match="FORMAT"):
         IVF(str(tmp_path / "trunc.index"))
-    hdr = np.array([10, 64, 20000, 3], np.uint64).tobytes()
-    (tmp_path / "hnsw.index").write_bytes(hdr)
-    with pytest.raises(ErqError, match="UNSUPPORTED"):
+    # K >= 20000 as the reference writes it: the centroids only in the hnswlib
+    # side file (inc/index/Initializer.hpp:117-121), so the main file lacks
+    # the K x D centroid block - refused with a clear status
+    K, D, N, EX = 20000, 64, 20000, 3
+    body = (np.array([N, D, K, EX], np.uint64).tobytes() + np.ones(K, np.uint64).tobytes()
+            + bytes(D * D * 4 + K * (4 * D + 128) + N * (D * EX // 8 + 8)))
+    (tmp_path / "hnsw.index").write_bytes(body)
+    with pytest.raises(ErqError, match="UNSUPPORTED.*side file"):
         IVF(str(tmp_path / "hnsw.index"))
     # the handle still works after the failed calls
     ids, _ = idx.search_batch(g["qrot"], int(g["k"]), int(g["nprobe"]))

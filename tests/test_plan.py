@@ -229,3 +229,34 @@ def test_host_buffers_pipelined_in_chunks(uneven):
                 assert (bits(d_h.numpy()) == bits(ref_d)).all(), (graphs, chunks)
                 assert (u_h.numpy() == nprobe).all()
     plan.free()
+
+
+def test_async_host_buffer_calls(uneven):
+    """erq_plan_search_async: consecutive calls alternate buffer slots (the
+    copy-in of one overlaps the search of the one before); every call's
+    results, read after the stream is synchronised, equal the synchronous
+    search's, and a synchronous call after asynchronous ones is ordered."""
+    from erq_b200 import Plan
+
+    idx, q, qr, _ = uneven
+    k, nprobe, nq = 50, 6, 500
+    plan = Plan(idx, max_batch=nq, k=k, nprobe=nprobe)
+    st = torch.cuda.current_stream()
+    batches = [np.ascontiguousarray(qr[i * nq:(i + 1) * nq]) for i in range(3)]
+    want = [idx.search_batch(b, k, nprobe) for b in batches]
+    qh = [torch.from_numpy(b).pin_memory() for b in batches]
+    outs = [(torch.empty((nq, k), dtype=torch.int32).pin_memory(),
+             torch.empty((nq, k), dtype=torch.float32).pin_memory()) for _ in range(6)]
+    for c in range(6):
+        plan.search_buffers_async(qh[c % 3], outs[c][0], outs[c][1], stream=st)
+    torch.cuda.synchronize()
+    for c in range(6):
+        wi, wd = want[c % 3]
+        assert (outs[c][0].numpy().view(np.uint32) == wi).all(), c
+        assert (bits(outs[c][1].numpy()) == bits(wd)).all(), c
+    plan.search_buffers_async(qh[1], outs[0][0], outs[0][1], stream=st)
+    ids, d, _ = plan.search(batches[2])
+    torch.cuda.synchronize()
+    assert (ids == want[2][0]).all()
+    assert (outs[0][0].numpy().view(np.uint32) == want[1][0]).all()
+    plan.free()
