@@ -66,6 +66,15 @@ CONFIGS = {
         bits=4, nq=10_000, k=100, seed=20241, nprobe=None, recall_target=0.95,
         train_queries=0, save_base=False,
         data="synthetic: the 1M x 1536 unit-sphere mixture of the headline workload, 4-bit"),
+    # learned probing + batching at scale: 10M x 768, Zipf clusters, 3/5/9 bits
+    "zipf768-10M": dict(
+        gen="gauss", n=10_000_000, dim=768, comps=16384, sigma=0.3, zipf=1.1, K=16384,
+        bits_list=(3, 5, 9), nq=2000, k=100, seed=20245, recall_target=0.95,
+        qps_queries=100_000, train_queries=20_000, max_batch=4096, c5=True,
+        data="synthetic: seeded 16384-component Gaussian mixture (centres N(0, I), sigma 0.3) "
+             "with Zipf(1.1) component weights, 10M base, d=768; recall on 2000 queries "
+             "(exact top-100 by a TF32 shortlist of 1024 re-ranked in float64), QPS on 100k "
+             "queries in batches of sizes drawn from 1..4096"),
     # the small CPU-runnable case
     "gauss128-100k-4bit": dict(
         gen="gauss", n=100_000, dim=128, comps=256, sigma=0.3, zipf=None, K=1024,
@@ -369,18 +378,18 @@ def timed(step, steps, warmup, world, stream, clock_gpu=None):
     return max_over_ranks(e0.elapsed_time(e1), world), prof, clocks
 
 
-def learned_model(idx, d, cfg, plain_nprobe):
+def learned_model(idx, d, cfg, plain_nprobe, train=None):
     """The probe model of this workload, trained once and cached: labels from
     the plain search on the training queries, features from the probe kernel,
     training on the GPU by the library's kernels."""
     from erq_b200 import learned
 
     bins = learned.scaled_bins(plain_nprobe, cfg["K"])
-    path = os.path.join(d, "probe-" + "-".join(map(str, bins)) + ".model")
+    path = os.path.join(d, f"probe-b{cfg['bits']}-" + "-".join(map(str, bins)) + ".model")
     if os.path.exists(path):
         return learned.ProbeModel.load(path), json.load(open(path + ".json"))
     t0 = time.time()
-    train_q = np.load(os.path.join(d, "train_query.npy"))
+    train_q = np.load(os.path.join(d, "train_query.npy")) if train is None else train
     rot = idx.rotate(train_q)
     del train_q
     labels = learned.make_labels(idx, rot, cfg["k"], bins)
@@ -845,6 +854,109 @@ def run_secondary(args):
     return out
 
 
+# ----------------------------------------------- 10M x 768 recall/QPS curves
+def run_c5(args, cfg, name):
+    """Per bit width: the plain search's recall@10/@100 and QPS against nprobe,
+    and the learned search's against its confidence, with 100k queries in
+    uneven batches through a plan (max_batch 4096).  Data, clustering (the
+    library's k-means), index construction (the library's builder) and the
+    ground truth on the GPU; nothing of that is timed."""
+    import torch
+
+    from erq_b200 import IVF, Plan, datasets, learned, metrics
+    from erq_b200.build_index import build_index_gpu
+    from erq_b200.clustering import kmeans
+
+    torch.cuda.set_device(0)
+    work = cache_dir(name, dict(cfg, bits=0))
+    os.makedirs(work, exist_ok=True)
+    t0 = time.time()
+    nq_all = cfg["nq"] + cfg["qps_queries"] + cfg["train_queries"]
+    base, qall = datasets.gaussian_mixture_torch(cfg["n"], cfg["dim"], cfg["comps"], cfg["sigma"],
+                                                 cfg["seed"], nq_all, cfg["zipf"])
+    log(f"c5: data at {time.time() - t0:.1f}s")
+    cent, ids = kmeans(base, cfg["K"], iters=20, seed=cfg["seed"] + 1)
+    log(f"c5: k-means at {time.time() - t0:.1f}s")
+    q_eval = qall[:cfg["nq"]]
+    q_qps = qall[cfg["nq"]:cfg["nq"] + cfg["qps_queries"]].cpu().numpy()
+    q_train = qall[cfg["nq"] + cfg["qps_queries"]:].cpu().numpy()
+    gt, _ = datasets.ground_truth_shortlist(base, q_eval, cfg["k"])
+    gt = gt.cpu().numpy().astype(np.uint32)
+    q_eval = q_eval.cpu().numpy()
+    log(f"c5: ground truth at {time.time() - t0:.1f}s")
+    rng = np.random.default_rng(cfg["seed"] + 5)
+    sizes = []
+    while sum(sizes) < cfg["qps_queries"]:
+        sizes.append(int(min(cfg["max_batch"], np.exp(rng.uniform(0, np.log(cfg["max_batch"]))))))
+    sizes[-1] -= sum(sizes) - cfg["qps_queries"]
+    qd = torch.from_numpy(q_qps).cuda()
+    k = cfg["k"]
+    out = {}
+    for bits in cfg["bits_list"]:
+        path = os.path.join(work, f"ivf{bits}.index")
+        tb = time.time()
+        build_index_gpu(base, cent, ids, bits, path, seed=cfg["seed"] + bits)
+        build_s = time.time() - tb
+        idx = IVF(path)
+        res = {"build_s": round(build_s, 1), "plain": [], "learned": []}
+        ids_d = torch.empty((cfg["max_batch"], k), dtype=torch.int32, device="cuda")
+
+        def qps_of(plan):
+            st = torch.cuda.current_stream()
+            o = 0
+            for b in sizes[:8]:  # warm-up and graph capture of some sizes
+                plan.search_buffers(qd[:b], ids_d[:b], stream=st)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            for b in sizes:
+                plan.search_buffers(qd[o:o + b], ids_d[:b], stream=st)
+                o += b
+            e1.record(st)
+            torch.cuda.synchronize()
+            return cfg["qps_queries"] / (e0.elapsed_time(e1) / 1e3)
+
+        chosen = None
+        for nprobe in (1, 2, 4, 8, 16, 32, 64, 128, 256, 512, 1024):
+            r_ids, _ = idx.search_raw(q_eval, k, nprobe, with_dists=False)
+            r100 = metrics.recall_at_k(r_ids, gt, k)
+            r10 = metrics.recall_at_k(r_ids[:, :10], gt[:, :10], 10)
+            plan = Plan(idx, max_batch=cfg["max_batch"], k=k, nprobe=nprobe, raw=True)
+            qps = qps_of(plan)
+            plan.free()
+            res["plain"].append({"nprobe": nprobe, "recall@10": round(r10, 4),
+                                 "recall@100": round(r100, 4), "qps": round(qps, 1)})
+            log(f"c5 {bits}-bit nprobe {nprobe}: {res['plain'][-1]}")
+            if chosen is None and r100 >= cfg["recall_target"]:
+                chosen = nprobe
+            if r100 > 0.995:
+                break
+        if chosen is not None:
+            cfg_l = dict(cfg, bits=bits)
+            model, meta = learned_model(idx, work, cfg_l, chosen, train=q_train)
+            res["model"] = meta
+            plan_l = Plan(idx, max_batch=cfg["max_batch"], k=k, nprobe=chosen, model=model, raw=True)
+            for conf in (0.02, 0.1, 0.3, 0.5, 0.7, 0.9, 0.99):
+                plan_l.set_learned(conf, LEARNED_MIN_PROB)
+                ids_l, _, used = learned.search_learned(idx, model, idx.rotate(q_eval), k, chosen,
+                                                        conf, LEARNED_MIN_PROB)
+                qps = qps_of(plan_l)
+                res["learned"].append({"confidence": conf, "mean_nprobe": round(float(used.mean()), 1),
+                                       "recall@10": round(metrics.recall_at_k(ids_l[:, :10], gt[:, :10], 10), 4),
+                                       "recall@100": round(metrics.recall_at_k(ids_l, gt, k), 4),
+                                       "qps": round(qps, 1)})
+                log(f"c5 {bits}-bit learned {res['learned'][-1]}")
+            plan_l.free()
+            model.free()
+        res["plain_nprobe_at_target"] = chosen
+        idx.free()
+        out[f"{bits}-bit"] = res
+        os.remove(path)
+    print(json.dumps({"metric": "recall@10/100 and QPS curves, 10M x 768 Zipf, K=16384",
+                      "workload": name, "data": cfg["data"], "batch_sizes": len(sizes),
+                      "results": out}), flush=True)
+
+
 # ---------------------------------------------------- batched latency mode
 def run_latency(args, cfg, name):
     """Per batch size B of cfg["latency_batches"]: a plan autotuned for B,
@@ -1033,7 +1145,9 @@ def main():
     if args.impl == "reference":
         run_reference(args, cfg, args.config)
     else:
-        if cfg.get("latency_batches"):
+        if cfg.get("c5"):
+            run_c5(args, cfg, args.config)
+        elif cfg.get("latency_batches"):
             run_latency(args, cfg, args.config)
         else:
             out = run_ours(args, cfg, args.config)

@@ -142,14 +142,66 @@ def sphere_mixture_torch(n: int, d: int, n_comp: int, sigma: float, seed: int,
 
 
 def gaussian_mixture_torch(n: int, d: int, n_comp: int, sigma: float, seed: int,
-                           n_query: int = 0, device="cuda"):
+                           n_query: int = 0, zipf_s: float | None = None, device="cuda"):
+    """GPU twin of ``gaussian_mixture``; Zipf(zipf_s) component weights when
+    given (the weights assigned to components in a seeded random order)."""
     import torch
 
     g = torch.Generator(device=device).manual_seed(seed)
     centres = torch.randn(n_comp, d, generator=g, device=device)
-    comp = torch.randint(0, n_comp, (n + n_query,), generator=g, device=device)
-    x = centres[comp] + sigma * torch.randn(n + n_query, d, generator=g, device=device)
+    if zipf_s is None:
+        comp = torch.randint(0, n_comp, (n + n_query,), generator=g, device=device)
+    else:
+        w = torch.from_numpy(zipf_weights(n_comp, zipf_s)).to(device)
+        perm = torch.randperm(n_comp, generator=g, device=device)
+        comp = perm[torch.multinomial(w, n + n_query, replacement=True, generator=g)]
+    x = torch.empty(n + n_query, d, device=device)
+    step = 1 << 20
+    for s in range(0, n + n_query, step):
+        c = comp[s:s + step]
+        x[s:s + step] = centres[c] + sigma * torch.randn(c.numel(), d, generator=g, device=device)
     return x[:n], x[n:]
+
+
+def ground_truth_shortlist(base, query, k: int, shortlist: int = 1024, qstep: int = 1024,
+                           bstep: int = 1 << 20):
+    """Top-k by squared L2 for large bases: a TF32 distance pass keeps the
+    ``shortlist`` nearest per query, which are then ranked exactly in float64.
+    Returns (ids int64 [nq, k], dists float64 [nq, k])."""
+    import torch
+
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = True
+    try:
+        nq = query.shape[0]
+        cand_d = torch.full((nq, shortlist), float("inf"), device=base.device)
+        cand_i = torch.zeros((nq, shortlist), dtype=torch.long, device=base.device)
+        for b0 in range(0, base.shape[0], bstep):
+            b = base[b0:b0 + bstep]
+            bb = (b * b).sum(1)
+            for q0 in range(0, nq, qstep):
+                q = query[q0:q0 + qstep]
+                d = bb[None, :] - 2.0 * (q @ b.T)
+                kk = min(shortlist, d.shape[1])
+                vd, vi = d.topk(kk, dim=1, largest=False)
+                cd = torch.cat([cand_d[q0:q0 + qstep], vd], 1)
+                ci = torch.cat([cand_i[q0:q0 + qstep], vi + b0], 1)
+                o = cd.topk(shortlist, dim=1, largest=False).indices
+                cand_d[q0:q0 + qstep] = cd.gather(1, o)
+                cand_i[q0:q0 + qstep] = ci.gather(1, o)
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = prev
+    best_i = torch.empty((nq, k), dtype=torch.long, device=base.device)
+    best_d = torch.empty((nq, k), dtype=torch.float64, device=base.device)
+    rstep = 128
+    for q0 in range(0, nq, rstep):
+        q = query[q0:q0 + rstep].double()
+        ci = cand_i[q0:q0 + rstep]
+        ex = ((base[ci].double() - q[:, None, :]) ** 2).sum(2)
+        o = torch.argsort(ex, dim=1, stable=True)[:, :k]
+        best_i[q0:q0 + rstep] = ci.gather(1, o)
+        best_d[q0:q0 + rstep] = ex.gather(1, o)
+    return best_i, best_d
 
 
 def kmeans_torch(x, k: int, iters: int = 20, seed: int = 0):
