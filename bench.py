@@ -72,7 +72,8 @@ CONFIGS = {
         bits_list=(3, 5, 9), nq=2000, k=100, seed=20245, recall_target=0.95,
         qps_queries=100_000, train_queries=20_000, max_batch=4096, c5=True,
         data="synthetic: seeded 16384-component Gaussian mixture (centres N(0, I), sigma 0.3) "
-             "with Zipf(1.1) component weights, 10M base, d=768; recall on 2000 queries "
+             "with Zipf(1.1) component weights, 10M base, d=768, clustered by erq_kmeans; "
+             "recall on 2000 queries "
              "(exact top-100 by a TF32 shortlist of 1024 re-ranked in float64), QPS on 100k "
              "queries in batches of sizes drawn from 1..4096"),
     # the small CPU-runnable case
@@ -863,8 +864,8 @@ def run_c5(args, cfg, name):
     ground truth on the GPU; nothing of that is timed."""
     import torch
 
-    from erq_b200 import IVF, Plan, datasets, learned, metrics
-    from erq_b200.build_index import build_index_gpu
+    from erq_b200 import IVF, Plan, datasets, indexfile, learned, metrics
+    from erq_b200.build_index import build_index_torch
     from erq_b200.clustering import kmeans
 
     torch.cuda.set_device(0)
@@ -895,7 +896,12 @@ def run_c5(args, cfg, name):
     for bits in cfg["bits_list"]:
         path = os.path.join(work, f"ivf{bits}.index")
         tb = time.time()
-        build_index_gpu(base, cent, ids, bits, path, seed=cfg["seed"] + bits)
+        # the torch builder (plumbing): erq_build_index's exact fast_quantize
+        # keeps a priority queue per vector in global memory and is meant for
+        # reference-identical files, not for 10M vectors
+        indexfile.write_index(path, build_index_torch(base, torch.from_numpy(cent).cuda(),
+                                                      torch.from_numpy(ids.astype(np.int64)).cuda(),
+                                                      bits, seed=cfg["seed"] + bits))
         build_s = time.time() - tb
         idx = IVF(path)
         res = {"build_s": round(build_s, 1), "plain": [], "learned": []}

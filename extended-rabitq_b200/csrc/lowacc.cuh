@@ -229,11 +229,11 @@ __global__ void __launch_bounds__(kScanWarps * 32, 1) scan_lowacc_kernel(LowScan
     for (uint32_t n = 0; n < my_blocks && ok; ++n) {
         int acc = 0;
         for (uint32_t u = 0; u < us.nu; ++u, ++m) {
-            if (!us.wait(m)) {
+            if (!us.wait_next()) {
                 ok = false;
                 break;
             }
-            const uint32_t st = us.stage(m) + lane * 16;
+            const uint32_t st = us.stage_next() + lane * 16;
             const uint32_t c0 = u * kUnitChunks;
             const uint32_t nch = min((uint32_t)kUnitChunks, us.nc - c0);
 #pragma unroll
@@ -246,6 +246,7 @@ __global__ void __launch_bounds__(kScanWarps * 32, 1) scan_lowacc_kernel(LowScan
                 }
             }
             us.refill(m, lane);
+            us.advance();
         }
         if (!ok) break;
         const uint32_t b = warp + n * kScanWarps;

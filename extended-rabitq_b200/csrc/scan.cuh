@@ -54,9 +54,9 @@ __host__ __device__ constexpr uint32_t hex_table_bytes(int D) { return (uint32_t
 // qq entries (padded with zeros to whole chunks)
 __host__ __device__ constexpr int hex_qq_len(int D) { return hex_chunks(D) * 16 * kHexDims; }
 
-constexpr int kUnitChunks = 2;                   // chunks per staged copy
+constexpr int kUnitChunks = 4;                   // chunks per staged copy
 constexpr uint32_t kUnitBytes = kUnitChunks * 512;
-constexpr int kRing = 4;                         // staged copies per warp
+constexpr int kRing = 2;                         // staged copies per warp
 constexpr uint32_t kScanWaitLimit = 1u << 24;    // polls before a wait gives up
 constexpr uint32_t kScanDrainLimit = 1u << 26;   // polls of the exit drain
 constexpr uint32_t kScanTimeoutBit = 2u;         // bit of the device status word
@@ -256,14 +256,20 @@ struct UnitStream {
             issue(m + kRing);
         }
     }
-    // all lanes; false (warp-uniform) if the copy of unit m did not land in time
-    __device__ __forceinline__ bool wait(uint32_t m) const {
-        const uint32_t slot = (count + m) % kRing, parity = ((count + m) / kRing) & 1;
-        return __all_sync(0xffffffffu, mbar_wait(bars + 8 * slot, parity, kScanWaitLimit));
+    // The consumer's cursor: ring slot and barrier parity of the next unit
+    // (count + m); advance() after each consumed unit.
+    uint32_t slot = 0, phase = 0;
+    __device__ __forceinline__ void advance() {
+        if (++slot == (uint32_t)kRing) {
+            slot = 0;
+            phase ^= 1u;
+        }
     }
-    __device__ __forceinline__ uint32_t stage(uint32_t m) const {
-        return ring + ((count + m) % kRing) * kUnitBytes;
+    // all lanes; false (warp-uniform) if the next unit's copy did not land in time
+    __device__ __forceinline__ bool wait_next() const {
+        return __all_sync(0xffffffffu, mbar_wait(bars + 8 * slot, phase, kScanWaitLimit));
     }
+    __device__ __forceinline__ uint32_t stage_next() const { return ring + slot * kUnitBytes; }
     // lane 0, after a wait gave up at unit `consumed`: lets every copy issued
     // but not consumed land before the block exits or reuses the ring
     __device__ __forceinline__ void drain(uint32_t consumed) const {
@@ -341,21 +347,26 @@ __global__ void __launch_bounds__(kScanWarps * 32, 2) scan_kernel(ScanArgs a) {
 
     uint32_t m = 0;
     bool ok = true;
+    const uint32_t full_units = us.nc / kUnitChunks;  // units of kUnitChunks chunks per block
     for (uint32_t n = 0; n < my_blocks && ok; ++n) {
         int acc[1] = {0};
         for (uint32_t u = 0; u < us.nu; ++u, ++m) {
-            if (!us.wait(m)) {
+            if (!us.wait_next()) {
                 ok = false;
                 break;
             }
-            const uint32_t st = us.stage(m) + lane * 16;
-            const uint32_t c0 = u * kUnitChunks;
-            const uint32_t nch = min((uint32_t)kUnitChunks, us.nc - c0);
-            const uint32_t cb = tables_s + c0 * 2048;
+            const uint32_t st = us.stage_next() + lane * 16;
+            const uint32_t cb = tables_s + u * (kUnitChunks * 2048);
+            if (u < full_units) {
 #pragma unroll
-            for (uint32_t cc = 0; cc < (uint32_t)kUnitChunks; ++cc)
-                if (cc < nch) hex_lookup16<1, 0>(lds128(st + cc * 512), cb + cc * 2048, 1, acc);
+                for (uint32_t cc = 0; cc < (uint32_t)kUnitChunks; ++cc)
+                    hex_lookup16<1, 0>(lds128(st + cc * 512), cb + cc * 2048, 1, acc);
+            } else {
+                for (uint32_t cc = 0; cc < us.nc - u * kUnitChunks; ++cc)
+                    hex_lookup16<1, 0>(lds128(st + cc * 512), cb + cc * 2048, 1, acc);
+            }
             us.refill(m, lane);
+            us.advance();
         }
         if (!ok) break;
         const uint32_t b = warp + n * kScanWarps;

@@ -107,6 +107,8 @@ __global__ void __launch_bounds__(WARPS * 32) scan_batched_kernel(ScanBatchArgs 
     us.bars = bars_s + warp * kRing * 8;
     us.count = 0;
     us.total = 0;
+    us.slot = 0;
+    us.phase = 0;
     bool ok = true;
 
     while (true) {
@@ -180,23 +182,28 @@ __global__ void __launch_bounds__(WARPS * 32) scan_batched_kernel(ScanBatchArgs 
         const uint32_t tables_s = reinterpret_cast<volatile uint32_t*>(info)[2];
 
         uint32_t m = 0;
+        const uint32_t full_units = us.nc / kUnitChunks;
         for (uint32_t n = 0; n < my_blocks && ok; ++n) {
             int acc[QB];
 #pragma unroll
             for (int j = 0; j < QB; ++j) acc[j] = 0;
             for (uint32_t u = 0; u < us.nu; ++u, ++m) {
-                if (!us.wait(m)) {
+                if (!us.wait_next()) {
                     ok = false;
                     break;
                 }
-                const uint32_t st = us.stage(m) + lane * 16;
-                const uint32_t c0 = u * kUnitChunks;
-                const uint32_t nchk = min((uint32_t)kUnitChunks, us.nc - c0);
-                const uint32_t cb = tables_s + c0 * 2048;
+                const uint32_t st = us.stage_next() + lane * 16;
+                const uint32_t cb = tables_s + u * (kUnitChunks * 2048);
+                if (u < full_units) {
 #pragma unroll
-                for (uint32_t cc = 0; cc < (uint32_t)kUnitChunks; ++cc)
-                    if (cc < nchk) hex_lookup16<QB, QSTR>(lds128(st + cc * 512), cb + cc * 2048, qn, acc);
+                    for (uint32_t cc = 0; cc < (uint32_t)kUnitChunks; ++cc)
+                        hex_lookup16<QB, QSTR>(lds128(st + cc * 512), cb + cc * 2048, qn, acc);
+                } else {
+                    for (uint32_t cc = 0; cc < us.nc - u * kUnitChunks; ++cc)
+                        hex_lookup16<QB, QSTR>(lds128(st + cc * 512), cb + cc * 2048, qn, acc);
+                }
                 us.refill(m, lane);
+                us.advance();
             }
             if (!ok) break;
             const uint32_t b = us.b_first + n * WARPS;
