@@ -273,6 +273,27 @@ PARITY_QUERIES = 200
 # back to the fixed nprobe (8 depths: a uniform guess gives each 0.125).
 LEARNED_MIN_PROB = 0.25
 
+# DRAM bytes (read + write) per algorithmic byte, from one-pass ncu captures of
+# dram__bytes_read.sum + dram__bytes_write.sum on this bench's headline
+# workload (profiles/dram_traffic_sphere1536_1M_8bit.md); a launch's traffic
+# is that ratio times its algorithmic bytes.  Empty for a kernel not captured.
+DRAM_PER_ALGORITHMIC_BYTE = {}
+
+
+def json_peak():
+    """hbm_gbs of MEASURED_PEAKS.json, or None when the file is absent."""
+    try:
+        return json.load(open(os.path.join(REPO, "MEASURED_PEAKS.json"))).get("hbm_gbs")
+    except (OSError, ValueError):
+        return None
+
+
+def traffic_per_launch(kernel, step_bytes, launches_per_step):
+    r = DRAM_PER_ALGORITHMIC_BYTE.get(kernel)
+    if r is None or not launches_per_step:
+        return None
+    return int(r * step_bytes / launches_per_step)
+
 
 def reference_parity(index_path, idx, query, k, nprobe, model=None, confidence=None):
     """Results of the GPU search on the first PARITY_QUERIES queries against the
@@ -346,10 +367,11 @@ def choose_nprobe(idx, qraw, gt, cfg):
     return best
 
 
-def timed(step, steps, warmup, world, stream, clock_gpu=None):
+def timed(step, steps, warmup, world, stream, clock_gpu=None, label=None):
     """`warmup` untimed calls, then `steps` calls between CUDA events on
     `stream` bracketed by barrier + synchronize; returns (max-over-ranks ms,
-    per-kernel profile of the timed calls, clock samples)."""
+    per-kernel profile of the timed calls, clock samples).  `label` names an
+    NVTX range around the timed calls (for a profiler's range filter)."""
     import torch
 
     from erq_b200 import _lib as L
@@ -365,10 +387,14 @@ def timed(step, steps, warmup, world, stream, clock_gpu=None):
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     if sampler:
         sampler.mark_start()
+    if label:
+        torch.cuda.nvtx.range_push(label)
     e0.record(stream)
     for _ in range(steps):
         step()
     e1.record(stream)
+    if label:
+        torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
     if sampler:
         sampler.mark_end()
@@ -470,7 +496,8 @@ def run_ours(args, cfg, name):
     def plain_host():
         idx.search_raw(qh, k, nprobe, ids=ids_h, dists=dist_h, stream=stream)
 
-    ms_p, prof_p, clocks_p = timed(plain_dev, args.steps, args.warmup, world, stream, local)
+    ms_p, prof_p, clocks_p = timed(plain_dev, args.steps, args.warmup, world, stream, local,
+                                   label="plain")
     assert (ids_d.cpu().numpy().view(np.uint32) == ids0).all()
     plain = {"value": round(world * nq * args.steps / (ms_p / 1e3), 1), "nprobe": nprobe,
              "recall@100": round(recall, 5), "ms_per_step": round(ms_p / args.steps, 4),
@@ -487,7 +514,7 @@ def run_ours(args, cfg, name):
     # --- batched plans (CUDA graphs, work-list scan, autotuned tiles)
     from erq_b200 import Plan
 
-    def plan_mode(plan, expect):
+    def plan_mode(plan, expect, label):
         def dev():
             plan.search_buffers(qd, ids_d, dist_d, stream=stream)
 
@@ -497,7 +524,7 @@ def run_ours(args, cfg, name):
         def host_sync():  # each call returns with its results in host memory
             plan.search_buffers(qh, ids_h, dist_h, stream=stream)
 
-        ms, _, clocks = timed(dev, args.steps, args.warmup, world, stream, local)
+        ms, _, clocks = timed(dev, args.steps, args.warmup, world, stream, local, label=label)
         assert (ids_d.cpu().numpy().view(np.uint32) == expect).all()
         e2e = None
         if not args.no_e2e:
@@ -508,7 +535,7 @@ def run_ours(args, cfg, name):
             plan.e2e_sync_ms = e2e_sync
         # per-kernel times: the same steps with the kernels launched one by one
         plan.set_graphs(False)
-        _, prof, _ = timed(dev, args.steps, 1, world, stream)
+        _, prof, _ = timed(dev, args.steps, 1, world, stream, label=label + "-kernels")
         plan.set_graphs(True)
         return ms, e2e, clocks, prof
 
@@ -519,7 +546,7 @@ def run_ours(args, cfg, name):
     if not args.no_batched:
         plan_b = Plan(idx, max_batch=nq, k=k, nprobe=nprobe, raw=True)
         tune_b, _ = plan_b.autotune(query, reps=2)
-        ms_b, e2e_b, clocks_b, prof_b = plan_mode(plan_b, ids0)
+        ms_b, e2e_b, clocks_b, prof_b = plan_mode(plan_b, ids0, "batched")
         batched = {"value": round(world * nq * args.steps / (ms_b / 1e3), 1), "nprobe": nprobe,
                    "recall@100": round(recall, 5), "ms_per_step": round(ms_b / args.steps, 4),
                    "tuning": tune_b,
@@ -569,7 +596,7 @@ def run_ours(args, cfg, name):
             log(f"learned probe fallback rate {learned_fallback_rate:.5f}; refinement per "
                 "query: " + ", ".join(f"{kk} {v / nq:.1f}" for kk, v in rst_l.items()))
             tune_l, _ = plan_l.autotune(query, reps=2)
-            ms_l, e2e_l, clocks_l, prof_l = plan_mode(plan_l, ids_l)
+            ms_l, e2e_l, clocks_l, prof_l = plan_mode(plan_l, ids_l, "learned")
             take = np.arange(cids.shape[1])[None, :] < used.astype(np.int64)[:, None]
             scan_bytes_l = int(nblocks[cids.astype(np.int64)][take].sum()) * block_bytes
             learned_info = {"value": round(world * nq * args.steps / (ms_l / 1e3), 1),
@@ -594,34 +621,62 @@ def run_ours(args, cfg, name):
     mode = min(modes, key=lambda m: modes[m]["ms"])
     chosen = modes[mode]
 
+    # the scan at deeper probes (scan-dominated points of the plain path;
+    # not the headline, whose nprobe is the smallest reaching the target)
+    depth_sweep = []
+    if not args.no_depth_sweep:
+        nd = min(nq, 2000)
+        qd_s = qd[:nd]
+        ids_s = torch.empty((nd, k), dtype=torch.int32, device="cuda")
+        cids_d, _ = idx.debug_probe(qrot_h[:nd], 64)
+        for npd in (16, 64):
+            def depth_step():
+                idx.search_raw(qd_s, k, npd, ids=ids_s, with_dists=False, stream=stream)
+
+            ms_d, prof_d, _ = timed(depth_step, 5, 3, world, stream)
+            nl, tms = prof_d.get("scan", (0, 0.0))
+            sbytes = int(nblocks[cids_d[:, :npd].astype(np.int64)].sum()) * block_bytes
+            ach = sbytes * 5 / (tms / 1e3) / 1e9 if tms else 0.0
+            depth_sweep.append({"nprobe": npd, "queries": nd, "kernel": "scan_kernel",
+                                "scan_ms_per_step": round(tms / 5, 4),
+                                "scan_bytes_per_step": sbytes, "achieved_gbs": round(ach, 1),
+                                "frac": round(ach / (json_peak() or 6650.0), 4),
+                                "refine_ms_per_step": round(prof_d.get("refine", (0, 0.0))[1] / 5, 4),
+                                "ms_per_step": round(ms_d / 5, 4)})
+            log(f"scan depth sweep: {depth_sweep[-1]}")
+
     ratio = metrics.average_distance_ratio(query[:sub], base, chosen["ids"][:sub].astype(np.int64),
                                            gt[:sub].astype(np.int64), k)
     prof = chosen["prof"]
     launches = sum(v[0] for v in prof.values())
-    peaks = {}
-    try:
-        peaks = json.load(open(os.path.join(REPO, "MEASURED_PEAKS.json")))
-    except (OSError, ValueError):
-        pass
-    peak = peaks.get("hbm_gbs")
+    peak = json_peak()
     peak_src = "measured" if peak else "fallback"
     peak = peak or 6650.0
     # algorithmic bytes per step of the two HBM-side kernels: scan = the
     # probed clusters' code blocks (4D + 128 B per block), refine = the exact
     # candidates' EX-code rows + xipnorm + id (D*EX/8 + 8 B each)
-    kernel_names = {"scan": "scan_kernel" if mode == "plain" else "scan_batched_kernel",
-                    "refine": "refine_kernel"}
-    rooflines = {}
-    for kn, step_bytes in (("scan", chosen["scan_bytes"]), ("refine", chosen["refine_bytes"])):
-        n_launch, tot_ms = prof.get(kn, (0, 0.0))
-        if not n_launch:
-            continue
-        achieved = step_bytes * args.steps / n_launch / (tot_ms / n_launch / 1e3) / 1e9
-        rooflines[kn] = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
-                         "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
-                         "kernel": kernel_names[kn], "ms_per_step": round(tot_ms / args.steps, 4),
-                         "bytes_per_step": int(step_bytes),
-                         "peak_source": f"{peak_src} hbm_gbs (copy)"}
+    def mode_rooflines(m):
+        md = modes[m]
+        names = {"scan": "scan_kernel" if m == "plain" else "scan_batched_kernel",
+                 "refine": "refine_kernel"}
+        res = {}
+        for kn, step_bytes in (("scan", md["scan_bytes"]), ("refine", md["refine_bytes"])):
+            n_launch, tot_ms = md["prof"].get(kn, (0, 0.0))
+            if not n_launch:
+                continue
+            achieved = step_bytes * args.steps / n_launch / (tot_ms / n_launch / 1e3) / 1e9
+            res[kn] = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+                       "unit": "GB/s", "frac": round(achieved / peak, 4),
+                       "traffic": traffic_per_launch(names[kn], step_bytes, n_launch / args.steps),
+                       "kernel": names[kn], "ms_per_step": round(tot_ms / args.steps, 4),
+                       "bytes_per_step": int(step_bytes),
+                       "peak_source": f"{peak_src} hbm_gbs (copy)"}
+        return res
+
+    rooflines = mode_rooflines(mode)
+    for m, info in (("plain", plain), ("batched", batched), ("learned", learned_info)):
+        if info is not None and m in modes:
+            info["rooflines"] = mode_rooflines(m)
     dominant = max(rooflines, key=lambda kn: rooflines[kn]["ms_per_step"]) if rooflines else None
     e2e_ms = chosen["e2e_ms"]
     cpu = None
@@ -674,6 +729,7 @@ def run_ours(args, cfg, name):
             "gpu_launches": int(launches),
             "roofline": rooflines.get(dominant),
             "roofline_other": {kn: r for kn, r in rooflines.items() if kn != dominant},
+            "scan_depth_sweep": depth_sweep,
             "kernels_ms_per_step": {kk: round(v[1] / args.steps, 4) for kk, v in prof.items()
                                     if v[0]},
             "cpu_baseline": cpu,
@@ -1131,6 +1187,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer e2e timing")
     ap.add_argument("--no-learned", action="store_true", help="plain fixed-nprobe search only")
+    ap.add_argument("--no-depth-sweep", action="store_true",
+                    help="skip the plain-path scan timing at nprobe 16 and 64")
     ap.add_argument("--no-batched", action="store_true", help="skip the plain batched plan")
     ap.add_argument("--queries", type=int, default=0,
                     help="use only the first N queries of the batch (profiling cases)")

@@ -165,12 +165,13 @@ ERQ_API erq_status erq_search_learned_raw(const erq_index* index, const erq_prob
 typedef struct erq_plan erq_plan;
 
 typedef struct {
-    uint32_t queries_per_item;  /* Q: 1, 2, 4 or 8 */
+    uint32_t queries_per_item;  /* Q: 1, 2 or 4 queries sharing one cluster chunk */
     uint32_t blocks_per_item;   /* C: cluster chunk, in 32-vector blocks */
-    uint32_t warps;             /* warps per scan block: 4 or 8 (Q = 1 needs 4, Q = 8 needs 8) */
-    uint32_t refine_warps;      /* warps per refinement block: 4, 32 (the wide form, windows of
-                                   128 blocks), or 0 = 32 when the batch has no more queries
-                                   than SMs, else 4 */
+    uint32_t warps;             /* warps per scan block: 4 or 8 */
+    uint32_t refine_warps;      /* refinement form: 4 (a block of 4 warps per query, windows
+                                   of 16 blocks), 32 (the wide form, windows of 128 blocks),
+                                   or 0 = 32 when the batch has no more queries than SMs,
+                                   else 4 */
 } erq_plan_tuning;
 
 /* model may be NULL (plain fixed-nprobe search); with a model, nprobe is the

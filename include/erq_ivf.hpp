@@ -15,8 +15,10 @@
 //     included, with the output already sized rows x D);
 //   * errors throw erq::Error (the reference asserts or aborts);
 //   * search_batch answers many queries in one call (the GPU's fast path);
-//   * building an index (IVF(n, dim, k, b) + construct + save) stays with the
-//     reference's create_index, whose files this class reads.
+//   * building keeps the reference's calls (IVF(n, dim, k, b), construct,
+//     save; src/create_index.cpp:45-49) but runs at save(): construct only
+//     records its three pointers, which must stay valid until then, and
+//     set_rotation may fix the rotation (else one is drawn from a seed).
 #pragma once
 
 #include <cstdint>
@@ -87,6 +89,9 @@ class IVF {
    public:
     IVF() = default;
     explicit IVF(int device) : device_(device) {}
+    // IVF(n, dim, k, b) (inc/index/IVF.hpp:116-153): an index to be built.
+    IVF(size_t n, size_t dim, size_t k, size_t total_bits, int device = 0)
+        : device_(device), build_n_(n), build_dim_(dim), build_k_(k), build_bits_(total_bits) {}
     IVF(const IVF&) = delete;
     IVF& operator=(const IVF&) = delete;
     ~IVF() { erq_index_free(index_); }
@@ -117,6 +122,29 @@ class IVF {
         check(erq_search(index_, queries, nq, k, nprobe, ids, dists, stream));
     }
 
+    // IVF::construct (inc/index/IVF.hpp:155-217): data[n][dim], centroids[k][dim]
+    // (raw), cluster_ids[n]; host or device pointers, kept until save().
+    void construct(const float* data, const float* centroids, const uint32_t* cluster_ids) {
+        if (!build_n_) throw Error(ERQ_ERR_INVALID_ARGUMENT, "construct: use IVF(n, dim, k, b)");
+        data_ = data;
+        centroids_ = centroids;
+        cluster_ids_ = cluster_ids;
+    }
+    // The rotation to use (D x D row-major, D = dim rounded up to 64), in
+    // place of one drawn from `seed`; the file then equals the reference's
+    // for the same rotation.  Kept by pointer until save().
+    void set_rotation(const float* rotation, uint64_t seed = 0) {
+        rotation_ = rotation;
+        seed_ = seed;
+    }
+    // IVF::save (inc/index/IVF.hpp:219-252): quantises on the GPU
+    // (erq_build_index) and writes the index file.
+    void save(const char* filename) const {
+        if (!data_) throw Error(ERQ_ERR_INVALID_ARGUMENT, "save: nothing constructed");
+        check(erq_build_index(data_, build_n_, build_dim_, centroids_, build_k_, cluster_ids_,
+                              build_bits_, rotation_, seed_, filename, device_));
+    }
+
     size_t padded_dim() const { return info_.padded_dim; }  // IVF::padded_dim
     size_t k() const { return info_.num_clusters; }         // IVF::k
     size_t size() const { return info_.n; }
@@ -128,6 +156,13 @@ class IVF {
     erq_index* index_ = nullptr;
     erq_index_info info_{};
     Rotator rot_;
+    // build side
+    size_t build_n_ = 0, build_dim_ = 0, build_k_ = 0, build_bits_ = 0;
+    const float* data_ = nullptr;
+    const float* centroids_ = nullptr;
+    const uint32_t* cluster_ids_ = nullptr;
+    const float* rotation_ = nullptr;
+    uint64_t seed_ = 0;
 };
 
 }  // namespace erq

@@ -126,3 +126,25 @@ def test_build_with_own_rotation_searches(tmp_path):
     assert (got_d.view(np.uint32) == want_d.view(np.uint32)).all()
     o.close()
     idx.free()
+
+
+def test_create_index_driver_equals_reference(tmp_path):
+    """extended-rabitq_b200/examples/erq_create_index.cpp - the reference's
+    create_index over the C++ facade (IVF(n, dim, k, b) + construct + save)
+    - reads the same files and, given the reference's rotation, writes the
+    same index."""
+    from conftest import PKG
+
+    from erq_b200 import indexfile
+
+    base, cent, ids = _case(2500, 200, 16, 91)
+    ref_path = _reference_index(tmp_path, base, cent, ids, 7)
+    P = indexfile.read_index(ref_path).P
+    rot = tmp_path / "rotation.bin"
+    P.astype(np.float32).tofile(rot)
+    ref_copy = str(tmp_path / "ref.index")
+    os.replace(ref_path, ref_copy)
+    subprocess.run(["make", "-s", "-C", PKG, "bin/erq_create_index"], check=True)
+    subprocess.run([os.path.join(PKG, "bin", "erq_create_index"), str(tmp_path / "data"), "bld",
+                    "16", "7", str(rot)], check=True, stdout=subprocess.DEVNULL, timeout=300)
+    _compare(ref_copy, ref_path)

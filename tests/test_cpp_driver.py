@@ -41,8 +41,23 @@ def test_facade_rotate_takes_row_major_matrices(tmp_path):
 
 
 def test_driver_builds():
-    subprocess.run(["make", "-s", "-C", PKG, "bin/erq_test_search"], check=True)
+    subprocess.run(["make", "-s", "-C", PKG, "bin/erq_test_search", "bin/erq_create_index"],
+                   check=True)
     assert os.access(DRIVER, os.X_OK)
+    assert os.access(os.path.join(PKG, "bin", "erq_create_index"), os.X_OK)
+
+
+def test_facade_build_calls_compile(tmp_path):
+    """src/create_index.cpp:45-49: IVF ivf(N, DIM, K, B); ivf.construct(data,
+    centroids, cids); ivf.save(file) - the same calls on the facade."""
+    src = tmp_path / "b.cpp"
+    src.write_text(
+        '#include "erq_ivf.hpp"\n'
+        'int main() { std::vector<float> data(64), centroids(64); std::vector<uint32_t> cids(1);\n'
+        '  erq::IVF ivf(1, 64, 1, 9); ivf.construct(data.data(), centroids.data(), cids.data());\n'
+        '  if (data[0] > 1.f) ivf.save("x.index"); return 0; }\n')
+    subprocess.run(["g++", "-std=c++17", "-fsyntax-only", "-I", os.path.join(REPO, "include"),
+                    str(src)], check=True)
 
 
 def _write_dataset(root, ds, bits):
