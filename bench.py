@@ -70,12 +70,13 @@ CONFIGS = {
     "zipf768-10M": dict(
         gen="gauss", n=10_000_000, dim=768, comps=16384, sigma=0.3, zipf=1.1, K=16384,
         bits_list=(3, 5, 9), nq=2000, k=100, seed=20245, recall_target=0.95,
-        qps_queries=100_000, train_queries=20_000, max_batch=4096, c5=True,
+        qps_queries=100_000, train_queries=10_000, max_batch=4096, c5=True,
         data="synthetic: seeded 16384-component Gaussian mixture (centres N(0, I), sigma 0.3) "
              "with Zipf(1.1) component weights, 10M base, d=768, clustered by erq_kmeans; "
              "recall on 2000 queries "
-             "(exact top-100 by a TF32 shortlist of 1024 re-ranked in float64), QPS on 100k "
-             "queries in batches of sizes drawn from 1..4096"),
+             "(exact top-100 by a TF32 shortlist of 1024 re-ranked in float64), QPS on up to "
+             "100k queries in batches of sizes drawn from 1..4096 (a prefix of at least 8,192 "
+             "at deep probes); probe models trained on 10k further queries"),
     # the small CPU-runnable case
     "gauss128-100k-4bit": dict(
         gen="gauss", n=100_000, dim=128, comps=256, sigma=0.3, zipf=None, K=1024,
@@ -275,9 +276,12 @@ LEARNED_MIN_PROB = 0.25
 
 # DRAM bytes (read + write) per algorithmic byte, from one-pass ncu captures of
 # dram__bytes_read.sum + dram__bytes_write.sum on this bench's headline
-# workload (profiles/dram_traffic_sphere1536_1M_8bit.md); a launch's traffic
-# is that ratio times its algorithmic bytes.  Empty for a kernel not captured.
-DRAM_PER_ALGORITHMIC_BYTE = {}
+# workload (profiles/dram_traffic_sphere1536_1M_8bit.md: the plain path's
+# scan_kernel, the learned plan's scan_batched_kernel, the refinement in
+# every mode); a launch's traffic is that ratio times its algorithmic bytes.
+# The ratios hold for the headline workload, not for other configurations.
+DRAM_PER_ALGORITHMIC_BYTE = {"scan_kernel": 0.0589, "scan_batched_kernel": 0.294,
+                             "refine_kernel": 0.421}
 
 
 def json_peak():
@@ -420,7 +424,10 @@ def learned_model(idx, d, cfg, plain_nprobe, train=None):
     rot = idx.rotate(train_q)
     del train_q
     labels = learned.make_labels(idx, rot, cfg["k"], bins)
-    agree = learned.exhaustive_agreement(idx, rot[:1000], cfg["k"], bins[-1])
+    # exhaustive probing reads the whole index per query: fewer queries for
+    # the 10M-vector index
+    n_agree = 1000 if cfg["n"] <= 2_000_000 else 200
+    agree = learned.exhaustive_agreement(idx, rot[:n_agree], cfg["k"], bins[-1])
     feats = learned.probe_features(idx, rot)
     del rot
     model = learned.ProbeModel.train(feats, labels, bins, epochs=8, batch=1024, lr=1e-3,
@@ -430,6 +437,7 @@ def learned_model(idx, d, cfg, plain_nprobe, train=None):
             "labels": f"smallest depth whose top-{cfg['k']} set equals that at the deepest "
                       f"bin ({bins[-1]} probes)",
             "deepest_bin_equals_exhaustive": round(agree, 4),
+            "exhaustive_sample": n_agree,
             "final_loss": round(model.final_loss, 4), "train_s": round(time.time() - t0, 1)}
     model.save(path)
     json.dump(meta, open(path + ".json", "w"))
@@ -655,6 +663,8 @@ def run_ours(args, cfg, name):
     # algorithmic bytes per step of the two HBM-side kernels: scan = the
     # probed clusters' code blocks (4D + 128 B per block), refine = the exact
     # candidates' EX-code rows + xipnorm + id (D*EX/8 + 8 B each)
+    headline = name == DEFAULT_CONFIG and not args.queries and not args.nprobe
+
     def mode_rooflines(m):
         md = modes[m]
         names = {"scan": "scan_kernel" if m == "plain" else "scan_batched_kernel",
@@ -667,7 +677,8 @@ def run_ours(args, cfg, name):
             achieved = step_bytes * args.steps / n_launch / (tot_ms / n_launch / 1e3) / 1e9
             res[kn] = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
                        "unit": "GB/s", "frac": round(achieved / peak, 4),
-                       "traffic": traffic_per_launch(names[kn], step_bytes, n_launch / args.steps),
+                       "traffic": (traffic_per_launch(names[kn], step_bytes, n_launch / args.steps)
+                                   if headline else None),
                        "kernel": names[kn], "ms_per_step": round(tot_ms / args.steps, 4),
                        "bytes_per_step": int(step_bytes),
                        "peak_source": f"{peak_src} hbm_gbs (copy)"}
@@ -963,36 +974,52 @@ def run_c5(args, cfg, name):
         res = {"build_s": round(build_s, 1), "plain": [], "learned": []}
         ids_d = torch.empty((cfg["max_batch"], k), dtype=torch.int32, device="cuda")
 
-        def qps_of(plan):
+        def qps_of(plan, depth):
+            """QPS over the uneven batch sequence; deep probes take a prefix
+            of it (at least 8,192 queries) so one point stays under a minute."""
             st = torch.cuda.current_stream()
+            budget = max(8192, int(cfg["qps_queries"] * min(1.0, 32.0 / max(depth, 1.0))))
+            seq, tot = [], 0
+            for b in sizes:
+                if tot >= budget:
+                    break
+                seq.append(b)
+                tot += b
             o = 0
-            for b in sizes[:8]:  # warm-up and graph capture of some sizes
+            for b in seq[:8]:  # warm-up and graph capture of some sizes
                 plan.search_buffers(qd[:b], ids_d[:b], stream=st)
             torch.cuda.synchronize()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(st)
-            for b in sizes:
+            for b in seq:
                 plan.search_buffers(qd[o:o + b], ids_d[:b], stream=st)
                 o += b
             e1.record(st)
             torch.cuda.synchronize()
-            return cfg["qps_queries"] / (e0.elapsed_time(e1) / 1e3)
+            return tot / (e0.elapsed_time(e1) / 1e3), tot
 
         chosen = None
+        prev = -1.0
         for nprobe in (1, 2, 4, 8, 16, 32, 64, 128, 256, 512, 1024):
+            if nprobe > cfg["K"]:
+                break
             r_ids, _ = idx.search_raw(q_eval, k, nprobe, with_dists=False)
             r100 = metrics.recall_at_k(r_ids, gt, k)
             r10 = metrics.recall_at_k(r_ids[:, :10], gt[:, :10], 10)
             plan = Plan(idx, max_batch=cfg["max_batch"], k=k, nprobe=nprobe, raw=True)
-            qps = qps_of(plan)
+            qps, nqps = qps_of(plan, nprobe)
             plan.free()
             res["plain"].append({"nprobe": nprobe, "recall@10": round(r10, 4),
-                                 "recall@100": round(r100, 4), "qps": round(qps, 1)})
+                                 "recall@100": round(r100, 4), "qps": round(qps, 1),
+                                 "qps_queries": nqps})
             log(f"c5 {bits}-bit nprobe {nprobe}: {res['plain'][-1]}")
             if chosen is None and r100 >= cfg["recall_target"]:
                 chosen = nprobe
-            if r100 > 0.995:
+            # stop once recall saturates: the estimates' own error (the code
+            # width) caps it below 1 at few bits
+            if r100 > 0.995 or r100 - prev < 0.002:
                 break
+            prev = r100
         if chosen is not None:
             cfg_l = dict(cfg, bits=bits)
             model, meta = learned_model(idx, work, cfg_l, chosen, train=q_train)
@@ -1002,11 +1029,11 @@ def run_c5(args, cfg, name):
                 plan_l.set_learned(conf, LEARNED_MIN_PROB)
                 ids_l, _, used = learned.search_learned(idx, model, idx.rotate(q_eval), k, chosen,
                                                         conf, LEARNED_MIN_PROB)
-                qps = qps_of(plan_l)
+                qps, nqps = qps_of(plan_l, float(used.mean()))
                 res["learned"].append({"confidence": conf, "mean_nprobe": round(float(used.mean()), 1),
                                        "recall@10": round(metrics.recall_at_k(ids_l[:, :10], gt[:, :10], 10), 4),
                                        "recall@100": round(metrics.recall_at_k(ids_l, gt, k), 4),
-                                       "qps": round(qps, 1)})
+                                       "qps": round(qps, 1), "qps_queries": nqps})
                 log(f"c5 {bits}-bit learned {res['learned'][-1]}")
             plan_l.free()
             model.free()

@@ -53,9 +53,6 @@ ERQ_API erq_status erq_debug_probe_model_grads(const erq_probe_model* model, con
 ERQ_API erq_status erq_debug_probe_model_params(const erq_probe_model* model, float* params,
                                                 float* mean, float* stdv, uint32_t* bin_nprobe);
 
-/* C[M][N] = A[M][Kd] * B[N][Kd]^T on the tcgen05 GEMM of the search (BF16
- * operands given as raw 16-bit patterns, FP32 result), host buffers; Kd a
- * multiple of 64.  ERQ_ERR_TIMEOUT if one of its bounded waits ran out. */
 /* Polls each pipeline wait of the tcgen05 GEMM makes before it gives up
  * (0 restores the default of 2^26).  A small value makes the waits run out, so
  * a test can check that the GEMM then reports ERQ_ERR_TIMEOUT and leaves the
@@ -63,6 +60,9 @@ ERQ_API erq_status erq_debug_probe_model_params(const erq_probe_model* model, fl
  * MMAs finishing) always keep the default.  Process-wide. */
 ERQ_API erq_status erq_debug_set_gemm_wait_limit(uint32_t polls);
 
+/* C[M][N] = A[M][Kd] * B[N][Kd]^T on the tcgen05 GEMM of the search (BF16
+ * operands given as raw 16-bit patterns, FP32 result), host buffers; Kd a
+ * multiple of 64.  ERQ_ERR_TIMEOUT if one of its bounded waits ran out. */
 ERQ_API erq_status erq_debug_gemm_bf16(const uint16_t* A, const uint16_t* B, uint64_t M, uint64_t N,
                                        uint64_t Kd, float* C, int device);
 
