@@ -81,9 +81,8 @@ __device__ __forceinline__ void ip_step(float2 acc[2], const float4& u, uint32_t
 // quad, in the reference's order (IP*_fxu* in inc/utils/space.hpp): the 16
 // accumulators acc[l] take the dims l, l+16, l+32, ... in turn; lane r holds
 // acc[4r..4r+3].  Rows are in the lane-interleaved layout of layout.cuh;
-// each lane streams its own uint4s one ahead (a loop unrolled by 3, so the
-// compiler renames the buffers instead of copying them, then the last pass,
-// which fetches nothing).  uq4 = unit_q as float4.
+// each lane streams its own uint4s one ahead (a loop unrolled by 3, then the
+// last pass, which fetches nothing).  uq4 = unit_q as float4.
 // Returns the sums (the reduce tree: acc[l] + acc[l+8], then + 4, then
 // (0 + 2) + (1 + 3)) in every lane of the quad.
 template <int SB, int NC>
@@ -95,10 +94,15 @@ __device__ __forceinline__ void ex_ip_quad(const float4* __restrict__ uq4, const
     float2 acc[NC][2];
 #pragma unroll
     for (int c = 0; c < NC; ++c) acc[c][0] = acc[c][1] = make_float2(0.f, 0.f);
-    const uint4* rows[2] = {row0 + r, row1 + r};
+    // running pointers: each pass advances them by a constant, so the loads
+    // of a pass take immediate offsets
+    const uint4* rp[NC];
+    rp[0] = row0 + r;
+    if (NC > 1) rp[NC - 1] = row1 + r;
+    const float4* qp = uq4 + r;
     uint4 cur[NC];
 #pragma unroll
-    for (int c = 0; c < NC; ++c) cur[c] = __ldg(rows[c]);
+    for (int c = 0; c < NC; ++c) cur[c] = __ldg(rp[c]);
     const int Uf = steps / SPU;      // uint4s whose steps are all real
     const int Upf = min(Uf, U - 1);  // passes that fetch the next uint4
     int u = 0;
@@ -106,26 +110,31 @@ __device__ __forceinline__ void ex_ip_quad(const float4* __restrict__ uq4, const
     for (; u < Upf; ++u) {
         uint4 nn[NC];
 #pragma unroll
-        for (int c = 0; c < NC; ++c) nn[c] = __ldg(rows[c] + 4 * (u + 1));
+        for (int c = 0; c < NC; ++c) {
+            rp[c] += 4;
+            nn[c] = __ldg(rp[c]);
+        }
 #pragma unroll
         for (int t = 0; t < SPU; ++t) {
-            const float4 q = uq4[4 * (u * SPU + t) + r];
+            const float4 q = qp[4 * t];
 #pragma unroll
             for (int c = 0; c < NC; ++c) ip_step(acc[c], q, step_word<SB>(cur[c], t));
         }
+        qp += 4 * SPU;
 #pragma unroll
         for (int c = 0; c < NC; ++c) cur[c] = nn[c];
     }
     for (; u < Uf; ++u) {  // the last pass: nothing left to fetch
 #pragma unroll
         for (int t = 0; t < SPU; ++t) {
-            const float4 q = uq4[4 * (u * SPU + t) + r];
+            const float4 q = qp[4 * t];
 #pragma unroll
             for (int c = 0; c < NC; ++c) ip_step(acc[c], q, step_word<SB>(cur[c], t));
         }
+        qp += 4 * SPU;
     }
     for (int t = 0; t < steps - Uf * SPU; ++t) {  // a partly filled last uint4
-        const float4 q = uq4[4 * (Uf * SPU + t) + r];
+        const float4 q = qp[4 * t];
 #pragma unroll
         for (int c = 0; c < NC; ++c) ip_step(acc[c], q, step_word<SB>(cur[c], t));
     }
