@@ -539,6 +539,8 @@ erq_status configure_kernels(int D, int K, int k) {
                                                         K <= kProbeStageKeys ? K : 0)));
     ERQ_CUDA(cudaFuncSetAttribute(probe_exact_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)probe_exact_smem_bytes(D, std::min(kp2, kProbeSortSmemKeys))));
+    ERQ_CUDA(cudaFuncSetAttribute(probe_warp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)(kProbeWarpWarps * probe_warp_smem_per_warp(D))));
     ERQ_CUDA(cudaFuncSetAttribute(scan_lowacc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)low_scan_smem_bytes(D)));
     {
@@ -912,9 +914,16 @@ erq_status launch_probe_tc(const erq_index* idx, const Batch& b, uint64_t nprobe
         a.sort_cap = b.sort_cap;
     }
     {
+        // a warp per query when the candidate list fits its registers
+        const int msel = near_d ? std::max(a.M, kProbeFeatRank) : a.M;
+        const bool warp_form = !a.sort_global && K > kProbeWarpCap && msel < kProbeWarpCap;
         LaunchTimer t(kProbe, st);
-        probe_kernel<<<(unsigned)b.nq, kProbeThreads,
-                       probe_smem_bytes(D, a.sort_global ? 0 : a.Spow2, a.stage_keys ? K : 0), st>>>(a);
+        if (warp_form)
+            probe_warp_kernel<<<(unsigned)div_up(b.nq, kProbeWarpWarps), kProbeWarpWarps * 32,
+                                kProbeWarpWarps * probe_warp_smem_per_warp(D), st>>>(a);
+        else
+            probe_kernel<<<(unsigned)b.nq, kProbeThreads,
+                           probe_smem_bytes(D, a.sort_global ? 0 : a.Spow2, a.stage_keys ? K : 0), st>>>(a);
         t.finish();
         ERQ_CUDA(cudaGetLastError());
     }

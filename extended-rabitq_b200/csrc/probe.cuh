@@ -362,6 +362,249 @@ __global__ void __launch_bounds__(kProbeThreads) probe_kernel(ProbeArgs a) {
     if (misc[3] && warp == 0) probe_outputs(a, q, sk, lane);
 }
 
+// ---------------------------------------------------------------------------
+// Warp-per-query form of probe_kernel for the common case (the Msel
+// candidates fit kProbeWarpCap): the same four steps with the same results,
+// each query on one warp of a block of kProbeWarpWarps, no block barrier.
+// Step 1 reads the estimate row from global memory on every pass instead of
+// staging it: one pass for the smallest and largest order key, then radix
+// passes whose first digit is the 8 bits below the highest bit those two
+// differ in (the bits above are common to every key), until the digit's
+// bucket holding rank Msel + 1 ends at most kProbeWarpCap keys from the
+// bottom - its end is then the cut A (every key outside the list is at or
+// above it, and the list holds the Msel smallest) - or the last digit gives
+// the (Msel + 1)-th key itself.  Steps 2-4 as probe_kernel, with a half-warp
+// per exact distance.
+constexpr int kProbeWarpWarps = 8;
+constexpr int kProbeWarpCap = 128;  // list capacity: four sort keys per lane
+
+// Shared memory of one warp: q[D] in chain order | hist[256] | list u64 [cap] | misc
+__host__ __device__ constexpr size_t probe_warp_smem_per_warp(int D) {
+    return (size_t)D * 4 + 256 * 4 + (size_t)kProbeWarpCap * 8 + 32;
+}
+
+// Ascending bitonic sort of 32 * R keys, element j * 32 + lane in v[j].
+template <int R>
+__device__ __forceinline__ void warp_sort_regs(uint64_t (&v)[R], int lane) {
+    constexpr int N = 32 * R;
+#pragma unroll
+    for (int size = 2; size <= N; size <<= 1) {
+#pragma unroll
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            if (stride >= 32) {
+#pragma unroll
+                for (int j = 0; j < R; ++j) {
+                    const int pj = j ^ (stride >> 5);
+                    if (pj > j) {
+                        const bool up = ((j * 32 + lane) & size) == 0;
+                        const uint64_t x = v[j], y = v[pj];
+                        if ((x > y) == up) {
+                            v[j] = y;
+                            v[pj] = x;
+                        }
+                    }
+                }
+            } else {
+                const bool low = (lane & stride) == 0;
+#pragma unroll
+                for (int j = 0; j < R; ++j) {
+                    const uint64_t o = __shfl_xor_sync(0xffffffffu, v[j], stride);
+                    const bool up = ((j * 32 + lane) & size) == 0;
+                    v[j] = (low == up) ? (v[j] < o ? v[j] : o) : (v[j] < o ? o : v[j]);
+                }
+            }
+        }
+    }
+}
+
+// Ascending sort of keys[0..n), n <= kProbeWarpCap, by one warp.
+__device__ __forceinline__ void warp_sort_list(uint64_t* keys, int n, int lane) {
+    if (n <= 64) {
+        warp_sort64(keys, n, lane);
+        __syncwarp();
+        return;
+    }
+    uint64_t v[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) v[j] = j * 32 + lane < n ? keys[j * 32 + lane] : ~0ull;
+    warp_sort_regs<4>(v, lane);
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+        if (j * 32 + lane < n) keys[j * 32 + lane] = v[j];
+    __syncwarp();
+}
+
+__global__ void __launch_bounds__(kProbeWarpWarps * 32) probe_warp_kernel(ProbeArgs a) {
+    extern __shared__ __align__(16) uint8_t smem_raw[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int q = blockIdx.x * kProbeWarpWarps + warp;
+    if (q >= a.nq) return;  // whole warp; nothing below waits across warps
+    const int K = a.K, D = a.D;
+    uint8_t* base = smem_raw + (size_t)warp * probe_warp_smem_per_warp(D);
+    float* qs = reinterpret_cast<float*>(base);
+    uint32_t* hist = reinterpret_cast<uint32_t*>(qs + D);
+    uint64_t* sk = reinterpret_cast<uint64_t*>(hist + 256);
+    for (int i = lane; i < D; i += 32) qs[chain_pos(i)] = a.qrot[(size_t)q * D + i];
+    const float* aq = a.approx + (size_t)q * K;
+    const uint32_t lt = (1u << lane) - 1u;
+    // f(order key) for this lane's share of the row (128-bit loads when K % 4 == 0)
+    auto each_key = [&](auto&& f) {
+        if ((K & 3) == 0) {
+            const float4* aq4 = reinterpret_cast<const float4*>(aq);
+            for (int c4 = lane; c4 < (K >> 2); c4 += 32) {
+                const float4 v = __ldg(aq4 + c4);
+                f(order_key(v.x));
+                f(order_key(v.y));
+                f(order_key(v.z));
+                f(order_key(v.w));
+            }
+        } else {
+            for (int c = lane; c < K; c += 32) f(order_key(__ldg(aq + c)));
+        }
+    };
+
+    // 1. the smallest and largest order key
+    uint32_t lo = 0xffffffffu, hi = 0u;
+    each_key([&](uint32_t kk) {
+        lo = min(lo, kk);
+        hi = max(hi, kk);
+    });
+    lo = __reduce_min_sync(0xffffffffu, lo);
+    hi = __reduce_max_sync(0xffffffffu, hi);
+    const int Msel = a.near_d ? max(a.M, kProbeFeatRank) : a.M;
+    uint64_t kstar = (uint64_t)lo;  // all keys equal: nothing lies below the (Msel+1)-th
+    if (lo != hi) {
+        const int hb = 31 - __clz((int)(lo ^ hi));
+        int s = max(hb - 7, 0), w = hb - s + 1;  // the digit: bits [s, s + w)
+        uint64_t prefix = (uint64_t)lo >> (s + w) << (s + w);
+        uint32_t below = 0;  // keys under the current range
+        int rank = Msel + 1;
+        for (;;) {
+            for (int i = lane; i < 256; i += 32) hist[i] = 0;
+            __syncwarp();
+            const uint32_t dmask = (1u << w) - 1u;
+            const uint64_t want = prefix >> (s + w);
+            each_key([&](uint32_t kk) {
+                if (((uint64_t)kk >> (s + w)) == want) atomicAdd(&hist[(kk >> s) & dmask], 1u);
+            });
+            __syncwarp();
+            uint32_t h[8], sum = 0;
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                h[i] = hist[8 * lane + i];
+                sum += h[i];
+            }
+            uint32_t incl = sum;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += v;
+            }
+            const uint32_t excl = incl - sum;
+            const bool mine = excl < (uint32_t)rank && incl >= (uint32_t)rank;
+            // in the lane that holds it: the bin of rank, the keys below it, its count
+            int d = 7;
+            uint32_t run = excl, hdv = 0, acc = excl;
+            bool found = false;
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                if (!found && acc + h[i] >= (uint32_t)rank) {
+                    found = true;
+                    d = i;
+                    run = acc;
+                    hdv = h[i];
+                }
+                acc += h[i];
+            }
+            const int src = __ffs(__ballot_sync(0xffffffffu, mine)) - 1;
+            const int dg = __shfl_sync(0xffffffffu, 8 * lane + d, src);
+            const uint32_t before = __shfl_sync(0xffffffffu, run, src);
+            const uint32_t hd = __shfl_sync(0xffffffffu, hdv, src);
+            const uint64_t b_lo = prefix | ((uint64_t)dg << s);
+            if (s == 0) {  // the (Msel+1)-th key itself
+                kstar = b_lo;
+                break;
+            }
+            if (below + before + hd <= (uint32_t)kProbeWarpCap) {  // the bucket's end
+                kstar = b_lo + (1ull << s);
+                break;
+            }
+            below += before;
+            rank -= (int)before;
+            prefix = b_lo;
+            const int s2 = max(s - 8, 0);
+            w = s - s2;
+            s = s2;
+        }
+    }
+    // the list: every centroid whose key is below kstar, keyed by (estimate, id)
+    int ns = 0;
+    for (int c0 = 0; c0 < K; c0 += 32) {
+        const int c = c0 + lane;
+        const uint32_t kk = c < K ? order_key(__ldg(aq + c)) : 0xffffffffu;
+        const bool in = c < K && (uint64_t)kk < kstar;
+        const uint32_t m = __ballot_sync(0xffffffffu, in);
+        if (in) sk[ns + __popc(m & lt)] = ((uint64_t)kk << 32) | (uint64_t)c;
+        ns += __popc(m);
+    }
+    __syncwarp();
+    warp_sort_list(sk, ns, lane);
+    if (a.near_d) {
+        // the 64 smallest estimates, in order, are the distance features
+        for (int j = lane; j < kProbeFeatRank; j += 32)
+            a.near_d[(size_t)q * kProbeFeatRank + j] =
+                ns > 0 ? order_key_value((uint32_t)(sk[j < ns ? j : ns - 1] >> 32)) : 0.f;
+    }
+    // 2-3. exact distances of list positions [lo, hi), a half-warp each
+    const int n = min(a.check_rank, ns);
+    const float eps = a.eps_rel * (a.qn[q] + a.cn_max);
+    const int hw = lane >> 4, l = lane & 15;
+    uint32_t e_max_bits = 0u;  // the largest of the first n, as unsigned float bits
+    auto exact_range = [&](int p0, int p1) {
+        for (int i0 = p0; i0 < p1; i0 += 2) {
+            const int i = i0 + hw < p1 ? i0 + hw : i0;  // a half-warp past the end repeats
+            const uint32_t c = (uint32_t)(sk[i] & 0xffffffffu);
+            const float e = l2sqr16_chain(reinterpret_cast<const float4*>(qs),
+                                          reinterpret_cast<const float4*>(a.centroids + (size_t)c * D), D, l);
+            const float e0 = __shfl_sync(0xffffffffu, e, 0), e1 = __shfl_sync(0xffffffffu, e, 16);
+            if (lane == 0) sk[i0] = dist_key(e0, (uint32_t)(sk[i0] & 0xffffffffu));
+            if (lane == 16 && i0 + 1 < p1) sk[i0 + 1] = dist_key(e1, c);
+            e_max_bits = max(e_max_bits, __float_as_uint(e0));
+            if (i0 + 1 < p1) e_max_bits = max(e_max_bits, __float_as_uint(e1));
+            __syncwarp();
+        }
+    };
+    __syncwarp();
+    exact_range(0, n);
+    const float e_max = __uint_as_float(e_max_bits);
+    int P = ns;
+    for (int i0 = n; i0 < ns; i0 += 32) {
+        const int i = i0 + lane;
+        const bool qual = i < ns && order_key_value((uint32_t)(sk[i] >> 32)) - eps > e_max;
+        const uint32_t m = __ballot_sync(0xffffffffu, qual);
+        if (m) {
+            P = i0 + __ffs(m) - 1;
+            break;
+        }
+    }
+    const bool truncated = kstar < (1ull << 32);
+    const bool proven = P < ns || !truncated || (order_key_value((uint32_t)kstar) - eps > e_max);
+    exact_range(n, P);
+    warp_sort_list(sk, P, lane);
+    // a query whose cut is not proven goes to probe_exact_kernel
+    bool ok = ns >= a.check_rank;
+    if (ok && !proven) {
+        const float e_n = __uint_as_float((uint32_t)(sk[a.check_rank - 1] >> 32));
+        const float A = order_key_value((uint32_t)kstar);
+        ok = (A - eps > e_n) && (e_n == e_n);
+    }
+    if (lane == 0) {
+        a.fallback_flag[q] = ok ? 0u : 1u;
+        if (!ok && a.fallbacks) atomicAdd(a.fallbacks, 1u);
+    }
+    if (ok) probe_outputs(a, q, sk, lane);
+}
+
 // The exact nprobe nearest centroids of a query, by (distance, id), from all
 // K exact distances - for the queries whose cut probe_kernel could not prove
 // (fallback_flag set; `compute`: the exact L2Sqr16 values are computed here
