@@ -306,10 +306,13 @@ __global__ void __launch_bounds__(kProbeThreads) probe_kernel(ProbeArgs a) {
     const bool truncated = !select_all;  // A = value of kstar bounds the rest
     sort_prefix(sk, ns);
     if (a.near_d) {
-        // the 64 smallest estimates, in order, are the distance features
+        // the 64 smallest estimates, in order, are the distance features;
+        // ranks the list misses are ties at the cut, the (Msel+1)-th estimate
+        const float fill = truncated ? order_key_value(kstar)
+                                     : ns > 0 ? order_key_value((uint32_t)(sk[ns - 1] >> 32)) : 0.f;
         for (int j = tid; j < kProbeFeatRank; j += blockDim.x)
             a.near_d[(size_t)q * kProbeFeatRank + j] =
-                ns > 0 ? order_key_value((uint32_t)(sk[j < ns ? j : ns - 1] >> 32)) : 0.f;
+                j < ns ? order_key_value((uint32_t)(sk[j] >> 32)) : fill;
     }
     const int n = min(a.check_rank, ns);
     const float eps = a.eps_rel * (a.qn[q] + a.cn_max);
@@ -550,10 +553,13 @@ __global__ void __launch_bounds__(kProbeWarpWarps * 32) probe_warp_kernel(ProbeA
     __syncwarp();
     warp_sort_list(sk, ns, lane);
     if (a.near_d) {
-        // the 64 smallest estimates, in order, are the distance features
+        // the 64 smallest estimates, in order, are the distance features;
+        // ranks the list misses are ties at the cut, the (Msel+1)-th estimate
+        // (a list cut at a bucket's end holds more than 64)
+        const float fill = order_key_value((uint32_t)kstar);
         for (int j = lane; j < kProbeFeatRank; j += 32)
             a.near_d[(size_t)q * kProbeFeatRank + j] =
-                ns > 0 ? order_key_value((uint32_t)(sk[j < ns ? j : ns - 1] >> 32)) : 0.f;
+                j < ns ? order_key_value((uint32_t)(sk[j] >> 32)) : fill;
     }
     // 2-3. exact distances of list positions [lo, hi), a half-warp each
     const int n = min(a.check_rank, ns);
