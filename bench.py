@@ -276,12 +276,14 @@ LEARNED_MIN_PROB = 0.25
 
 # DRAM bytes (read + write) per algorithmic byte, from one-pass ncu captures of
 # dram__bytes_read.sum + dram__bytes_write.sum on this bench's headline
-# workload (profiles/dram_traffic_sphere1536_1M_8bit.md: the plain path's
-# scan_kernel, the learned plan's scan_batched_kernel, the refinement in
-# every mode); a launch's traffic is that ratio times its algorithmic bytes.
-# The ratios hold for the headline workload, not for other configurations.
-DRAM_PER_ALGORITHMIC_BYTE = {"scan_kernel": 0.0589, "scan_batched_kernel": 0.294,
-                             "refine_kernel": 0.421}
+# workload, per mode and kernel (profiles/dram_traffic_sphere1536_1M_8bit.md);
+# a launch's traffic is that ratio times its algorithmic bytes.  The ratios
+# hold for the headline workload, not for other configurations.
+DRAM_PER_ALGORITHMIC_BYTE = {
+    ("plain", "scan_kernel"): 0.0588, ("plain", "refine_kernel"): 0.418,
+    ("batched", "scan_batched_kernel"): 0.0579, ("batched", "refine_kernel"): 0.418,
+    ("learned", "scan_batched_kernel"): 0.297, ("learned", "refine_kernel"): 0.414,
+}
 
 
 def json_peak():
@@ -292,8 +294,8 @@ def json_peak():
         return None
 
 
-def traffic_per_launch(kernel, step_bytes, launches_per_step):
-    r = DRAM_PER_ALGORITHMIC_BYTE.get(kernel)
+def traffic_per_launch(mode, kernel, step_bytes, launches_per_step):
+    r = DRAM_PER_ALGORITHMIC_BYTE.get((mode, kernel))
     if r is None or not launches_per_step:
         return None
     return int(r * step_bytes / launches_per_step)
@@ -677,7 +679,7 @@ def run_ours(args, cfg, name):
             achieved = step_bytes * args.steps / n_launch / (tot_ms / n_launch / 1e3) / 1e9
             res[kn] = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
                        "unit": "GB/s", "frac": round(achieved / peak, 4),
-                       "traffic": (traffic_per_launch(names[kn], step_bytes, n_launch / args.steps)
+                       "traffic": (traffic_per_launch(m, names[kn], step_bytes, n_launch / args.steps)
                                    if headline else None),
                        "kernel": names[kn], "ms_per_step": round(tot_ms / args.steps, 4),
                        "bytes_per_step": int(step_bytes),
@@ -773,10 +775,11 @@ def _timed_calls(fn, calls, warmup):
 
 def secondary_small(args):
     """100k x 128, 4-bit, nprobe 16/32/64: one query per call (p50/p99 and
-    QPS) and the whole 1,000-query batch per call, with recall@100."""
+    QPS; through erq_search_raw and through a plan's replayed graph) and the
+    whole 1,000-query batch per call, with recall@100."""
     import torch
 
-    from erq_b200 import IVF, metrics
+    from erq_b200 import IVF, Plan, metrics
 
     name = "gauss128-100k-4bit"
     cfg = CONFIGS[name]
@@ -800,12 +803,25 @@ def secondary_small(args):
             idx.search_raw(qd[i:i + 1], k, nprobe, ids=ids[:1], dists=dist[:1], stream=st)
 
         one = _timed_calls(one_query, 300, 10)
+        # the same through a plan for batches of one (its CUDA graph replayed)
+        plan = Plan(idx, max_batch=1, k=k, nprobe=nprobe, raw=True)
+
+        def one_query_plan():
+            i = next(calls) % query.shape[0]
+            plan.search_buffers(qd[i:i + 1], ids[:1], dist[:1], stream=st)
+
+        one_p = _timed_calls(one_query_plan, 300, 10)
+        plan.free()
         batch = _timed_calls(lambda: idx.search_raw(qd, k, nprobe, ids=ids, dists=dist, stream=st),
                              20, 3)
         out[str(nprobe)] = {"recall@100": round(rec, 5),
                             "one_query_per_call": {"qps": round(1e3 / one.mean(), 1),
                                                    "p50_ms": round(float(np.percentile(one, 50)), 4),
                                                    "p99_ms": round(float(np.percentile(one, 99)), 4)},
+                            "one_query_per_call_plan": {
+                                "qps": round(1e3 / one_p.mean(), 1),
+                                "p50_ms": round(float(np.percentile(one_p, 50)), 4),
+                                "p99_ms": round(float(np.percentile(one_p, 99)), 4)},
                             "batch_1000_qps": round(1e3 * query.shape[0] / batch.mean(), 1)}
     idx.free()
     return {"workload": f"{name}: 100000x128, K=1024, 4-bit, top-100, one query per call and "
