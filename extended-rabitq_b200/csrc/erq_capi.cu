@@ -687,7 +687,10 @@ erq_status gemm_tc(const __nv_bfloat16* A, const __nv_bfloat16* B, float* C, int
             configured[dev] = true;
         }
     }
-    dim3 grid((unsigned)div_up(N, kTcBN), (unsigned)div_up(M, kTcBM));
+    // persistent: one CTA per SM (the ring leaves room for one), at most one per tile
+    const uint64_t tiles = (uint64_t)div_up(N, kTcBN) * (uint64_t)div_up(M, kTcBM);
+    if (tiles > 0x7fffffffull) return fail(ERQ_ERR_INVALID_ARGUMENT, "GEMM of %llu tiles", (unsigned long long)tiles);
+    const unsigned grid = (unsigned)std::min<uint64_t>(tiles, (uint64_t)device_sms());
     LaunchTimer t(kernel_id, st);
     gemm_tc_kernel<<<grid, kTcThreads, gemm_tc_smem_bytes(), st>>>(ta, tb, C, M, N, Kd, epi, status,
                                                                     g_tc_wait_limit.load());
