@@ -539,8 +539,10 @@ erq_status configure_kernels(int D, int K, int k) {
                                                         K <= kProbeStageKeys ? K : 0)));
     ERQ_CUDA(cudaFuncSetAttribute(probe_exact_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)probe_exact_smem_bytes(D, std::min(kp2, kProbeSortSmemKeys))));
-    ERQ_CUDA(cudaFuncSetAttribute(probe_warp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)(kProbeWarpWarps * probe_warp_smem_per_warp(D))));
+    for (const void* f : {(const void*)probe_warp_kernel<0>, (const void*)probe_warp_kernel<1>,
+                          (const void*)probe_warp_kernel<2>})
+        ERQ_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)(kProbeWarpWarps * probe_warp_smem_per_warp(D))));
     ERQ_CUDA(cudaFuncSetAttribute(scan_lowacc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)low_scan_smem_bytes(D)));
     {
@@ -724,7 +726,20 @@ struct Batch {
     uint32_t* fb_flag = nullptr;      // [nq] queries whose probe needs all K exact distances
     uint64_t* sortbuf = nullptr;      // [nq][sort_cap] probe sort keys too many for shared memory
     uint64_t sort_cap = 0;
+    // a split probe's sorted lists (launch_probe_tc / launch_probe_finish);
+    // allocated by the learned paths only
+    uint64_t* plist = nullptr;        // [nq][kProbeWarpCap]
+    uint32_t* plist_n = nullptr;      // [nq]
+    uint64_t* plist_cut = nullptr;    // [nq]
 };
+
+template <class Alloc>
+erq_status alloc_probe_lists(Alloc& s, uint64_t nq, Batch& b) {
+    ERQ_TRY(s.alloc(&b.plist, nq * kProbeWarpCap));
+    ERQ_TRY(s.alloc(&b.plist_n, nq));
+    ERQ_TRY(s.alloc(&b.plist_cut, nq));
+    return ERQ_OK;
+}
 
 int probe_candidates(uint64_t nprobe);
 
@@ -864,23 +879,12 @@ unsigned long long* refine_stats_counter() {
 
 // Coarse probe on tensor cores: split the rotated queries, estimate all
 // distances with the split-BF16 GEMM, then the exact probe kernel.
-erq_status launch_probe_tc(const erq_index* idx, const Batch& b, uint64_t nprobe, cudaStream_t st,
-                           float* near_d = nullptr) {
+// The arguments of the probe kernels for a batch (near_d: the features' 64
+// smallest estimates are wanted).
+erq_status probe_args(const erq_index* idx, const Batch& b, uint64_t nprobe, float* near_d,
+                      ProbeArgs& a, int& npow2) {
     const int D = (int)idx->D, K = (int)idx->K;
-    {
-        LaunchTimer t(kSplit, st);
-        split_rows_kernel<<<(unsigned)b.nq, 256, 0, st>>>(b.qrot, (int)b.nq, D, D, true, b.qsplit,
-                                                          b.qn);
-        t.finish();
-        ERQ_CUDA(cudaGetLastError());
-    }
-    {
-        GemmEpilogue epi;
-        epi.row_norm = b.qn;
-        epi.col_norm = idx->cn;
-        ERQ_TRY(gemm_tc(b.qsplit, idx->c_split, b.dist, (int)b.nq, K, 3 * D, epi, kGemm, st));
-    }
-    ProbeArgs a{};
+    a = ProbeArgs{};
     a.approx = b.dist;
     a.qrot = b.qrot;
     a.centroids = idx->c_chain;
@@ -909,35 +913,99 @@ erq_status launch_probe_tc(const erq_index* idx, const Batch& b, uint64_t nprobe
     a.fallback_flag = b.fb_flag;
     a.stage_keys = K <= kProbeStageKeys ? 1 : 0;
     a.exact_rows = b.dist;
-    const int npow2 = next_pow2((int)std::min<uint64_t>(nprobe, (uint64_t)K));
+    a.list = b.plist;
+    a.list_n = b.plist_n;
+    a.list_cut = b.plist_cut;
+    npow2 = next_pow2((int)std::min<uint64_t>(nprobe, (uint64_t)K));
     if (a.Spow2 > kProbeSortSmemKeys || npow2 > kProbeSortSmemKeys) {
         if (!b.sortbuf || b.sort_cap < (uint64_t)std::max(a.Spow2, npow2))
             return fail(ERQ_ERR_INVALID_ARGUMENT, "probe batch without a large enough sort buffer");
         a.sort_global = b.sortbuf;
         a.sort_cap = b.sort_cap;
     }
+    return ERQ_OK;
+}
+
+// a warp per query when the candidate list fits its registers
+bool probe_warp_form(const ProbeArgs& a) {
+    const int msel = a.near_d ? std::max(a.M, kProbeFeatRank) : a.M;
+    return !a.sort_global && a.K > kProbeWarpCap && msel < kProbeWarpCap;
+}
+
+// The fallback of the probe kernels: all K exact distances for the queries
+// whose cut was not proven.
+erq_status launch_probe_exact(const Batch& b, const ProbeArgs& a, int npow2, cudaStream_t st) {
+    LaunchTimer t(kProbe, st);
+    probe_exact_kernel<<<(unsigned)b.nq, kProbeThreads,
+                         probe_exact_smem_bytes(a.D, a.sort_global ? 0 : npow2), st>>>(a, 1, npow2);
+    t.finish();
+    ERQ_CUDA(cudaGetLastError());
+    return ERQ_OK;
+}
+
+// The coarse probe of a batch: split + estimate GEMM + exact top nprobe.
+// With `split` (and the batch's probe lists), a probe that runs in the warp
+// form stops after the features and the sorted lists (*split set): the rest
+// follows in launch_probe_finish once each query's depth is known.
+erq_status launch_probe_tc(const erq_index* idx, const Batch& b, uint64_t nprobe, cudaStream_t st,
+                           float* near_d = nullptr, bool* split = nullptr) {
+    const int D = (int)idx->D, K = (int)idx->K;
+    if (split) *split = false;
     {
-        // a warp per query when the candidate list fits its registers
-        const int msel = near_d ? std::max(a.M, kProbeFeatRank) : a.M;
-        const bool warp_form = !a.sort_global && K > kProbeWarpCap && msel < kProbeWarpCap;
+        LaunchTimer t(kSplit, st);
+        split_rows_kernel<<<(unsigned)b.nq, 256, 0, st>>>(b.qrot, (int)b.nq, D, D, true, b.qsplit,
+                                                          b.qn);
+        t.finish();
+        ERQ_CUDA(cudaGetLastError());
+    }
+    {
+        GemmEpilogue epi;
+        epi.row_norm = b.qn;
+        epi.col_norm = idx->cn;
+        ERQ_TRY(gemm_tc(b.qsplit, idx->c_split, b.dist, (int)b.nq, K, 3 * D, epi, kGemm, st));
+    }
+    ProbeArgs a;
+    int npow2 = 0;
+    ERQ_TRY(probe_args(idx, b, nprobe, near_d, a, npow2));
+    const bool warp_form = probe_warp_form(a);
+    const bool first_of_two = warp_form && split && b.plist;
+    {
         LaunchTimer t(kProbe, st);
-        if (warp_form)
-            probe_warp_kernel<<<(unsigned)div_up(b.nq, kProbeWarpWarps), kProbeWarpWarps * 32,
-                                kProbeWarpWarps * probe_warp_smem_per_warp(D), st>>>(a);
+        const unsigned wgrid = (unsigned)div_up(b.nq, kProbeWarpWarps);
+        const size_t wsmem = kProbeWarpWarps * probe_warp_smem_per_warp(D);
+        if (first_of_two)
+            probe_warp_kernel<1><<<wgrid, kProbeWarpWarps * 32, wsmem, st>>>(a);
+        else if (warp_form)
+            probe_warp_kernel<0><<<wgrid, kProbeWarpWarps * 32, wsmem, st>>>(a);
         else
             probe_kernel<<<(unsigned)b.nq, kProbeThreads,
                            probe_smem_bytes(D, a.sort_global ? 0 : a.Spow2, a.stage_keys ? K : 0), st>>>(a);
         t.finish();
         ERQ_CUDA(cudaGetLastError());
     }
+    if (first_of_two) {
+        *split = true;
+        return ERQ_OK;
+    }
+    return launch_probe_exact(b, a, npow2, st);
+}
+
+// The second launch of a split probe: each query's exact distances up to the
+// depth q_check[q] it will scan (at most nprobe), from its sorted list.
+erq_status launch_probe_finish(const erq_index* idx, const Batch& b, uint64_t nprobe, cudaStream_t st,
+                               const int* q_check) {
+    ProbeArgs a;
+    int npow2 = 0;
+    ERQ_TRY(probe_args(idx, b, nprobe, nullptr, a, npow2));
+    a.q_check = q_check;
     {
         LaunchTimer t(kProbe, st);
-        probe_exact_kernel<<<(unsigned)b.nq, kProbeThreads,
-                             probe_exact_smem_bytes(D, a.sort_global ? 0 : npow2), st>>>(a, 1, npow2);
+        probe_warp_kernel<2><<<(unsigned)div_up(b.nq, kProbeWarpWarps), kProbeWarpWarps * 32,
+                               kProbeWarpWarps * probe_warp_smem_per_warp(a.D), st>>>(a);
         t.finish();
         ERQ_CUDA(cudaGetLastError());
     }
-    return ERQ_OK;
+    return launch_probe_exact(b, a, npow2, st);
 }
 
 erq_status launch_probe(const erq_index* idx, const Batch& b, uint64_t nprobe, cudaStream_t st) {
@@ -1466,8 +1534,8 @@ erq_status mlp_infer(const erq_probe_model* m, const float* feats, const MlpWork
 // With a model and xs, also its standardised first-layer input.
 erq_status features_device(const erq_index* idx, const Batch& b, uint64_t nprobe, float* near_d,
                            float* feats, cudaStream_t st, const erq_probe_model* m = nullptr,
-                           __nv_bfloat16* xs = nullptr) {
-    ERQ_TRY(launch_probe_tc(idx, b, nprobe, st, near_d));
+                           __nv_bfloat16* xs = nullptr, bool* split = nullptr) {
+    ERQ_TRY(launch_probe_tc(idx, b, nprobe, st, near_d, split));
     LaunchTimer t(kMlp, st);
     probe_features_kernel<<<(unsigned)b.nq, 128, 0, st>>>(
         b.qrot, (int)idx->D, b.qn, near_d, (int)b.nq, feats, m && xs ? m->mean : nullptr,
@@ -1969,12 +2037,14 @@ erq_status erq_probe_features(const erq_index* idx, const float* rotated_queries
     const uint64_t bq = batch_queries(idx, std::max<uint64_t>(nprobe, 1), nq);
     Batch b;
     ERQ_TRY(alloc_batch(s, idx, bq, nprobe, b));
+    ERQ_TRY(alloc_probe_lists(s, bq, b));
     float* near_d = nullptr;
     ERQ_TRY(s.alloc(&near_d, bq * kFeatDists));
     for (uint64_t q0 = 0; q0 < nq; q0 += bq) {
         b.nq = std::min(bq, nq - q0);
         b.qrot = q + q0 * idx->D;
-        ERQ_TRY(features_device(idx, b, nprobe, near_d, fout + q0 * kMlpIn, st));
+        bool split = false;  // the features need no probe list: a split probe stops there
+        ERQ_TRY(features_device(idx, b, nprobe, near_d, fout + q0 * kMlpIn, st, nullptr, nullptr, &split));
     }
     if (!f_dev) {
         ERQ_CUDA(cudaMemcpyAsync(features, fout, nq * kMlpIn * 4, cudaMemcpyDeviceToHost, st));
@@ -2265,6 +2335,7 @@ static erq_status search_learned_entry(const erq_index* idx, const erq_probe_mod
     const uint64_t bq = batch_queries(idx, nprobe_max, nq);
     Batch b;
     ERQ_TRY(alloc_batch(s, idx, bq, nprobe_max, b));
+    ERQ_TRY(alloc_probe_lists(s, bq, b));
     float *near_d = nullptr, *feats = nullptr;
     ERQ_TRY(s.alloc(&near_d, bq * kFeatDists));
     ERQ_TRY(s.alloc(&feats, bq * kMlpIn));
@@ -2274,7 +2345,8 @@ static erq_status search_learned_entry(const erq_index* idx, const erq_probe_mod
         b.nq = std::min(bq, nq - q0);
         b.qrot = q + q0 * idx->D;
         const int B = (int)b.nq;
-        ERQ_TRY(features_device(idx, b, nprobe_max, near_d, feats, st, m, wk.xs));
+        bool split = false;
+        ERQ_TRY(features_device(idx, b, nprobe_max, near_d, feats, st, m, wk.xs, &split));
         ERQ_TRY(mlp_infer(m, feats, wk, B, wk.probs, st, true));
         {
             LaunchTimer t(kMlp, st);
@@ -2284,6 +2356,8 @@ static erq_status search_learned_entry(const erq_index* idx, const erq_probe_mod
             t.finish();
         }
         ERQ_CUDA(cudaGetLastError());
+        // exact distances only as deep as each query's chosen depth
+        if (split) ERQ_TRY(launch_probe_finish(idx, b, nprobe_max, st, used + q0));
         erq_status oe;
         const bool ordered = launch_order(idx, b, nprobe_max, st, used + q0, &oe);
         ERQ_TRY(oe);
@@ -2975,7 +3049,8 @@ erq_status plan_pipeline(erq_plan* p, uint64_t nq, const erq_plan_tuning& t, cud
     if (p->model) {
         const erq_probe_model* m = p->model;
         const int B = (int)nq;
-        ERQ_TRY(features_device(idx, b, p->nprobe_run, p->near_d, p->feats, st, m, p->wk.xs));
+        bool split = false;
+        ERQ_TRY(features_device(idx, b, p->nprobe_run, p->near_d, p->feats, st, m, p->wk.xs, &split));
         ERQ_TRY(mlp_infer(m, p->feats, p->wk, B, p->wk.probs, st, true));
         {
             LaunchTimer lt(kMlp, st);
@@ -2985,6 +3060,8 @@ erq_status plan_pipeline(erq_plan* p, uint64_t nq, const erq_plan_tuning& t, cud
             lt.finish();
         }
         ERQ_CUDA(cudaGetLastError());
+        // exact distances only as deep as each query's chosen depth
+        if (split) ERQ_TRY(launch_probe_finish(idx, b, p->nprobe_run, st, p->used));
         qnp = p->used;
     } else {
         ERQ_TRY(launch_probe_tc(idx, b, p->nprobe_run, st));
@@ -3159,6 +3236,7 @@ erq_status erq_plan_create(const erq_index* idx, const erq_probe_model* model, u
         ERQ_TRY((scan_batched_configure<4, 8>(D, &p->per_sm[5])));
     }
     ERQ_TRY(alloc_batch(p->arena, idx, max_batch, p->nprobe_run, p->b));
+    if (model) ERQ_TRY(alloc_probe_lists(p->arena, max_batch, p->b));
     ERQ_TRY(p->arena.alloc(&p->qin, max_batch * (p->raw ? idx->DIM : idx->D)));
     ERQ_TRY(p->arena.alloc(&p->qrot, max_batch * idx->D));
     ERQ_TRY(p->arena.alloc(&p->ids, max_batch * k));

@@ -50,6 +50,14 @@ struct ProbeArgs {
     uint64_t sort_cap;        // keys per query in sort_global
     float* exact_rows;        // [nq][K]: probe_exact_kernel's exact distances (it may
                               // overwrite the estimates there)
+    // probe_warp_kernel in two launches (<1>, then <2>; <0>: one launch):
+    // <1> selects, sorts and writes the features, and keeps each query's
+    // sorted list here; <2> finishes from it with the per-query check rank
+    // q_check (the depth a probe model chose in between)
+    uint64_t* list;           // [nq][kProbeWarpCap]
+    uint32_t* list_n;         // [nq]
+    uint64_t* list_cut;       // [nq]
+    const int* q_check;       // [nq] (phase 2)
 };
 
 constexpr int kProbeThreads = 256;
@@ -437,6 +445,9 @@ __device__ __forceinline__ void warp_sort_list(uint64_t* keys, int n, int lane) 
     __syncwarp();
 }
 
+// PHASE 0: the whole probe; 1: through the features, keeping the sorted list;
+// 2: the rest from that list (ProbeArgs::phase documents the two launches).
+template <int PHASE>
 __global__ void __launch_bounds__(kProbeWarpWarps * 32) probe_warp_kernel(ProbeArgs a) {
     extern __shared__ __align__(16) uint8_t smem_raw[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -447,122 +458,140 @@ __global__ void __launch_bounds__(kProbeWarpWarps * 32) probe_warp_kernel(ProbeA
     float* qs = reinterpret_cast<float*>(base);
     uint32_t* hist = reinterpret_cast<uint32_t*>(qs + D);
     uint64_t* sk = reinterpret_cast<uint64_t*>(hist + 256);
-    for (int i = lane; i < D; i += 32) qs[chain_pos(i)] = a.qrot[(size_t)q * D + i];
+    if (PHASE != 1)
+        for (int i = lane; i < D; i += 32) qs[chain_pos(i)] = a.qrot[(size_t)q * D + i];
     const float* aq = a.approx + (size_t)q * K;
     const uint32_t lt = (1u << lane) - 1u;
-    // f(order key) for this lane's share of the row (128-bit loads when K % 4 == 0)
-    auto each_key = [&](auto&& f) {
-        if ((K & 3) == 0) {
-            const float4* aq4 = reinterpret_cast<const float4*>(aq);
-            for (int c4 = lane; c4 < (K >> 2); c4 += 32) {
-                const float4 v = __ldg(aq4 + c4);
-                f(order_key(v.x));
-                f(order_key(v.y));
-                f(order_key(v.z));
-                f(order_key(v.w));
-            }
-        } else {
-            for (int c = lane; c < K; c += 32) f(order_key(__ldg(aq + c)));
-        }
-    };
-
-    // 1. the smallest and largest order key
-    uint32_t lo = 0xffffffffu, hi = 0u;
-    each_key([&](uint32_t kk) {
-        lo = min(lo, kk);
-        hi = max(hi, kk);
-    });
-    lo = __reduce_min_sync(0xffffffffu, lo);
-    hi = __reduce_max_sync(0xffffffffu, hi);
-    const int Msel = a.near_d ? max(a.M, kProbeFeatRank) : a.M;
-    uint64_t kstar = (uint64_t)lo;  // all keys equal: nothing lies below the (Msel+1)-th
-    if (lo != hi) {
-        const int hb = 31 - __clz((int)(lo ^ hi));
-        int s = max(hb - 7, 0), w = hb - s + 1;  // the digit: bits [s, s + w)
-        uint64_t prefix = (uint64_t)lo >> (s + w) << (s + w);
-        uint32_t below = 0;  // keys under the current range
-        int rank = Msel + 1;
-        for (;;) {
-            for (int i = lane; i < 256; i += 32) hist[i] = 0;
-            __syncwarp();
-            const uint32_t dmask = (1u << w) - 1u;
-            const uint64_t want = prefix >> (s + w);
-            each_key([&](uint32_t kk) {
-                if (((uint64_t)kk >> (s + w)) == want) atomicAdd(&hist[(kk >> s) & dmask], 1u);
-            });
-            __syncwarp();
-            uint32_t h[8], sum = 0;
-#pragma unroll
-            for (int i = 0; i < 8; ++i) {
-                h[i] = hist[8 * lane + i];
-                sum += h[i];
-            }
-            uint32_t incl = sum;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
-                if (lane >= o) incl += v;
-            }
-            const uint32_t excl = incl - sum;
-            const bool mine = excl < (uint32_t)rank && incl >= (uint32_t)rank;
-            // in the lane that holds it: the bin of rank, the keys below it, its count
-            int d = 7;
-            uint32_t run = excl, hdv = 0, acc = excl;
-            bool found = false;
-#pragma unroll
-            for (int i = 0; i < 8; ++i) {
-                if (!found && acc + h[i] >= (uint32_t)rank) {
-                    found = true;
-                    d = i;
-                    run = acc;
-                    hdv = h[i];
-                }
-                acc += h[i];
-            }
-            const int src = __ffs(__ballot_sync(0xffffffffu, mine)) - 1;
-            const int dg = __shfl_sync(0xffffffffu, 8 * lane + d, src);
-            const uint32_t before = __shfl_sync(0xffffffffu, run, src);
-            const uint32_t hd = __shfl_sync(0xffffffffu, hdv, src);
-            const uint64_t b_lo = prefix | ((uint64_t)dg << s);
-            if (s == 0) {  // the (Msel+1)-th key itself
-                kstar = b_lo;
-                break;
-            }
-            if (below + before + hd <= (uint32_t)kProbeWarpCap) {  // the bucket's end
-                kstar = b_lo + (1ull << s);
-                break;
-            }
-            below += before;
-            rank -= (int)before;
-            prefix = b_lo;
-            const int s2 = max(s - 8, 0);
-            w = s - s2;
-            s = s2;
-        }
-    }
-    // the list: every centroid whose key is below kstar, keyed by (estimate, id)
+    uint64_t kstar = 0;
     int ns = 0;
-    for (int c0 = 0; c0 < K; c0 += 32) {
-        const int c = c0 + lane;
-        const uint32_t kk = c < K ? order_key(__ldg(aq + c)) : 0xffffffffu;
-        const bool in = c < K && (uint64_t)kk < kstar;
-        const uint32_t m = __ballot_sync(0xffffffffu, in);
-        if (in) sk[ns + __popc(m & lt)] = ((uint64_t)kk << 32) | (uint64_t)c;
-        ns += __popc(m);
-    }
-    __syncwarp();
-    warp_sort_list(sk, ns, lane);
-    if (a.near_d) {
-        // the 64 smallest estimates, in order, are the distance features;
-        // ranks the list misses are ties at the cut, the (Msel+1)-th estimate
-        // (a list cut at a bucket's end holds more than 64)
-        const float fill = order_key_value((uint32_t)kstar);
-        for (int j = lane; j < kProbeFeatRank; j += 32)
-            a.near_d[(size_t)q * kProbeFeatRank + j] =
-                j < ns ? order_key_value((uint32_t)(sk[j] >> 32)) : fill;
+    if (PHASE == 2) {  // the list phase 1 kept
+        ns = (int)a.list_n[q];
+        kstar = a.list_cut[q];
+        for (int j = lane; j < ns; j += 32) sk[j] = a.list[(size_t)q * kProbeWarpCap + j];
+        __syncwarp();
+    } else {
+        // f(order key) for this lane's share of the row (128-bit loads when K % 4 == 0)
+        auto each_key = [&](auto&& f) {
+            if ((K & 3) == 0) {
+                const float4* aq4 = reinterpret_cast<const float4*>(aq);
+                for (int c4 = lane; c4 < (K >> 2); c4 += 32) {
+                    const float4 v = __ldg(aq4 + c4);
+                    f(order_key(v.x));
+                    f(order_key(v.y));
+                    f(order_key(v.z));
+                    f(order_key(v.w));
+                }
+            } else {
+                for (int c = lane; c < K; c += 32) f(order_key(__ldg(aq + c)));
+            }
+        };
+
+        // 1. the smallest and largest order key
+        uint32_t lo = 0xffffffffu, hi = 0u;
+        each_key([&](uint32_t kk) {
+            lo = min(lo, kk);
+            hi = max(hi, kk);
+        });
+        lo = __reduce_min_sync(0xffffffffu, lo);
+        hi = __reduce_max_sync(0xffffffffu, hi);
+        const int Msel = a.near_d ? max(a.M, kProbeFeatRank) : a.M;
+        kstar = (uint64_t)lo;  // all keys equal: nothing lies below the (Msel+1)-th
+        if (lo != hi) {
+            const int hb = 31 - __clz((int)(lo ^ hi));
+            int s = max(hb - 7, 0), w = hb - s + 1;  // the digit: bits [s, s + w)
+            uint64_t prefix = (uint64_t)lo >> (s + w) << (s + w);
+            uint32_t below = 0;  // keys under the current range
+            int rank = Msel + 1;
+            for (;;) {
+                for (int i = lane; i < 256; i += 32) hist[i] = 0;
+                __syncwarp();
+                const uint32_t dmask = (1u << w) - 1u;
+                const uint64_t want = prefix >> (s + w);
+                each_key([&](uint32_t kk) {
+                    if (((uint64_t)kk >> (s + w)) == want) atomicAdd(&hist[(kk >> s) & dmask], 1u);
+                });
+                __syncwarp();
+                uint32_t h[8], sum = 0;
+    #pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    h[i] = hist[8 * lane + i];
+                    sum += h[i];
+                }
+                uint32_t incl = sum;
+    #pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o) incl += v;
+                }
+                const uint32_t excl = incl - sum;
+                const bool mine = excl < (uint32_t)rank && incl >= (uint32_t)rank;
+                // in the lane that holds it: the bin of rank, the keys below it, its count
+                int d = 7;
+                uint32_t run = excl, hdv = 0, acc = excl;
+                bool found = false;
+    #pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    if (!found && acc + h[i] >= (uint32_t)rank) {
+                        found = true;
+                        d = i;
+                        run = acc;
+                        hdv = h[i];
+                    }
+                    acc += h[i];
+                }
+                const int src = __ffs(__ballot_sync(0xffffffffu, mine)) - 1;
+                const int dg = __shfl_sync(0xffffffffu, 8 * lane + d, src);
+                const uint32_t before = __shfl_sync(0xffffffffu, run, src);
+                const uint32_t hd = __shfl_sync(0xffffffffu, hdv, src);
+                const uint64_t b_lo = prefix | ((uint64_t)dg << s);
+                if (s == 0) {  // the (Msel+1)-th key itself
+                    kstar = b_lo;
+                    break;
+                }
+                if (below + before + hd <= (uint32_t)kProbeWarpCap) {  // the bucket's end
+                    kstar = b_lo + (1ull << s);
+                    break;
+                }
+                below += before;
+                rank -= (int)before;
+                prefix = b_lo;
+                const int s2 = max(s - 8, 0);
+                w = s - s2;
+                s = s2;
+            }
+        }
+        // the list: every centroid whose key is below kstar, keyed by (estimate, id)
+        for (int c0 = 0; c0 < K; c0 += 32) {
+            const int c = c0 + lane;
+            const uint32_t kk = c < K ? order_key(__ldg(aq + c)) : 0xffffffffu;
+            const bool in = c < K && (uint64_t)kk < kstar;
+            const uint32_t m = __ballot_sync(0xffffffffu, in);
+            if (in) sk[ns + __popc(m & lt)] = ((uint64_t)kk << 32) | (uint64_t)c;
+            ns += __popc(m);
+        }
+        __syncwarp();
+        warp_sort_list(sk, ns, lane);
+        if (a.near_d) {
+            // the 64 smallest estimates, in order, are the distance features;
+            // ranks the list misses are ties at the cut, the (Msel+1)-th estimate
+            // (a list cut at a bucket's end holds more than 64)
+            const float fill = order_key_value((uint32_t)kstar);
+            for (int j = lane; j < kProbeFeatRank; j += 32)
+                a.near_d[(size_t)q * kProbeFeatRank + j] =
+                    j < ns ? order_key_value((uint32_t)(sk[j] >> 32)) : fill;
+        }
+        if (PHASE == 1) {  // keep the list for phase 2
+            for (int j = lane; j < ns; j += 32) a.list[(size_t)q * kProbeWarpCap + j] = sk[j];
+            if (lane == 0) {
+                a.list_n[q] = (uint32_t)ns;
+                a.list_cut[q] = kstar;
+            }
+            return;
+        }
     }
     // 2-3. exact distances of list positions [lo, hi), a half-warp each
-    const int n = min(a.check_rank, ns);
+    const int check = PHASE == 2 ? a.q_check[q] : a.check_rank;
+    const int n = min(check, ns);
     const float eps = a.eps_rel * (a.qn[q] + a.cn_max);
     const int hw = lane >> 4, l = lane & 15;
     uint32_t e_max_bits = 0u;  // the largest of the first n, as unsigned float bits
@@ -597,10 +626,11 @@ __global__ void __launch_bounds__(kProbeWarpWarps * 32) probe_warp_kernel(ProbeA
     const bool proven = P < ns || !truncated || (order_key_value((uint32_t)kstar) - eps > e_max);
     exact_range(n, P);
     warp_sort_list(sk, P, lane);
-    // a query whose cut is not proven goes to probe_exact_kernel
-    bool ok = ns >= a.check_rank;
+    // a query whose cut is not proven goes to probe_exact_kernel (so does one
+    // whose list is shorter than the nprobe slots the outputs fill)
+    bool ok = ns >= check && ns >= a.nprobe;
     if (ok && !proven) {
-        const float e_n = __uint_as_float((uint32_t)(sk[a.check_rank - 1] >> 32));
+        const float e_n = __uint_as_float((uint32_t)(sk[check - 1] >> 32));
         const float A = order_key_value((uint32_t)kstar);
         ok = (A - eps > e_n) && (e_n == e_n);
     }
