@@ -282,7 +282,7 @@ LEARNED_MIN_PROB = 0.25
 DRAM_PER_ALGORITHMIC_BYTE = {
     ("plain", "scan_kernel"): 0.0588, ("plain", "refine_kernel"): 0.418,
     ("batched", "scan_batched_kernel"): 0.0579, ("batched", "refine_kernel"): 0.418,
-    ("learned", "scan_batched_kernel"): 0.297, ("learned", "refine_kernel"): 0.414,
+    ("learned", "scan_batched_kernel"): 0.262, ("learned", "refine_kernel"): 0.415,
 }
 
 
