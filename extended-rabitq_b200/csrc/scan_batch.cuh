@@ -13,7 +13,10 @@
 // builds the QB queries' 6-dim tables exactly as scan_kernel does, at a fixed
 // stride of QSTR bytes per query, while the copies land.  A code byte's table
 // address is formed once (one byte permute) and read for every query of the
-// item with immediate offsets j * QSTR.  S, delta and sumq land where the
+// item with immediate offsets j * QSTR.  The last warp, which takes the
+// fewest of an item's blocks, claims the next item and reads its cluster,
+// pairs and sqy while the other warps finish, so a new item starts with its
+// copies and table loads at once.  S, delta and sumq land where the
 // per-pair kernel puts them: every stage downstream is unchanged and the sums
 // are bit-identical.
 #pragma once
@@ -80,6 +83,55 @@ __device__ __forceinline__ uint32_t item_cluster(const uint32_t* __restrict__ it
     return (uint32_t)lo;
 }
 
+// Words of the next-item record in shared memory (written by one warp):
+// [0] item, [1] cluster, [2] first pair of the cluster's run, [3] pairs in
+// the run, [4] blocks, [5] the cluster's first item, [6] its first block,
+// [7] unused, then the item's pairs [QB] and their probe_sqy [QB] (zero past
+// the item's last query).
+__host__ __device__ constexpr int scan_item_words(int QB) { return 8 + 2 * QB; }
+
+// Claims the next work item and reads everything the block needs to start it
+// (cluster, run, blocks, pairs, sqy) into `nx`, by one whole warp.  Run by
+// the warp with the fewest blocks while the others finish the current item,
+// so these dependent loads stay off the item's critical path.
+template <int QB>
+__device__ __forceinline__ void claim_item(const ScanBatchArgs& a, uint32_t total, uint32_t* nx,
+                                           int lane) {
+    uint32_t it = 0;
+    if (lane == 0) it = atomicAdd(a.item_counter, 1u);
+    it = __shfl_sync(0xffffffffu, it, 0);
+    if (it < total) {
+        const uint32_t c = item_cluster(a.item_off, a.K, it, lane);
+        const uint32_t start = c ? a.bucket_end[c - 1] : 0u;
+        const uint32_t m_c = a.bucket_end[c] - start;
+        const uint32_t nb = a.c_nblocks[c];
+        const uint32_t ioff = a.item_off[c];
+        const uint32_t fblock = a.c_first_block[c];
+        const uint32_t nch = max(1u, (nb + a.CB - 1) / a.CB);
+        const uint32_t qblk = (it - ioff) / nch;
+        const uint32_t qn = min((uint32_t)QB, m_c - qblk * QB);
+        if (lane < QB) {
+            uint32_t pair = 0;
+            float sqy = 0.f;
+            if ((uint32_t)lane < qn) {
+                pair = a.order_pairs[start + qblk * QB + lane];
+                sqy = a.probe_sqy[pair];
+            }
+            nx[8 + lane] = pair;
+            reinterpret_cast<float*>(nx)[8 + QB + lane] = sqy;
+        }
+        if (lane == 0) {
+            nx[1] = c;
+            nx[2] = start;
+            nx[3] = m_c;
+            nx[4] = nb;
+            nx[5] = ioff;
+            nx[6] = fblock;
+        }
+    }
+    if (lane == 0) nx[0] = it;
+}
+
 // Table bytes per query slot of the batched kernel: the classes of padded
 // dimension the kernels are built for.
 __host__ __device__ constexpr int scan_qstride(int D) {
@@ -87,11 +139,13 @@ __host__ __device__ constexpr int scan_qstride(int D) {
 }
 
 // Shared memory: [pad to 256][QB tables, QSTR apart][ring][unit_q][qq][bars]
-// [red 64 words][item fields 4][per-query delta, lower-bound constants, shift]
+// [red 64 words][4 words: table address][per-query delta, lower-bound
+// constants, shift][next-item record]
 __host__ __device__ constexpr size_t scan_batch_smem_bytes(int QB, int W, int QSTR, int D) {
     return 256 + (size_t)(QB == 1 ? (int)hex_table_bytes(D) : QB * QSTR) +
            (size_t)W * kRing * kUnitBytes + (size_t)D * 4 + (size_t)hex_qq_len(D) * 2 +
-           (size_t)W * kRing * 8 + 64 * 4 + 4 * 4 + (size_t)QB * 8 * 4;
+           (size_t)W * kRing * 8 + 64 * 4 + 4 * 4 + (size_t)QB * 8 * 4 +
+           (size_t)scan_item_words(QB) * 4;
 }
 
 template <int QB, int WARPS, int QSTR>
@@ -108,15 +162,19 @@ __global__ void __launch_bounds__(WARPS * 32) scan_batched_kernel(ScanBatchArgs 
     int16_t* qq = reinterpret_cast<int16_t*>(unit_q + D);
     const uint32_t bars_s = (uint32_t)__cvta_generic_to_shared(qq + hex_qq_len(D));
     float* red = reinterpret_cast<float*>(smem_raw + (bars_s - raw_s) + WARPS * kRing * 8);
-    uint32_t* info = reinterpret_cast<uint32_t*>(red + 64);     // item fields
+    uint32_t* info = reinterpret_cast<uint32_t*>(red + 64);     // [2]: the tables' address
     float* jk = reinterpret_cast<float*>(info + 4);             // [QB][8]: delta, c1, c2, c3, shift
+    uint32_t* nx = reinterpret_cast<uint32_t*>(jk + QB * 8);    // next-item record
     const float one_over_sqrtD = recip_via_double(__fsqrt_rn((float)D));
     const uint32_t total = a.item_off[a.K];
 
+    constexpr int kClaimWarp = WARPS - 1;  // takes the fewest blocks of every item
     if (tid == 0) {
         for (int i = 0; i < WARPS * kRing; ++i) mbar_init(bars_s + 8 * i, 1);
         mbar_init_fence();
+        info[2] = raw_s + pad;
     }
+    if (warp == kClaimWarp) claim_item<QB>(a, total, nx, lane);
     __syncthreads();
 
     UnitStream us;
@@ -133,31 +191,20 @@ __global__ void __launch_bounds__(WARPS * 32) scan_batched_kernel(ScanBatchArgs 
     bool ok = true;
 
     while (true) {
-        if (warp == 0) {
-            uint32_t it = 0;
-            if (lane == 0) it = atomicAdd(a.item_counter, 1u);
-            it = __shfl_sync(0xffffffffu, it, 0);
-            const uint32_t c = it < total ? item_cluster(a.item_off, a.K, it, lane) : 0u;
-            if (lane == 0) {
-                info[0] = it;
-                info[1] = c;
-                info[2] = raw_s + pad;
-            }
-        }
-        __syncthreads();
-        const uint32_t it = info[0];
+        // the item claimed during the previous one (or before the loop); every
+        // read of the record comes before the block barrier that precedes the
+        // claiming warp's next write
+        const uint32_t it = nx[0];
         if (it >= total) break;
-        const uint32_t c = info[1];
-        const uint32_t start = c ? a.bucket_end[c - 1] : 0u;
-        const uint32_t m_c = a.bucket_end[c] - start;
-        const uint32_t nb = a.c_nblocks[c];
+        const uint32_t c = nx[1];
+        const uint32_t m_c = nx[3];
+        const uint32_t nb = nx[4];
         const uint32_t nch = max(1u, (nb + a.CB - 1) / a.CB);
-        const uint32_t local = it - a.item_off[c];
+        const uint32_t local = it - nx[5];
         const uint32_t qblk = local / nch, chunk = local - qblk * nch;
-        const uint32_t p0 = start + qblk * QB;
         const int qn = (int)min((uint32_t)QB, m_c - qblk * QB);
         const uint32_t b0 = chunk * a.CB, b1 = min(nb, b0 + a.CB);
-        const uint32_t fblock = a.c_first_block[c];
+        const uint32_t fblock = nx[6];
 
         // this warp's blocks of the item: b0 + warp, b0 + warp + WARPS, ...
         us.count += us.total;
@@ -170,11 +217,11 @@ __global__ void __launch_bounds__(WARPS * 32) scan_batched_kernel(ScanBatchArgs 
         // tables of the item's queries (scan.cuh)
         uint32_t pairs[QB];
 #pragma unroll
-        for (int j = 0; j < QB; ++j) pairs[j] = j < qn ? a.order_pairs[p0 + j] : 0u;
+        for (int j = 0; j < QB; ++j) pairs[j] = nx[8 + j];
         for (int j = 0; j < qn; ++j) {
-            const uint32_t pair = a.order_pairs[p0 + j];
+            const uint32_t pair = nx[8 + j];
             const uint32_t q = pair / (uint32_t)a.nprobe;
-            const float sqy = a.probe_sqy[pair];
+            const float sqy = reinterpret_cast<const float*>(nx)[8 + QB + j];
             PairPrep pp;
             hex_prepare<WARPS * 32>(a.qrot + (size_t)q * D, a.centroids + (size_t)c * D, sqy, D,
                                     unit_q, qq, tables + j * tstride, red, pp);
@@ -250,7 +297,8 @@ __global__ void __launch_bounds__(WARPS * 32) scan_batched_kernel(ScanBatchArgs 
             }
             us.total = 0;
         }
-        __syncthreads();  // tables, jk and info are reused by the next item
+        if (warp == kClaimWarp) claim_item<QB>(a, total, nx, lane);
+        __syncthreads();  // tables, jk and the record are reused by the next item
     }
 }
 
