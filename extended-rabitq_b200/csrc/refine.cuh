@@ -188,12 +188,22 @@ __device__ __forceinline__ void pool_merge_block(float* pool_d, uint32_t* pool_i
                                                  float* cs, int lane) {
     const uint32_t cm = __ballot_sync(0xffffffffu, cand);
     const int nc = __popc(cm);
+    // Up to kFew candidates stay on their lanes: a candidate's rank among the
+    // block's candidates and the pool entries below it are counted by
+    // broadcast, which places it without sorting.  More are sorted (bitonic,
+    // lane j then holds the j-th) and placed by binary search.
+    constexpr int kFew = 8;
+    const bool few = nc <= kFew;
     float dv = d;
     uint32_t val = id;
-    if (nc == 1) {
-        const int src = __ffs(cm) - 1;
-        dv = __shfl_sync(0xffffffffu, d, src);
-        val = __shfl_sync(0xffffffffu, id, src);
+    bool mine = cand;
+    int rk = 0;
+    if (few) {
+        const uint64_t key = merge_key(d, lane, cand);
+        for (uint32_t m = cm; m; m &= m - 1u) {
+            const int src = __ffs(m) - 1;
+            rk += merge_key(__shfl_sync(0xffffffffu, d, src), src, true) < key;
+        }
     } else {
         uint64_t key = merge_key(d, lane, cand);
 #pragma unroll
@@ -211,18 +221,19 @@ __device__ __forceinline__ void pool_merge_block(float* pool_d, uint32_t* pool_i
                 }
             }
         }
+        rk = lane;
+        mine = lane < nc;
     }
-    // lane j (< nc) holds the j-th candidate
-    constexpr int kFew = 8;  // up to this many: counts by broadcast, else binary search
-    int lo = 0;
-    if (nc <= kFew) {
+    int lo = 0;  // pool entries below the candidate (a new value goes before equal ones)
+    if (few) {
         for (int i0 = 0; i0 < size; i0 += 32) {
             const int i = i0 + lane;
             const float pdv = i < size ? pool_d[i] : 0.f;
-            for (int j = 0; j < nc; ++j) {
-                const float dj = __shfl_sync(0xffffffffu, dv, j);
+            for (uint32_t m = cm; m; m &= m - 1u) {
+                const int src = __ffs(m) - 1;
+                const float dj = __shfl_sync(0xffffffffu, d, src);
                 const int c = __popc(__ballot_sync(0xffffffffu, i < size && pdv < dj));
-                if (lane == j) lo += c;
+                if (lane == src) lo += c;
             }
         }
     } else {
@@ -235,8 +246,9 @@ __device__ __forceinline__ void pool_merge_block(float* pool_d, uint32_t* pool_i
             }
         }
     }
-    const int rc = lane < nc ? lane + lo : k;
-    const int first = __shfl_sync(0xffffffffu, lo, 0);  // entries below it stay put
+    const int rc = mine ? rk + lo : k;
+    // entries below the smallest candidate's place stay put
+    const int first = (int)__reduce_min_sync(0xffffffffu, mine ? (uint32_t)lo : 0xffffffffu);
     __syncwarp();
     // move pool entries, top chunk first: entry i goes to i + c(i) >= i, and
     // i + c(i) strictly increases with i, so no chunk overwrites an entry
@@ -250,8 +262,8 @@ __device__ __forceinline__ void pool_merge_block(float* pool_d, uint32_t* pool_i
             pid = pool_id[i];
         }
         int c = 0;
-        if (nc <= kFew) {
-            for (int j = 0; j < nc; ++j) c += __shfl_sync(0xffffffffu, dv, j) <= pd;
+        if (few) {
+            for (uint32_t m = cm; m; m &= m - 1u) c += __shfl_sync(0xffffffffu, d, __ffs(m) - 1) <= pd;
         } else if (i < size) {
             int h2 = nc;
             while (c < h2) {
