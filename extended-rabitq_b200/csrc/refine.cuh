@@ -152,6 +152,7 @@ __device__ __forceinline__ void ex_ip_quad(const float4* __restrict__ uq4, const
 
 constexpr int kRefineThreads = 128;     // 4 warps per query
 constexpr int kWindowBlocks = 16;       // blocks whose candidates are refined together
+constexpr int kFirstWindowBlocks = 8;   // the same in the query's first probed cluster
 // Wide form for small batches (a query per SM): more warps, longer windows.
 constexpr int kWideWarps = 32;
 constexpr int kWideWindowBlocks = 128;
@@ -354,13 +355,18 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 8 : 1) refine_kernel(
         const float* bmin = a.bmin ? a.bmin + a.s_off[qp] / 32 : nullptr;
         const uint32_t nblocks = (n + 31) >> 5;
         bool uq_ready = false;
+        // The first cluster's threshold falls fast (the pool fills, then
+        // tightens), so a long window there lists many lanes that its replay
+        // drops; later clusters' thresholds barely move and long windows save
+        // barriers.
+        const int wcap = (WARPS == 4 && p == 0) ? kFirstWindowBlocks : WB;
         for (uint32_t wb = 0; wb < nblocks;) {
             const float d0 = *s_distk;
             const int filled = misc[1];
             // While the pool is filling every lane is a candidate: take just
             // enough blocks to fill it, so few lanes are refined in vain.
-            const int want = filled < k ? min(WB, max(1, (k - filled + 31) / 32))
-                                        : WB;
+            const int want = filled < k ? min(wcap, max(1, (k - filled + 31) / 32))
+                                        : wcap;
             __syncthreads();
             // warp 0 picks the window: the next `want` blocks from wb whose
             // smallest lower bound is below the threshold (a block above it
@@ -397,7 +403,7 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 8 : 1) refine_kernel(
             // lower bounds and the candidate superset, 4 blocks per warp
 #pragma unroll
             for (int i = 0; i < WB / (kThreads / 32); ++i) {
-                const int b = warp * (WB / (kThreads / 32)) + i;
+                const int b = i * (kThreads / 32) + warp;  // round robin: short windows use every warp
                 if (b < nbw) {  // uniform per warp
                     const uint32_t blk = w_blk[b];
                     const float ipq = __fmul_rn(__int2float_rn(S[32 * blk + lane]), delta);
