@@ -186,20 +186,37 @@ __device__ __forceinline__ uint64_t merge_key(float d, int lane, bool cand) {
 // (distance > its k-th): they would rank >= k and move no other entry.
 __device__ __forceinline__ void pool_merge_block(float* pool_d, uint32_t* pool_id, int& size, int k,
                                                  float& distk, bool cand, float d, uint32_t id,
-                                                 float* cs, int lane) {
+                                                 float* cs, int lane, bool count_all = false) {
     const uint32_t cm = __ballot_sync(0xffffffffu, cand);
     const int nc = __popc(cm);
-    // Up to kFew candidates stay on their lanes: a candidate's rank among the
-    // block's candidates and the pool entries below it are counted by
-    // broadcast, which places it without sorting.  More are sorted (bitonic,
-    // lane j then holds the j-th) and placed by binary search.
-    constexpr int kFew = 8;
-    const bool few = nc <= kFew;
+    // each candidate's place among the pool entries: those below it (a new
+    // value goes before equal ones), by binary search on the sorted pool
+    const auto place = [&](bool m, float v) {
+        int l = 0;
+        if (m) {
+            int hi = size;
+            while (l < hi) {
+                const int mid = (l + hi) >> 1;
+                if (pool_d[mid] < v) l = mid + 1; else hi = mid;
+            }
+        }
+        return l;
+    };
+    // Up to kFew candidates (any number with count_all) stay on their lanes:
+    // a candidate's rank among the block's candidates is counted by broadcast,
+    // and each pool entry counts the candidates below it.  More are sorted
+    // (bitonic, lane j then holds the j-th).  Sorting pays while the pool fills
+    // (blocks of up to 32 candidates spread over the whole pool); in a query's
+    // later clusters counting is cheaper at any number.
+    constexpr int kFew = 4;
+    const bool few = count_all || nc <= kFew;
+    int lo = 0;
     float dv = d;
     uint32_t val = id;
     bool mine = cand;
     int rk = 0;
     if (few) {
+        lo = place(cand, d);
         const uint64_t key = merge_key(d, lane, cand);
         for (uint32_t m = cm; m; m &= m - 1u) {
             const int src = __ffs(m) - 1;
@@ -224,32 +241,12 @@ __device__ __forceinline__ void pool_merge_block(float* pool_d, uint32_t* pool_i
         }
         rk = lane;
         mine = lane < nc;
-    }
-    int lo = 0;  // pool entries below the candidate (a new value goes before equal ones)
-    if (few) {
-        for (int i0 = 0; i0 < size; i0 += 32) {
-            const int i = i0 + lane;
-            const float pdv = i < size ? pool_d[i] : 0.f;
-            for (uint32_t m = cm; m; m &= m - 1u) {
-                const int src = __ffs(m) - 1;
-                const float dj = __shfl_sync(0xffffffffu, d, src);
-                const int c = __popc(__ballot_sync(0xffffffffu, i < size && pdv < dj));
-                if (lane == src) lo += c;
-            }
-        }
-    } else {
         cs[lane] = dv;
-        if (lane < nc) {
-            int hi = size;
-            while (lo < hi) {
-                const int mid = (lo + hi) >> 1;
-                if (pool_d[mid] < dv) lo = mid + 1; else hi = mid;
-            }
-        }
+        lo = place(mine, dv);
     }
-    const int rc = mine ? rk + lo : k;
     // entries below the smallest candidate's place stay put
     const int first = (int)__reduce_min_sync(0xffffffffu, mine ? (uint32_t)lo : 0xffffffffu);
+    const int rc = mine ? rk + lo : k;
     __syncwarp();
     // move pool entries, top chunk first: entry i goes to i + c(i) >= i, and
     // i + c(i) strictly increases with i, so no chunk overwrites an entry
@@ -517,7 +514,7 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 8 : 1) refine_kernel(
                     const bool enter = below && (size < k || !(ed > distk));
                     if (__ballot_sync(0xffffffffu, enter))
                         pool_merge_block(pool_d, pool_id, size, k, distk, enter, ed,
-                                         w_id[32 * b + lane], cs, lane);
+                                         w_id[32 * b + lane], cs, lane, p > 0);
                 }
                 if (lane == 0) {
                     *s_distk = distk;

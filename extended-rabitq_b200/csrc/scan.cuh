@@ -181,8 +181,18 @@ __device__ void hex_prepare(const float* __restrict__ q, const float* __restrict
         qq[i] = i < D ? (int16_t)quantize_round(__fdiv_rn(unit_q[i], delta)) : (int16_t)0;
     if (warp == 0) {
         float acc = 0.f;
-        if (lane < 16)
-            for (int i = lane; i < D; i += 16) acc = __fadd_rn(acc, unit_q[i]);
+        if (lane < 16) {
+            // the chain's order is fixed; its loads are not: 8 at a time ahead of the adds
+            int i = lane;
+            for (; i + 7 * 16 < D; i += 8 * 16) {
+                float v[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) v[u] = unit_q[i + 16 * u];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) acc = __fadd_rn(acc, v[u]);
+            }
+            for (; i < D; i += 16) acc = __fadd_rn(acc, unit_q[i]);
+        }
         const float s = tree16_sum(acc);
         if (lane == 0) red[NW] = normal ? s : __fmul_rn((float)D, fill);
     }
