@@ -280,9 +280,9 @@ LEARNED_MIN_PROB = 0.25
 # a launch's traffic is that ratio times its algorithmic bytes.  The ratios
 # hold for the headline workload, not for other configurations.
 DRAM_PER_ALGORITHMIC_BYTE = {
-    ("plain", "scan_kernel"): 0.0588, ("plain", "refine_kernel"): 0.418,
-    ("batched", "scan_batched_kernel"): 0.0579, ("batched", "refine_kernel"): 0.418,
-    ("learned", "scan_batched_kernel"): 0.262, ("learned", "refine_kernel"): 0.415,
+    ("plain", "scan_kernel"): 0.0589, ("plain", "refine_kernel"): 0.397,
+    ("batched", "scan_batched_kernel"): 0.0578, ("batched", "refine_kernel"): 0.400,
+    ("learned", "scan_batched_kernel"): 0.262, ("learned", "refine_kernel"): 0.397,
 }
 
 
