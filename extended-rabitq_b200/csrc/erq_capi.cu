@@ -227,6 +227,7 @@ struct erq_index {
     uint32_t* c_size = nullptr;
     uint32_t* c_nblocks = nullptr;
     uint32_t* c_size_rank = nullptr;  // [K] rank of each cluster by decreasing size (ties by id)
+    uint32_t* c_by_size = nullptr;    // [K] the clusters by decreasing size (ties by id)
     // split-BF16 operands of the tensor-core GEMMs (gemm.cuh)
     __nv_bfloat16* c_split = nullptr;   // [K][3D] centroids (hi | lo | hi)
     __nv_bfloat16* pt_split = nullptr;  // [D][3D] rows of P^T (hi | lo | hi)
@@ -247,7 +248,8 @@ struct erq_index {
         }
         for (void* p : {(void*)P, (void*)centroids, (void*)codes, (void*)onorm, (void*)excode,
                         (void*)xipnorm, (void*)ids, (void*)c_first_block, (void*)c_first_vec,
-                        (void*)c_size, (void*)c_nblocks, (void*)c_size_rank, (void*)c_split, (void*)pt_split,
+                        (void*)c_size, (void*)c_nblocks, (void*)c_size_rank, (void*)c_by_size, (void*)c_split,
+                        (void*)pt_split,
                         (void*)cn, (void*)c_chain, (void*)fac_ip, (void*)fac_sumxb, (void*)fac_err})
             if (p) cudaFree(p);
         if (prev >= 0) cudaSetDevice(prev);
@@ -444,6 +446,8 @@ erq_status load_impl(const char* path, erq_index* idx) {
         for (uint64_t r = 0; r < K; ++r) rank[byz[r]] = (uint32_t)r;
         ERQ_TRY(dev_alloc(idx, &idx->c_size_rank, K));
         ERQ_CUDA(cudaMemcpy(idx->c_size_rank, rank.data(), K * 4, cudaMemcpyHostToDevice));
+        ERQ_TRY(dev_alloc(idx, &idx->c_by_size, K));
+        ERQ_CUDA(cudaMemcpy(idx->c_by_size, byz.data(), K * 4, cudaMemcpyHostToDevice));
     }
     // split-BF16 GEMM operands: centroids and the rows of P^T
     ERQ_TRY(dev_alloc(idx, &idx->c_split, K * 3 * D));
@@ -2988,8 +2992,8 @@ erq_status launch_scan_batched(erq_plan* p, uint64_t nq, const erq_plan_tuning& 
     {
         LaunchTimer lt(kOrder, st);
         scan_items_count_kernel<<<(unsigned)div_up(K, 256), 256, 0, st>>>(
-            p->b.buckets, idx->c_nblocks, K, (int)t.queries_per_item, (int)t.blocks_per_item,
-            p->item_off);
+            p->b.buckets, idx->c_nblocks, idx->c_by_size, K, (int)t.queries_per_item,
+            (int)t.blocks_per_item, p->item_off);
         lt.finish();
     }
     {
@@ -3016,6 +3020,7 @@ erq_status launch_scan_batched(erq_plan* p, uint64_t nq, const erq_plan_tuning& 
     a.order_pairs = p->b.order_pairs;
     a.bucket_end = p->b.buckets;
     a.item_off = p->item_off;
+    a.c_order = idx->c_by_size;
     a.item_counter = p->counter;
     a.K = K;
     a.D = (int)idx->D;

@@ -43,30 +43,36 @@ struct ScanBatchArgs {
     float* bmin;                   // optional: smallest lower bound per scanned block
     const uint32_t* order_pairs;   // pairs sorted by cluster
     const uint32_t* bucket_end;    // [K + 1]: end of cluster c's run in order_pairs
-    const uint32_t* item_off;      // [K + 1]: first item of cluster c; [K] = item count
+    const uint32_t* c_order;       // [K]: the clusters in the order their items run
+    const uint32_t* item_off;      // [K + 1]: first item of c_order[j]; [K] = item count
     uint32_t* item_counter;        // zeroed before the launch
     uint32_t* status;              // device status word (bit kScanTimeoutBit)
     int K, D, nprobe, CB;
 };
 
-// items of cluster c: ceil(m_c / QB) query blocks x max(1, ceil(nb_c / CB))
-// chunks (an empty cluster still gets one item: its pairs need delta, sumq).
+// items of the j-th cluster c of c_order: ceil(m_c / QB) query blocks x
+// max(1, ceil(nb_c / CB)) chunks (an empty cluster still gets one item: its
+// pairs need delta, sumq; none when no pair probes c).  The clusters go
+// largest first, so the work list ends with short items and the persistent
+// blocks finish together.
 __global__ void scan_items_count_kernel(const uint32_t* __restrict__ bucket_end,
-                                        const uint32_t* __restrict__ c_nblocks, int K, int QB, int CB,
+                                        const uint32_t* __restrict__ c_nblocks,
+                                        const uint32_t* __restrict__ c_order, int K, int QB, int CB,
                                         uint32_t* __restrict__ item_off) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c == 0) item_off[K] = 0;
-    if (c >= K) return;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j == 0) item_off[K] = 0;
+    if (j >= K) return;
+    const uint32_t c = c_order[j];
     const uint32_t m = bucket_end[c] - (c ? bucket_end[c - 1] : 0u);
     const uint32_t nch = max(1u, (c_nblocks[c] + CB - 1) / CB);
-    item_off[c] = m ? ((m + QB - 1) / QB) * nch : 0u;
+    item_off[j] = m ? ((m + QB - 1) / QB) * nch : 0u;
 }
 
-// The cluster that owns item `it` (it < item_off[K]): the last c in [0, K)
-// with item_off[c] <= it (a cluster without items shares its successor's
-// offset, so the last one is the owner).  A 32-way search by one warp: each
-// round every lane tests one split point of the range, so K = 4096 takes 3
-// dependent loads where a binary search takes 12.
+// The position in c_order of the cluster that owns item `it` (it <
+// item_off[K]): the last j in [0, K) with item_off[j] <= it (a cluster without
+// items shares its successor's offset, so the last one is the owner).  A
+// 32-way search by one warp: each round every lane tests one split point of
+// the range, so K = 4096 takes 3 dependent loads where a binary search takes 12.
 __device__ __forceinline__ uint32_t item_cluster(const uint32_t* __restrict__ item_off, int K,
                                                  uint32_t it, int lane) {
     int lo = 0, n = K;  // invariant: item_off[lo] <= it; the owner lies in [lo, lo + n)
@@ -101,11 +107,12 @@ __device__ __forceinline__ void claim_item(const ScanBatchArgs& a, uint32_t tota
     if (lane == 0) it = atomicAdd(a.item_counter, 1u);
     it = __shfl_sync(0xffffffffu, it, 0);
     if (it < total) {
-        const uint32_t c = item_cluster(a.item_off, a.K, it, lane);
+        const uint32_t j = item_cluster(a.item_off, a.K, it, lane);
+        const uint32_t c = a.c_order[j];
         const uint32_t start = c ? a.bucket_end[c - 1] : 0u;
         const uint32_t m_c = a.bucket_end[c] - start;
         const uint32_t nb = a.c_nblocks[c];
-        const uint32_t ioff = a.item_off[c];
+        const uint32_t ioff = a.item_off[j];
         const uint32_t fblock = a.c_first_block[c];
         const uint32_t nch = max(1u, (nb + a.CB - 1) / a.CB);
         const uint32_t qblk = (it - ioff) / nch;
