@@ -287,12 +287,13 @@ __device__ __forceinline__ void pool_merge_block(float* pool_d, uint32_t* pool_i
 }
 
 // One block of WARPS warps per query (4, or 32 in the wide form).  Per window
-// of up to WB blocks of the current cluster (16, or 128): every warp computes
-// the lower bounds of WB / WARPS = 4 blocks and lists
-// the lanes below the threshold as it stands at the window's start (a superset
-// of the exact candidates, because the threshold only falls); the 32 quads
-// compute the listed candidates' exact distances (8 quads per warp; warps without a candidate
-// skip the round); warp 0 then replays the window in the reference's order -
+// of up to WB blocks of the current cluster (16, or 128; 8 in a query's first
+// cluster in the 4-warp form): the warps compute the lower bounds of the
+// window's blocks, dealt round robin, and list the lanes below the threshold
+// as it stands at the window's start (a superset of the exact candidates,
+// because the threshold only falls); the quads compute the listed candidates'
+// exact distances (8 quads per warp; warps without a candidate skip the
+// round); warp 0 then replays the window in the reference's order -
 // each block's mask against the threshold at that block's start, the block's
 // candidates merged into the pool as inserting them in lane order would.
 template <int EX, int WARPS, int WB>
