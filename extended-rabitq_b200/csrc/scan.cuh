@@ -132,12 +132,12 @@ struct PairPrep {
 };
 
 // Steps 1-3 and the tables of one (query, cluster) pair, by all NT threads of
-// the block (three block barriers).  unit_q: D floats; qq: hex_qq_len(D)
-// int16; tab: hex_table_bytes(D) bytes, 256-aligned; red: at least 40 words,
-// red[32] the shift accumulator.  q, c: the rotated query and centroid.
+// the block (two block barriers).  unit_q: D floats; tab: hex_table_bytes(D)
+// bytes, 256-aligned; red: at least 32 + NT / 32 words.  q, c: the rotated
+// query and centroid.
 template <int NT>
 __device__ void hex_prepare(const float* __restrict__ q, const float* __restrict__ c, float sqy,
-                            int D, float* unit_q, int16_t* qq, uint8_t* tab, float* red,
+                            int D, float* unit_q, uint8_t* tab, float* red,
                             PairPrep& out) {
     constexpr int NW = NT / 32;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -147,7 +147,6 @@ __device__ void hex_prepare(const float* __restrict__ q, const float* __restrict
     const float fill = recip_via_double(__fsqrt_rn((float)D));
     const float4* qv = reinterpret_cast<const float4*>(q);
     const float4* cv = reinterpret_cast<const float4*>(c);
-    int* shift_acc = reinterpret_cast<int*>(red + 32);
 
     // 1. unit_q and max |unit_q|
     float vmax = 0.f;
@@ -169,43 +168,25 @@ __device__ void hex_prepare(const float* __restrict__ q, const float* __restrict
     for (int o = 16; o > 0; o >>= 1) vmax = fmaxf(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
     if (lane == 0) red[warp] = vmax;
     __syncthreads();
-    if (tid == 0) *shift_acc = 0;  // after the barrier: the last call's readers are done
     vmax = red[0];
 #pragma unroll
     for (int w = 1; w < NW; ++w) vmax = fmaxf(vmax, red[w]);
     const float delta = __fdiv_rn(vmax, 8191.f);
 
-    // 2. qq (zero past D) and, on warp 0, sumq (16 ordered chains + tree)
-    const int nqq = hex_qq_len(D);
-    for (int i = tid; i < nqq; i += NT)
-        qq[i] = i < D ? (int16_t)quantize_round(__fdiv_rn(unit_q[i], delta)) : (int16_t)0;
-    if (warp == 0) {
-        float acc = 0.f;
-        if (lane < 16) {
-            // the chain's order is fixed; its loads are not: 8 at a time ahead of the adds
-            int i = lane;
-            for (; i + 7 * 16 < D; i += 8 * 16) {
-                float v[8];
-#pragma unroll
-                for (int u = 0; u < 8; ++u) v[u] = unit_q[i + 16 * u];
-#pragma unroll
-                for (int u = 0; u < 8; ++u) acc = __fadd_rn(acc, v[u]);
-            }
-            for (; i < D; i += 16) acc = __fadd_rn(acc, unit_q[i]);
-        }
-        const float s = tree16_sum(acc);
-        if (lane == 0) red[NW] = normal ? s : __fmul_rn((float)D, fill);
-    }
-    __syncthreads();
-
-    // 3. tables, one thread per table: entry 8m + l = H[m] + L[l] with
+    // 2. tables, one thread per table, each quantizing its own six dims
+    //    (qq = round-half-away(unit_q / delta), zero past D): entry 8m + l = H[m] + L[l] with
     //    L[l] = sum of q0..q2 over the bits of l minus their negative part and
     //    H[m] the same of q3..q5; the eight 16-byte rows go out in an order
     //    rotated by t, so the lanes of a warp store to distinct banks
     int vsum = 0;
     const int ntab = hex_chunks(D) * 16;
     for (int t = tid; t < ntab; t += NT) {
-        const int16_t* qt = qq + kHexDims * t;
+        int qt[kHexDims];
+#pragma unroll
+        for (int j = 0; j < kHexDims; ++j) {
+            const int i = kHexDims * t + j;
+            qt[j] = i < D ? (int)(int16_t)quantize_round(__fdiv_rn(unit_q[i], delta)) : 0;
+        }
         const int q0 = qt[0], q1 = qt[1], q2 = qt[2], q3 = qt[3], q4 = qt[4], q5 = qt[5];
         const int vlo = min(q0, 0) + min(q1, 0) + min(q2, 0);
         const int vhi = min(q3, 0) + min(q4, 0) + min(q5, 0);
@@ -227,11 +208,35 @@ __device__ void hex_prepare(const float* __restrict__ q, const float* __restrict
         vsum += vlo + vhi;
     }
     vsum = __reduce_add_sync(0xffffffffu, vsum);
-    if (lane == 0 && vsum) atomicAdd(shift_acc, vsum);
+    if (lane == 0) reinterpret_cast<int*>(red)[32 + warp] = vsum;
+    // sumq (16 ordered chains + tree) on the last warp, which holds the
+    // fewest tables when they do not fill the block
+    if (warp == NW - 1) {
+        float acc = 0.f;
+        if (lane < 16) {
+            // the chain's order is fixed; its loads are not: 8 at a time ahead of the adds
+            int i = lane;
+            for (; i + 7 * 16 < D; i += 8 * 16) {
+                float v[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) v[u] = unit_q[i + 16 * u];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) acc = __fadd_rn(acc, v[u]);
+            }
+            for (; i < D; i += 16) acc = __fadd_rn(acc, unit_q[i]);
+        }
+        const float s = tree16_sum(acc);
+        if (lane == 0) red[NW] = normal ? s : __fmul_rn((float)D, fill);
+    }
     __syncthreads();
+    // every red word read below was written before the barrier above, and the
+    // next call writes them only after its first barrier, which these reads precede
+    int shift = 0;
+#pragma unroll
+    for (int w = 0; w < NW; ++w) shift += reinterpret_cast<const int*>(red)[32 + w];
     out.delta = delta;
     out.sumq = red[NW];
-    out.shift = *reinterpret_cast<volatile int*>(shift_acc);
+    out.shift = shift;
 }
 
 // One warp's stream of staged code units for one cluster (or chunk of it):
@@ -291,10 +296,10 @@ struct UnitStream {
     }
 };
 
-// Shared memory of scan_kernel: [pad to 256][tables][ring][unit_q][qq][bars][red 64]
+// Shared memory of scan_kernel: [pad to 256][tables][ring][unit_q][bars][red 64]
 __host__ __device__ constexpr size_t scan_smem_bytes(int D) {
     return 256 + (size_t)hex_table_bytes(D) + (size_t)kScanWarps * kRing * kUnitBytes +
-           (size_t)D * 4 + (size_t)hex_qq_len(D) * 2 + (size_t)kScanWarps * kRing * 8 + 64 * 4;
+           (size_t)D * 4 + (size_t)kScanWarps * kRing * 8 + 64 * 4;
 }
 
 __global__ void __launch_bounds__(kScanWarps * 32, 2) scan_kernel(ScanArgs a) {
@@ -307,8 +312,7 @@ __global__ void __launch_bounds__(kScanWarps * 32, 2) scan_kernel(ScanArgs a) {
     uint8_t* tables = smem_raw + pad;
     const uint32_t ring_off = pad + hex_table_bytes(D);
     float* unit_q = reinterpret_cast<float*>(smem_raw + ring_off + kScanWarps * kRing * kUnitBytes);
-    int16_t* qq = reinterpret_cast<int16_t*>(unit_q + D);
-    const uint32_t bars_s = (uint32_t)__cvta_generic_to_shared(qq + hex_qq_len(D));
+    const uint32_t bars_s = (uint32_t)__cvta_generic_to_shared(unit_q + D);
     float* red = reinterpret_cast<float*>(smem_raw + (bars_s - raw_s) + kScanWarps * kRing * 8);
 
     const uint32_t pair = a.order ? a.order[blockIdx.x] : blockIdx.x;
@@ -342,13 +346,14 @@ __global__ void __launch_bounds__(kScanWarps * 32, 2) scan_kernel(ScanArgs a) {
 
     PairPrep pp;
     hex_prepare<kScanWarps * 32>(a.qrot + (size_t)q * D, a.centroids + (size_t)cid * D,
-                                 a.probe_sqy[pair], D, unit_q, qq, tables, red, pp);
+                                 a.probe_sqy[pair], D, unit_q, tables, red, pp);
     if (tid == 0) {
         a.qp_sumq[pair] = pp.sumq;
         a.qp_delta[pair] = pp.delta;
     }
     // The lookups are inline PTX; their addresses derive from this shared read,
     // which cannot move above the barriers of hex_prepare.
+    static_assert(32 + kScanWarps <= 40, "hex_prepare's per-warp sums end below red[40]");
     const uint32_t tables_s = reinterpret_cast<volatile uint32_t*>(red)[40];
     const float y = __fsqrt_rn(a.probe_sqy[pair]);
     const LbConsts lbk = lb_consts(pp.sumq, y, recip_via_double(__fsqrt_rn((float)D)));

@@ -145,13 +145,12 @@ __host__ __device__ constexpr int scan_qstride(int D) {
     return D <= 768 ? 16384 : (D <= 1536 ? 32768 : 45056);
 }
 
-// Shared memory: [pad to 256][QB tables, QSTR apart][ring][unit_q][qq][bars]
+// Shared memory: [pad to 256][QB tables, QSTR apart][ring][unit_q][bars]
 // [red 64 words][4 words: table address][per-query delta, lower-bound
 // constants, shift][next-item record]
 __host__ __device__ constexpr size_t scan_batch_smem_bytes(int QB, int W, int QSTR, int D) {
     return 256 + (size_t)(QB == 1 ? (int)hex_table_bytes(D) : QB * QSTR) +
-           (size_t)W * kRing * kUnitBytes + (size_t)D * 4 + (size_t)hex_qq_len(D) * 2 +
-           (size_t)W * kRing * 8 + 64 * 4 + 4 * 4 + (size_t)QB * 8 * 4 +
+           (size_t)W * kRing * kUnitBytes + (size_t)D * 4 + (size_t)W * kRing * 8 + 64 * 4 + 4 * 4 + (size_t)QB * 8 * 4 +
            (size_t)scan_item_words(QB) * 4;
 }
 
@@ -166,8 +165,7 @@ __global__ void __launch_bounds__(WARPS * 32) scan_batched_kernel(ScanBatchArgs 
     uint8_t* tables = smem_raw + pad;
     const uint32_t ring_off = pad + QB * tstride;
     float* unit_q = reinterpret_cast<float*>(smem_raw + ring_off + WARPS * kRing * kUnitBytes);
-    int16_t* qq = reinterpret_cast<int16_t*>(unit_q + D);
-    const uint32_t bars_s = (uint32_t)__cvta_generic_to_shared(qq + hex_qq_len(D));
+    const uint32_t bars_s = (uint32_t)__cvta_generic_to_shared(unit_q + D);
     float* red = reinterpret_cast<float*>(smem_raw + (bars_s - raw_s) + WARPS * kRing * 8);
     uint32_t* info = reinterpret_cast<uint32_t*>(red + 64);     // [2]: the tables' address
     float* jk = reinterpret_cast<float*>(info + 4);             // [QB][8]: delta, c1, c2, c3, shift
@@ -231,7 +229,7 @@ __global__ void __launch_bounds__(WARPS * 32) scan_batched_kernel(ScanBatchArgs 
             const float sqy = reinterpret_cast<const float*>(nx)[8 + QB + j];
             PairPrep pp;
             hex_prepare<WARPS * 32>(a.qrot + (size_t)q * D, a.centroids + (size_t)c * D, sqy, D,
-                                    unit_q, qq, tables + j * tstride, red, pp);
+                                    unit_q, tables + j * tstride, red, pp);
             if (tid == 0) {
                 if (chunk == 0) {
                     a.qp_sumq[pair] = pp.sumq;
