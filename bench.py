@@ -281,8 +281,8 @@ LEARNED_MIN_PROB = 0.25
 # hold for the headline workload, not for other configurations.
 DRAM_PER_ALGORITHMIC_BYTE = {
     ("plain", "scan_kernel"): 0.0589, ("plain", "refine_kernel"): 0.397,
-    ("batched", "scan_batched_kernel"): 0.0578, ("batched", "refine_kernel"): 0.400,
-    ("learned", "scan_batched_kernel"): 0.262, ("learned", "refine_kernel"): 0.397,
+    ("batched", "scan_batched_kernel"): 0.0587, ("batched", "refine_kernel"): 0.397,
+    ("learned", "scan_batched_kernel"): 0.260, ("learned", "refine_kernel"): 0.397,
 }
 
 
