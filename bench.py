@@ -524,7 +524,48 @@ def run_ours(args, cfg, name):
     # --- batched plans (CUDA graphs, work-list scan, autotuned tiles)
     from erq_b200 import Plan
 
-    def plan_mode(plan, expect, label):
+    qh2 = qh.clone().pin_memory()
+    ids_h2 = torch.empty_like(ids_h).pin_memory()
+    dist_h2 = torch.empty_like(dist_h).pin_memory()
+
+    def timed_two_plans(plans, steps, warmup):
+        """Pinned host buffers, two plans of the same settings on two streams,
+        consecutive steps alternating between them (a serving loop with two
+        batches in flight): a step's copies in and out run under the other
+        plan's search.  Timed between CUDA events on `stream`, the second
+        stream joined before the end event; returns max-over-ranks ms."""
+        streams = (stream, torch.cuda.Stream())
+        bufs = ((qh, ids_h, dist_h), (qh2, ids_h2, dist_h2))
+
+        def step(i):
+            plans[i % 2].search_buffers_async(*bufs[i % 2], stream=streams[i % 2])
+
+        for i in range(warmup):
+            step(i)
+        torch.cuda.synchronize()
+        barrier(world)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(streams[0])
+        streams[1].wait_event(e0)
+        for i in range(steps):
+            step(i)
+        streams[0].wait_stream(streams[1])
+        e1.record(streams[0])
+        torch.cuda.synchronize()
+        barrier(world)
+        return max_over_ranks(e0.elapsed_time(e1), world)
+
+    def twin_plan(plan, tune, mdl=None, conf=None):
+        """A second plan with `plan`'s settings, for the two-stream serving loop."""
+        tw = Plan(idx, max_batch=nq, k=k, nprobe=nprobe, model=mdl, raw=True)
+        if mdl is not None:
+            tw.set_learned(conf, LEARNED_MIN_PROB)
+        tw.set_tuning(nq, tune["queries_per_item"], tune["blocks_per_item"], tune["warps"],
+                      tune["refine_warps"])
+        return tw
+
+    def plan_mode(plan, expect, label, twin=None):
         def dev():
             plan.search_buffers(qd, ids_d, dist_d, stream=stream)
 
@@ -537,12 +578,20 @@ def run_ours(args, cfg, name):
         ms, _, clocks = timed(dev, args.steps, args.warmup, world, stream, local, label=label)
         assert (ids_d.cpu().numpy().view(np.uint32) == expect).all()
         e2e = None
+        plan.e2e_one_stream_ms = None
         if not args.no_e2e:
             e2e, _, _ = timed(host, args.steps, args.warmup, world, stream)
             assert (ids_h.numpy().view(np.uint32) == expect).all()
+            plan.e2e_one_stream_ms = e2e
             e2e_sync, _, _ = timed(host_sync, args.steps, args.warmup, world, stream)
             assert (ids_h.numpy().view(np.uint32) == expect).all()
             plan.e2e_sync_ms = e2e_sync
+            if twin is not None:
+                ids_h.fill_(-1)
+                ids_h2.fill_(-1)
+                e2e = timed_two_plans((plan, twin), args.steps, args.warmup)
+                assert (ids_h.numpy().view(np.uint32) == expect).all()
+                assert (ids_h2.numpy().view(np.uint32) == expect).all()
         # per-kernel times: the same steps with the kernels launched one by one
         plan.set_graphs(False)
         _, prof, _ = timed(dev, args.steps, 1, world, stream, label=label + "-kernels")
@@ -556,7 +605,8 @@ def run_ours(args, cfg, name):
     if not args.no_batched:
         plan_b = Plan(idx, max_batch=nq, k=k, nprobe=nprobe, raw=True)
         tune_b, _ = plan_b.autotune(query, reps=2)
-        ms_b, e2e_b, clocks_b, prof_b = plan_mode(plan_b, ids0, "batched")
+        twin_b = None if args.no_e2e else twin_plan(plan_b, tune_b)
+        ms_b, e2e_b, clocks_b, prof_b = plan_mode(plan_b, ids0, "batched", twin_b)
         batched = {"value": round(world * nq * args.steps / (ms_b / 1e3), 1), "nprobe": nprobe,
                    "recall@100": round(recall, 5), "ms_per_step": round(ms_b / args.steps, 4),
                    "tuning": tune_b,
@@ -564,11 +614,15 @@ def run_ours(args, cfg, name):
                                            if v[0]}}
         if e2e_b is not None:
             batched["e2e"] = round(world * nq * args.steps / (e2e_b / 1e3), 1)
+            batched["e2e_one_stream"] = round(world * nq * args.steps / (plan_b.e2e_one_stream_ms / 1e3), 1)
             batched["e2e_sync"] = round(world * nq * args.steps / (plan_b.e2e_sync_ms / 1e3), 1)
         modes["batched"] = {"ms": ms_b, "prof": prof_b, "clocks": clocks_b, "recall": recall,
                             "ids": ids0, "scan_bytes": scan_bytes_plain, "e2e_ms": e2e_b,
+                            "e2e_one_stream_ms": plan_b.e2e_one_stream_ms,
                             "refine_bytes": cand_plain * cand_bytes}
         plan_b.free()
+        if twin_b is not None:
+            twin_b.free()
 
     # --- learned per-query depth, batched
     learned_info = None
@@ -606,7 +660,10 @@ def run_ours(args, cfg, name):
             log(f"learned probe fallback rate {learned_fallback_rate:.5f}; refinement per "
                 "query: " + ", ".join(f"{kk} {v / nq:.1f}" for kk, v in rst_l.items()))
             tune_l, _ = plan_l.autotune(query, reps=2)
-            ms_l, e2e_l, clocks_l, prof_l = plan_mode(plan_l, ids_l, "learned")
+            twin_l = None if args.no_e2e else twin_plan(plan_l, tune_l, model, conf)
+            ms_l, e2e_l, clocks_l, prof_l = plan_mode(plan_l, ids_l, "learned", twin_l)
+            if twin_l is not None:
+                twin_l.free()
             take = np.arange(cids.shape[1])[None, :] < used.astype(np.int64)[:, None]
             scan_bytes_l = int(nblocks[cids.astype(np.int64)][take].sum()) * block_bytes
             learned_info = {"value": round(world * nq * args.steps / (ms_l / 1e3), 1),
@@ -622,9 +679,12 @@ def run_ours(args, cfg, name):
                             "model": meta}
             if e2e_l is not None:
                 learned_info["e2e"] = round(world * nq * args.steps / (e2e_l / 1e3), 1)
+                learned_info["e2e_one_stream"] = round(
+                    world * nq * args.steps / (plan_l.e2e_one_stream_ms / 1e3), 1)
                 learned_info["e2e_sync"] = round(world * nq * args.steps / (plan_l.e2e_sync_ms / 1e3), 1)
             modes["learned"] = {"ms": ms_l, "prof": prof_l, "clocks": clocks_l, "recall": r_l,
                                 "ids": ids_l, "scan_bytes": scan_bytes_l, "e2e_ms": e2e_l,
+                                "e2e_one_stream_ms": plan_l.e2e_one_stream_ms,
                                 "refine_bytes": cand_l * cand_bytes}
             learned_for_parity = (model, conf)
         plan_l.free()
@@ -737,8 +797,12 @@ def run_ours(args, cfg, name):
                 "d2h_bytes_per_step": int(nq * k * 8),
                 "api": ("erq_search_raw, pinned host buffers, one synchronous call per step"
                         if mode == "plain" else
-                        "erq_plan_search_async, pinned host buffers: a step's query copy-in "
-                        "overlaps the previous step's search; results copied out every step")},
+                        "erq_plan_search_async on two plans of the same settings and two "
+                        "streams, consecutive steps alternating, pinned host buffers: a step's "
+                        "copies in and out run under the other plan's search; queries copied in "
+                        "and results copied out every step"),
+                "one_stream": (None if chosen.get("e2e_one_stream_ms") is None else round(
+                    world * nq * args.steps / (chosen["e2e_one_stream_ms"] / 1e3), 1))},
             "gpu_launches": int(launches),
             "roofline": rooflines.get(dominant),
             "roofline_other": {kn: r for kn, r in rooflines.items() if kn != dominant},
